@@ -1,0 +1,711 @@
+// dampm_api.cu -- the extern "C" boundary (include/dampm_cuda.h).
+//
+// Host orchestration of the sm_100a step: device buffers owned by the
+// context, all kernels enqueued on one stream, loop state kept on the device
+// (Scalars) so that dampm_step() never synchronises.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dampm_cuda.h"
+#include "dampm_kernels.h"
+#include "ms_kernels.h"
+
+using namespace dampm;
+
+struct dampm_ctx {
+  dampm_grid grid{};
+  dampm_params params{};
+  dampm_ms_params ms{};
+  int precision = DAMPM_FP64;
+  Geom G{};
+  Phys P{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  long long cap = 0;
+  int nn = 0, nc = 0;
+  Particles p{};
+  Nodes nodes{};
+  double *Z = nullptr, *dZdx = nullptr, *dZdy = nullptr;
+  int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr,
+      *tile_sum = nullptr;
+  int ntiles = 0;
+  double* led_part = nullptr;
+  int n_led = 0;
+  Scalars* S = nullptr;
+  Scalars* Sh = nullptr;  // pinned host mirror
+  MsBuffers msb{};
+  bool terrain_ok = false, particles_ok = false;
+  bool ms_enabled = false;
+  bool record = false;
+  bool record_alloc = false;
+  long long it_host = 0;  // passes enqueued since upload (= device it while active)
+  long long launches = 0;
+  std::string err;
+  std::vector<void*> allocs;
+  // timing
+  bool timing = false;
+  std::vector<cudaEvent_t> evpool;
+  int evused = 0;
+  std::vector<int> evclass;  // class of the interval ending at event k
+};
+
+namespace {
+
+#define CK(call)                                                          \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);      \
+      return DAMPM_ERR_CUDA;                                              \
+    }                                                                     \
+  } while (0)
+
+int fail(dampm_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+template <class T>
+int dalloc(dampm_ctx* ctx, T** ptr, size_t n) {
+  void* q = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+  if (e != cudaSuccess) {
+    ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return DAMPM_ERR_CUDA;
+  }
+  ctx->allocs.push_back(q);
+  *ptr = static_cast<T*>(q);
+  return DAMPM_OK;
+}
+
+int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return int(b);
+}
+
+void ev_mark(dampm_ctx* ctx, int cls) {
+  if (!ctx->timing) return;
+  if (ctx->evused == (int)ctx->evpool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->evpool.push_back(e);
+    ctx->evclass.push_back(0);
+  }
+  ctx->evclass[ctx->evused] = cls;
+  cudaEventRecord(ctx->evpool[ctx->evused], ctx->stream);
+  ctx->evused++;
+}
+
+int alloc_record(dampm_ctx* ctx) {
+  if (ctx->record_alloc) return DAMPM_OK;
+  const long long cap = ctx->cap;
+  Particles& p = ctx->p;
+  double** pf[] = {&p.apx, &p.apy, &p.Zp, &p.hpZ, &p.dZxp, &p.dZyp,
+                   &p.Fpx, &p.Fpy, &p.Frx, &p.Fry};
+  for (double** q : pf) {
+    int rc = dalloc(ctx, q, cap);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(*q, 0, cap * sizeof(double), ctx->stream));
+  }
+  Nodes& n = ctx->nodes;
+  double** nf[] = {&n.Mv,   &n.mvx,  &n.mvy,   &n.avx,   &n.avy,
+                   &n.vvx,  &n.vvy,  &n.FPxv,  &n.FPyv,  &n.Fricx,
+                   &n.Fricy, &n.Fintx, &n.Finty, &n.HV};
+  for (double** q : nf) {
+    int rc = dalloc(ctx, q, ctx->nn);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(*q, 0, ctx->nn * sizeof(double), ctx->stream));
+  }
+  ctx->record_alloc = true;
+  return DAMPM_OK;
+}
+
+int alloc_particles(dampm_ctx* ctx, long long cap) {
+  ctx->cap = cap;
+  Particles& p = ctx->p;
+  double** f[] = {&p.x,     &p.y,     &p.vpx,    &p.vpy,    &p.hp,
+                  &p.F11,   &p.F12,   &p.F22,    &p.Mp,     &p.Vp,
+                  &p.H,     &p.Ap,    &p.mpx,    &p.mpy,    &p.Fbx,
+                  &p.Fby,   &p.vpx_dx, &p.vpx_dy, &p.vpy_dx, &p.vpy_dy,
+                  &p.xp,    &p.yp};
+  for (double** q : f) {
+    int rc = dalloc(ctx, q, cap);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(*q, 0, cap * sizeof(double), ctx->stream));
+  }
+  int** fi[] = {&p.label, &p.level, &p.key, &ctx->slot, &ctx->perm};
+  for (int** q : fi) {
+    int rc = dalloc(ctx, q, cap);
+    if (rc) return rc;
+  }
+  int rc = ms_alloc(ctx->msb, cap, ctx->nc, [&](void** q, size_t bytes) {
+    return dalloc(ctx, reinterpret_cast<unsigned char**>(q), bytes);
+  });
+  if (rc) return rc;
+  if (ctx->record) return alloc_record(ctx);
+  return DAMPM_OK;
+}
+
+// Enqueues the binning of the current particles (SORT).
+void enqueue_sort(dampm_ctx* ctx) {
+  const int gp = grid_for(ctx->cap, 256);
+  k_count<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->count, ctx->slot, ctx->S);
+  k_scan_tiles<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(ctx->count, ctx->nc,
+                                                              ctx->tile_sum, ctx->S);
+  k_scan_tile_sums<<<1, kScanThreads, 0, ctx->stream>>>(ctx->tile_sum, ctx->ntiles,
+                                                        ctx->S);
+  k_scan_apply<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(
+      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->S);
+  k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->slot, ctx->start,
+                                         ctx->perm, ctx->S);
+  k_segment_order<<<grid_for(ctx->nc, 256), 256, 0, ctx->stream>>>(
+      ctx->start, ctx->nc, ctx->perm, ctx->S);
+  ctx->launches += 6;
+}
+
+int enqueue_pass(dampm_ctx* ctx) {
+  const long long it_next = ctx->it_host + 1;
+  const bool ms_due = ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 &&
+                      ctx->ms.call_interval > 0 &&
+                      (it_next % ctx->ms.call_interval) == 0;
+  // the pass after the merge/split call needs the gradients of this one
+  const bool grad_next = ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 &&
+                         ctx->ms.call_interval > 0 &&
+                         ((it_next + 1) % ctx->ms.call_interval) == 0;
+  ev_mark(ctx, 3);
+  k_step_begin<<<1, 1, 0, ctx->stream>>>(ctx->S, ctx->G, ctx->P);
+  ctx->launches += 1;
+  if (ms_due) {
+    enqueue_sort(ctx);
+    ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc,
+                                ctx->G, ctx->P, ctx->ms, ctx->S, ctx->cap,
+                                ctx->stream, /*use_step_dt=*/1, 0.0);
+    k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(
+        ctx->p.x, ctx->p.y, ctx->p.key, ctx->G, ctx->S);
+    ctx->launches += 1;
+  }
+  ev_mark(ctx, 0);
+  enqueue_sort(ctx);
+  ev_mark(ctx, 1);
+  dim3 pg((ctx->grid.Ney + 1 + kTR - 1) / kTR, (ctx->grid.Nex + 1 + kLC - 1) / kLC);
+  k_p2g<<<pg, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
+      ctx->p, ctx->perm, ctx->start, ctx->Z, ctx->nodes, ctx->led_part, ctx->G,
+      ctx->P, ctx->S, ctx->record ? 1 : 0);
+  ev_mark(ctx, 3);
+  k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->n_led, ctx->S);
+  ev_mark(ctx, 2);
+  k_g2p<<<grid_for(ctx->cap, kG2PThreads), kG2PThreads, 0, ctx->stream>>>(
+      ctx->p, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
+      (grad_next || ctx->record) ? 1 : 0);
+  ev_mark(ctx, 3);
+  k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->S);
+  ctx->launches += 4;
+  ctx->it_host = it_next;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  return DAMPM_OK;
+}
+
+int sync_status(dampm_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->Sh, ctx->S, sizeof(Scalars), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->Sh->status & kStatusCapacity)
+    return fail(ctx, DAMPM_ERR_CAPACITY, "particle capacity exceeded by merge/split");
+  if (ctx->Sh->status)
+    return fail(ctx, DAMPM_ERR_DEVICE, "device status word set");
+  return DAMPM_OK;
+}
+
+Phys make_phys(const dampm_params& d) {
+  Phys P{};
+  P.g = d.g;
+  P.rho = d.rho;
+  P.mu = d.mu;
+  P.tauy = d.tauy;
+  P.xi = d.xi;
+  const double fric_ang = d.phi * M_PI / 180.;  // main/optim_par.cpp:193
+  P.tan_fa = std::tan(fric_ang);
+  P.BING = d.BINGHAM_ON;
+  P.FON = d.FRICTION_ON;
+  P.CFL = d.CFL;
+  P.eq_level = d.eq_level;
+  P.DT_FIXED = d.DT_FIXED;
+  P.T = d.T;
+  P.BC = d.BC_FLAG;
+  P.NSTEPS = d.NSTEPS;
+  P.fixed = d.DT_FIXED > 0.0 ? 1 : 0;
+  return P;
+}
+
+__global__ void k_int_to_double(const int* a, double* b, const Scalars* S) {
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x)
+    b[i] = double(a[i]);
+}
+
+// Ap, mom, Fb as the reference stores them at the end of a step
+// (main/optim_par.cpp:600-626), from the persistent state.
+__global__ void k_derived(Particles p, Phys P, const Scalars* S, int which,
+                          double* out) {
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    const double hp = p.hp[i];
+    double v = 0.0;
+    if (which == 0) v = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
+    else if (which == 1) v = p.vpx[i] * p.Mp[i];
+    else if (which == 2) v = p.vpy[i] * p.Mp[i];
+    else {
+      double fx, fy;
+      voellmy(P, p.vpx[i], p.vpy[i], hp, fx, fy);
+      v = (which == 3) ? fx : fy;
+    }
+    out[i] = v;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dampm_version(void) { return "dampm-b200 0.1 (sm_100a)"; }
+
+const char* dampm_last_error(dampm_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
+                     const dampm_ms_params* ms, int precision,
+                     long long capacity, void* cuda_stream, dampm_ctx** out) {
+  if (!grid || !params || !out) return DAMPM_ERR_ARG;
+  if (grid->Nex < 1 || grid->Ney < 1 || !(grid->hx > 0) || !(grid->hy > 0))
+    return DAMPM_ERR_ARG;
+  if (precision != DAMPM_FP64) return DAMPM_ERR_ARG;
+  const long long nn = (long long)(grid->Nex + 1) * (grid->Ney + 1);
+  if (nn > 0x7fffffffLL) return DAMPM_ERR_ARG;
+  dampm_ctx* ctx = new dampm_ctx();
+  ctx->grid = *grid;
+  ctx->params = *params;
+  if (ms) {
+    ctx->ms = *ms;
+  } else {  // main/mpm_data.h:102-112
+    ctx->ms = dampm_ms_params{0.9, 0.30, 0.0, 1e30, 0.05, 0.01, -2, 2, 2, 10, 1e9};
+  }
+  ctx->precision = precision;
+  ctx->G.nrows = grid->Ney;
+  ctx->G.ncols = grid->Nex;
+  ctx->G.hx = grid->hx;
+  ctx->G.hy = grid->hy;
+  ctx->G.Lx = grid->Nex * grid->hx;
+  ctx->G.Ly = grid->Ney * grid->hy;
+  ctx->P = make_phys(*params);
+  ctx->nn = int(nn);
+  ctx->nc = grid->Nex * grid->Ney;
+  ctx->cap = capacity;
+  if (cuda_stream) {
+    ctx->stream = static_cast<cudaStream_t>(cuda_stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return DAMPM_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+  }
+  int rc = DAMPM_OK;
+  rc = rc ? rc : dalloc(ctx, &ctx->Z, nn);
+  rc = rc ? rc : dalloc(ctx, &ctx->dZdx, nn);
+  rc = rc ? rc : dalloc(ctx, &ctx->dZdy, nn);
+  rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvxL, nn);
+  rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvyL, nn);
+  ctx->ntiles = (ctx->nc + kScanTile - 1) / kScanTile;
+  rc = rc ? rc : dalloc(ctx, &ctx->count, ctx->nc);
+  rc = rc ? rc : dalloc(ctx, &ctx->start, size_t(ctx->nc) + 1);
+  rc = rc ? rc : dalloc(ctx, &ctx->tile_sum, size_t(ctx->ntiles) + 1);
+  const int strips = (grid->Ney + 1 + kTR - 1) / kTR;
+  const int chunks = (grid->Nex + 1 + kLC - 1) / kLC;
+  if (chunks > 65535) rc = rc ? rc : fail(ctx, DAMPM_ERR_ARG, "grid too wide");
+  ctx->n_led = strips * chunks;
+  rc = rc ? rc : dalloc(ctx, &ctx->led_part, size_t(ctx->n_led) * 6);
+  rc = rc ? rc : dalloc(ctx, &ctx->S, 1);
+  if (rc == DAMPM_OK) {
+    if (cudaMallocHost(&ctx->Sh, sizeof(Scalars)) != cudaSuccess) rc = DAMPM_ERR_CUDA;
+  }
+  if (rc == DAMPM_OK) {
+    cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream);
+    cudaMemsetAsync(ctx->nodes.vvxL, 0, sizeof(double) * nn, ctx->stream);
+    cudaMemsetAsync(ctx->nodes.vvyL, 0, sizeof(double) * nn, ctx->stream);
+    cudaMemsetAsync(ctx->S, 0, sizeof(Scalars), ctx->stream);
+    const size_t smem = p2g_smem_bytes();
+    if (cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smem)) != cudaSuccess)
+      rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+  }
+  if (rc != DAMPM_OK) {
+    dampm_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return DAMPM_OK;
+}
+
+int dampm_ctx_destroy(dampm_ctx* ctx) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void* q : ctx->allocs) cudaFree(q);
+  for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->Sh) cudaFreeHost(ctx->Sh);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return DAMPM_OK;
+}
+
+int dampm_upload_terrain(dampm_ctx* ctx, const double* Z, const double* dZdx,
+                         const double* dZdy) {
+  if (!ctx || !Z || !dZdx || !dZdy) return DAMPM_ERR_ARG;
+  const size_t b = sizeof(double) * ctx->nn;
+  CK(cudaMemcpyAsync(ctx->Z, Z, b, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->dZdx, dZdx, b, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->dZdy, dZdy, b, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->terrain_ok = true;
+  return DAMPM_OK;
+}
+
+int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
+                           const double* y, const double* Mp, const double* Ap,
+                           const double* vpx, const double* vpy,
+                           const double* hp, const double* mom_px,
+                           const double* mom_py, const double* Vp) {
+  if (!ctx || np < 0 || np > 0x7fffffffLL) return DAMPM_ERR_ARG;
+  if (np > 0 && (!x || !y || !Mp || !Ap || !vpx || !vpy || !hp || !mom_px ||
+                 !mom_py || !Vp))
+    return DAMPM_ERR_ARG;
+  if (!ctx->terrain_ok) return fail(ctx, DAMPM_ERR_STATE, "upload terrain first");
+  if (ctx->p.x == nullptr) {
+    long long cap = ctx->cap > 0 ? ctx->cap : 2 * np + 1024;
+    if (cap < np) return fail(ctx, DAMPM_ERR_CAPACITY, "capacity below particle count");
+    int rc = alloc_particles(ctx, cap);
+    if (rc) return rc;
+  } else if (np > ctx->cap) {
+    return fail(ctx, DAMPM_ERR_CAPACITY, "capacity below particle count");
+  }
+  const size_t b = sizeof(double) * np;
+  Particles& p = ctx->p;
+  if (np > 0) {
+    CK(cudaMemcpyAsync(p.x, x, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.y, y, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.xp, x, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.yp, y, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.Mp, Mp, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.Ap, Ap, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.vpx, vpx, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.vpy, vpy, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.hp, hp, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.mpx, mom_px, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.mpy, mom_py, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.Vp, Vp, b, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  Scalars s0{};
+  s0.fresh = 1;
+  s0.np = int(np);
+  *ctx->Sh = s0;
+  CK(cudaMemcpyAsync(ctx->S, ctx->Sh, sizeof(Scalars), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));  // Sh is reused below
+  if (np > 0) {
+    k_init_particles<<<grid_for(np, 256), 256, 0, ctx->stream>>>(
+        p, ctx->Z, ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np));
+    CK(cudaGetLastError());
+  }
+  ctx->it_host = 0;
+  ctx->particles_ok = true;
+  return sync_status(ctx);
+}
+
+int dampm_enable_merge_split(dampm_ctx* ctx, int enable) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  ctx->ms_enabled = enable != 0;
+  return DAMPM_OK;
+}
+
+int dampm_record_outputs(dampm_ctx* ctx, int enable) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  ctx->record = enable != 0;
+  if (ctx->record && ctx->p.x) return alloc_record(ctx);
+  return DAMPM_OK;
+}
+
+int dampm_step(dampm_ctx* ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return DAMPM_ERR_ARG;
+  if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
+  ctx->launches = 0;
+  ctx->evused = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = enqueue_pass(ctx);
+    if (rc) return rc;
+  }
+  ev_mark(ctx, 3);
+  return DAMPM_OK;
+}
+
+int dampm_sync(dampm_ctx* ctx) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  return sync_status(ctx);
+}
+
+int dampm_run(dampm_ctx* ctx, long long max_steps, int chunk,
+              long long* steps_done) {
+  if (!ctx || chunk < 1) return DAMPM_ERR_ARG;
+  long long done = 0;
+  int it0 = 0;
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  it0 = ctx->Sh->it;
+  while (done < max_steps) {
+    const int n = int(std::min<long long>(chunk, max_steps - done));
+    rc = dampm_step(ctx, n);
+    if (rc) return rc;
+    rc = sync_status(ctx);
+    if (rc) return rc;
+    done += n;
+    if (!ctx->Sh->active) break;
+  }
+  // passes whose loop condition failed did nothing: realign the host count
+  ctx->it_host = ctx->Sh->it;
+  if (steps_done) *steps_done = ctx->Sh->it - it0;
+  return DAMPM_OK;
+}
+
+int dampm_status(dampm_ctx* ctx, int* it, double* t, double* dt_last,
+                 long long* np) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  if (it) *it = ctx->Sh->it;
+  if (t) *t = ctx->Sh->t;
+  if (dt_last) *dt_last = ctx->Sh->dt;
+  if (np) *np = ctx->Sh->np;
+  return DAMPM_OK;
+}
+
+int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
+  // bin with the current positions, then decide + emit (an always-active
+  // pass: the loop condition does not apply to a standalone call)
+  Scalars* S = ctx->S;
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  const int active_save = ctx->Sh->active;
+  ctx->Sh->active = 1;
+  CK(cudaMemcpyAsync(&S->active, &ctx->Sh->active, sizeof(int),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  enqueue_sort(ctx);
+  ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
+             ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt);
+  k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.x, ctx->p.y,
+                                                           ctx->p.key, ctx->G, ctx->S);
+  CK(cudaGetLastError());
+  rc = sync_status(ctx);
+  if (rc) return rc;
+  ctx->Sh->active = active_save;
+  CK(cudaMemcpyAsync(&S->active, &ctx->Sh->active, sizeof(int),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  if (counts)
+    for (int k = 0; k < 4; ++k) counts[k] = ctx->Sh->ms_counts[k];
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
+  if (!ctx || !field || !out) return DAMPM_ERR_ARG;
+  if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "no particles");
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  const int np = ctx->Sh->np;
+  const bool fresh = ctx->Sh->fresh != 0;
+  const std::string f(field);
+  Particles& p = ctx->p;
+  const double* src = nullptr;
+  const int* isrc = nullptr;
+  int derived = -1;
+  if (f == "x") src = p.x;
+  else if (f == "y") src = p.y;
+  else if (f == "Mp") src = p.Mp;
+  else if (f == "Vp") src = p.Vp;
+  else if (f == "H") src = p.H;
+  else if (f == "hp") src = p.hp;
+  else if (f == "vpx" || f == "vpxL") src = p.vpx;
+  else if (f == "vpy" || f == "vpyL") src = p.vpy;
+  else if (f == "F_11") src = p.F11;
+  else if (f == "F_12" || f == "F_21") src = p.F12;
+  else if (f == "F_22") src = p.F22;
+  else if (f == "xp") src = p.xp;
+  else if (f == "yp") src = p.yp;
+  else if (f == "vpx_dx") src = p.vpx_dx;
+  else if (f == "vpx_dy") src = p.vpx_dy;
+  else if (f == "vpy_dx") src = p.vpy_dx;
+  else if (f == "vpy_dy") src = p.vpy_dy;
+  else if (f == "label") isrc = p.label;
+  else if (f == "level") isrc = p.level;
+  else if (f == "Ap") { if (fresh) src = p.Ap; else derived = 0; }
+  else if (f == "mom_px") { if (fresh) src = p.mpx; else derived = 1; }
+  else if (f == "mom_py") { if (fresh) src = p.mpy; else derived = 2; }
+  else if (f == "Fb_x") { if (fresh) src = p.Fbx; else derived = 3; }
+  else if (f == "Fb_y") { if (fresh) src = p.Fby; else derived = 4; }
+  else if (ctx->record_alloc) {
+    if (f == "apx") src = p.apx;
+    else if (f == "apy") src = p.apy;
+    else if (f == "Zp") src = p.Zp;
+    else if (f == "hpZ") src = p.hpZ;
+    else if (f == "dZxp") src = p.dZxp;
+    else if (f == "dZyp") src = p.dZyp;
+    else if (f == "Fpx") src = p.Fpx;
+    else if (f == "Fpy") src = p.Fpy;
+    else if (f == "Fric_px") src = p.Frx;
+    else if (f == "Fric_py") src = p.Fry;
+  }
+  if (!src && !isrc && derived < 0)
+    return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown particle field " + f);
+  if (np == 0) return DAMPM_OK;
+  if (isrc || derived >= 0) {
+    // reuse the merge/split scratch as a staging buffer
+    double* tmp = ctx->msb.stage;
+    if (isrc)
+      k_int_to_double<<<grid_for(np, 256), 256, 0, ctx->stream>>>(isrc, tmp, ctx->S);
+    else
+      k_derived<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->P, ctx->S,
+                                                            derived, tmp);
+    CK(cudaGetLastError());
+    src = tmp;
+  }
+  CK(cudaMemcpyAsync(out, src, sizeof(double) * np, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+int dampm_download_nodal(dampm_ctx* ctx, const char* field, double* out) {
+  if (!ctx || !field || !out) return DAMPM_ERR_ARG;
+  const std::string f(field);
+  const double* src = nullptr;
+  Nodes& n = ctx->nodes;
+  if (f == "vvxL") src = n.vvxL;
+  else if (f == "vvyL") src = n.vvyL;
+  else if (f == "Z") src = ctx->Z;
+  else if (f == "dZdx") src = ctx->dZdx;
+  else if (f == "dZdy") src = ctx->dZdy;
+  else if (ctx->record_alloc) {
+    if (f == "Mv") src = n.Mv;
+    else if (f == "mom_vx") src = n.mvx;
+    else if (f == "mom_vy") src = n.mvy;
+    else if (f == "avx") src = n.avx;
+    else if (f == "avy") src = n.avy;
+    else if (f == "vvx") src = n.vvx;
+    else if (f == "vvy") src = n.vvy;
+    else if (f == "FPxv") src = n.FPxv;
+    else if (f == "FPyv") src = n.FPyv;
+    else if (f == "Fric_x") src = n.Fricx;
+    else if (f == "Fric_y") src = n.Fricy;
+    else if (f == "F_int_vx") src = n.Fintx;
+    else if (f == "F_int_vy") src = n.Finty;
+    else if (f == "HV") src = n.HV;
+  }
+  if (!src) return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown nodal field " + f);
+  CK(cudaMemcpyAsync(out, src, sizeof(double) * ctx->nn, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+int dampm_ledgers(dampm_ctx* ctx, double out[9]) {
+  if (!ctx || !out) return DAMPM_ERR_ARG;
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  std::memcpy(out, ctx->Sh->ledger, sizeof(double) * 9);
+  return DAMPM_OK;
+}
+
+int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
+                    const double* Ap, const double* mom_px,
+                    const double* mom_py, const double* Fb_x,
+                    const double* Fb_y) {
+  if (!ctx || !fields || np < 0 || np > ctx->cap) return DAMPM_ERR_ARG;
+  if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
+  Particles& p = ctx->p;
+  double* dst[11] = {p.x, p.y, p.vpx, p.vpy, p.hp, p.F11, p.F12, p.F22,
+                     p.Mp, p.Vp, p.H};
+  const size_t b = sizeof(double) * np;
+  for (int k = 0; k < 11; ++k) {
+    if (!fields[k]) return DAMPM_ERR_ARG;
+    CK(cudaMemcpyAsync(dst[k], fields[k], b, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  const bool fresh = Ap && mom_px && mom_py && Fb_x && Fb_y;
+  if (fresh) {
+    CK(cudaMemcpyAsync(p.Ap, Ap, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.mpx, mom_px, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.mpy, mom_py, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.Fbx, Fb_x, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.Fby, Fb_y, b, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  ctx->Sh->np = int(np);
+  ctx->Sh->fresh = fresh ? 1 : 0;
+  ctx->Sh->red_cur[0] = ctx->Sh->red_cur[1] = ctx->Sh->red_cur[2] = 0ull;
+  CK(cudaMemcpyAsync(ctx->S, ctx->Sh, sizeof(Scalars), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.x, p.y, p.key, ctx->G, ctx->S);
+  k_reduce_state<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->S);
+  CK(cudaGetLastError());
+  return DAMPM_OK;
+}
+
+int dampm_get_state(dampm_ctx* ctx, double* const* fields) {
+  if (!ctx || !fields) return DAMPM_ERR_ARG;
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  Particles& p = ctx->p;
+  const double* src[11] = {p.x, p.y, p.vpx, p.vpy, p.hp, p.F11, p.F12, p.F22,
+                           p.Mp, p.Vp, p.H};
+  const size_t b = sizeof(double) * ctx->Sh->np;
+  for (int k = 0; k < 11; ++k) {
+    if (!fields[k]) return DAMPM_ERR_ARG;
+    CK(cudaMemcpyAsync(fields[k], src[k], b, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+long long dampm_last_launch_count(dampm_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int dampm_last_timings(dampm_ctx* ctx, int enable_events, double out[5]) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (out) {
+    for (int k = 0; k < 5; ++k) out[k] = 0.0;
+    if (ctx->evused > 1) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      for (int k = 1; k < ctx->evused; ++k) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->evpool[k - 1], ctx->evpool[k]));
+        // interval (k-1, k] belongs to the class recorded at event k-1
+        const int cls = ctx->evclass[k - 1];
+        out[cls] += ms;
+        out[4] += ms;
+      }
+    }
+  }
+  ctx->timing = enable_events != 0;
+  return DAMPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,70 @@
+// dampm_kernels.h -- device buffers and kernel entry points of the step.
+#pragma once
+#include <cstddef>
+
+#include "dampm_device.cuh"
+
+namespace dampm {
+
+// P2G tiling: kTR node rows per strip, kLC node columns per chunk, particle
+// records staged in shared memory kCap at a time, 2*kTR threads per CTA.
+constexpr int kTR = 64;
+constexpr int kLC = 8;
+constexpr int kCap = 256;
+constexpr int kP2GThreads = 2 * kTR;
+constexpr int kG2PThreads = 256;
+constexpr int kScanTile = 4096;
+constexpr int kScanThreads = 1024;
+
+// Particle SoA in reference index order (FP64 path).
+struct Particles {
+  // persistent state
+  double *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
+  int *label, *level, *key;
+  // values stored by the reference at the end of a step; read by the next
+  // P2G only when Scalars::fresh is set (after upload or merge/split)
+  double *Ap, *mpx, *mpy, *Fbx, *Fby;
+  // velocity gradients (merge/split input, outputs)
+  double *vpx_dx, *vpx_dy, *vpy_dx, *vpy_dy;
+  // output-only fields (allocated when outputs are recorded)
+  double *apx, *apy, *Zp, *hpZ, *dZxp, *dZyp, *Fpx, *Fpy, *Frx, *Fry;
+  double *xp, *yp;
+};
+
+// Nodal fields, quadgrid node order.
+struct Nodes {
+  double *vvxL, *vvyL;
+  // recorded only on output steps
+  double *Mv, *mvx, *mvy, *avx, *avy, *vvx, *vvy, *FPxv, *FPyv, *Fricx,
+      *Fricy, *Fintx, *Finty, *HV;
+};
+
+__global__ void k_step_begin(Scalars* S, Geom G, Phys P);
+__global__ void k_step_end(Scalars* S);
+__global__ void k_init_particles(Particles p, const double* Z,
+                                 const double* dZdx, const double* dZdy,
+                                 Geom G, Phys P, Scalars* S, int np);
+__global__ void k_keys(const double* x, const double* y, int* key, Geom G,
+                       const Scalars* S);
+__global__ void k_reduce_state(Particles p, Scalars* S);
+__global__ void k_count(const int* key, int* count, int* slot,
+                        const Scalars* S);
+__global__ void k_scan_tiles(const int* count, int n, int* tile_sum,
+                             const Scalars* S);
+__global__ void k_scan_tile_sums(int* tile_sum, int ntiles, const Scalars* S);
+__global__ void k_scan_apply(int* count, int n, const int* tile_sum,
+                             int* start, const Scalars* S);
+__global__ void k_scatter(const int* key, const int* slot, const int* start,
+                          int* perm, const Scalars* S);
+__global__ void k_segment_order(const int* start, int ncells, int* perm,
+                                const Scalars* S);
+__global__ void k_p2g(Particles p, const int* perm, const int* cstart,
+                      const double* Z, Nodes nodes, double* led_part, Geom G,
+                      Phys P, const Scalars* S, int record);
+__global__ void k_ledger_final(const double* led_part, int nparts, Scalars* S);
+__global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
+                      Phys P, Scalars* S, int record, int want_grad);
+
+size_t p2g_smem_bytes();
+
+}  // namespace dampm

@@ -1,0 +1,460 @@
+// ms_kernels.cu -- adaptive merge/split (main/merge_split_ops_cmes.h) as
+// prefix-scan stream compaction on sm_100a.
+//
+//   materialise : Ap/mom/Fb as stored by the reference (when not fresh)
+//   mark        : per particle SPLIT / MERGE_PRIMARY candidates  (:143-168)
+//   split cap   : rank of each split in (cell, index) order, keep < max_ops
+//                 (:179-184)
+//   pairing     : one thread per cell, greedy nearest co-moving partner in
+//                 index order, then undo merges while the cell would drop
+//                 below min_particles_per_cell (:186-248).  When the global
+//                 merge budget could bind, one thread walks all cells in
+//                 order instead (exact n_merge semantics).
+//   scan        : exclusive scan of the weights {1,2,1,0} in index order
+//                 (:268-274)
+//   emit        : split 1->2 along the principal stretch, merge 2->1 at the
+//                 centre of mass (:321-418); copy back; np := Nnew
+#include <cfloat>
+
+#include "dampm_device.cuh"
+#include "ms_kernels.h"
+
+namespace dampm {
+namespace {
+
+constexpr int KEEP = 0, SPLIT = 1, MERGE_PRIMARY = 2, MERGE_SECONDARY = 3;
+
+struct MsCfg {
+  double alpha, beta, split_hp_min, shear_split, hp_min, max_dv;
+  int min_level, max_level, min_ppc;
+  long long max_ops;  // (int)data.ms_max_ops, main/gpu_offload.cpp:317
+  double dt_host;
+  int use_step_dt;
+};
+
+__global__ void k_ms_materialize(Particles p, Phys P, const Scalars* S) {
+  if (!S->active || S->fresh) return;
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    const double hp = p.hp[i];
+    p.Ap[i] = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
+    p.mpx[i] = p.vpx[i] * p.Mp[i];
+    p.mpy[i] = p.vpy[i] * p.Mp[i];
+    double fx, fy;
+    voellmy(P, p.vpx[i], p.vpy[i], hp, fx, fy);
+    p.Fbx[i] = fx;
+    p.Fby[i] = fy;
+  }
+}
+
+__global__ void k_ms_mark(Particles p, Geom G, MsCfg c, int* act, int cap,
+                          Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  const double dt = c.use_step_dt ? S->dt : c.dt_host;
+  const double min_h = (G.hy < G.hx) ? G.hy : G.hx;
+  const double r_split = c.alpha * min_h;
+  const double r_merge = c.beta * min_h;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap;
+       i += gridDim.x * blockDim.x) {
+    int a = KEEP;
+    if (i < np) {
+      const double r_i = sqrt(p.Ap[i]);
+      const double exx = p.vpx_dx[i], eyy = p.vpy_dy[i];
+      const double exy = 0.5 * (p.vpx_dy[i] + p.vpy_dx[i]);
+      const double gdot = sqrt(2.0 * (exx * exx + eyy * eyy + 2.0 * exy * exy));
+      const bool stretched = (r_i > r_split);
+      const bool sheared = (gdot * dt > c.shear_split);
+      const bool thick = (r_i < r_merge);
+      const double hp = p.hp[i];
+      const bool thin_skip = (hp < c.split_hp_min);
+      const int lvl = p.level[i];
+      if ((stretched || sheared) && !thin_skip && (lvl > c.min_level))
+        a = SPLIT;
+      else if (thick && hp > c.hp_min && lvl < c.max_level)
+        a = MERGE_PRIMARY;
+    }
+    act[i] = a;
+  }
+}
+
+// flag[j] = (particle at sorted position j is marked SPLIT)
+__global__ void k_ms_split_flags(const int* perm, const int* act, int* flag,
+                                 int cap, const Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cap;
+       j += gridDim.x * blockDim.x)
+    flag[j] = (j < np && act[perm[j]] == SPLIT) ? 1 : 0;
+}
+
+// rank[j] = number of splits before sorted position j; demote beyond max_ops
+__global__ void k_ms_split_cap(const int* perm, const int* rank, int* act,
+                               MsCfg c, const Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np;
+       j += gridDim.x * blockDim.x) {
+    const int i = perm[j];
+    if (act[i] == SPLIT && (long long)rank[j] >= c.max_ops) act[i] = KEEP;
+  }
+}
+
+// Pairing of one cell, merge_split_ops_cmes.h:186-248.  `budget` is the
+// number of merges still allowed (n_merge < max_ops).  Returns the merges
+// kept after the undo loop.
+__device__ long long pair_cell(int b, int e, const int* perm, int* act,
+                               int* partner, int* paired, const Particles& p,
+                               double max_dv2, int min_ppc, long long budget) {
+  long long n = 0;
+  for (int j = b; j < e; ++j) paired[j] = 0;
+  for (int ji = b; ji < e && n < budget; ++ji) {
+    const int i1 = perm[ji];
+    if (act[i1] != MERGE_PRIMARY || paired[ji]) continue;
+    double best = DBL_MAX;
+    int bj = -1;
+    const double x1 = p.x[i1], y1 = p.y[i1], u1 = p.vpx[i1], v1 = p.vpy[i1];
+    for (int jj = ji + 1; jj < e; ++jj) {
+      const int i2 = perm[jj];
+      if (act[i2] != MERGE_PRIMARY || paired[jj]) continue;
+      const double dx = x1 - p.x[i2];
+      const double dy = y1 - p.y[i2];
+      const double d2 = dx * dx + dy * dy;
+      const double dvx = u1 - p.vpx[i2];
+      const double dvy = v1 - p.vpy[i2];
+      if (d2 < best && (dvx * dvx + dvy * dvy) < max_dv2) {
+        best = d2;
+        bj = jj;
+      }
+    }
+    if (bj >= 0) {
+      act[perm[bj]] = MERGE_SECONDARY;
+      partner[i1] = perm[bj];
+      paired[ji] = 1;
+      paired[bj] = 1;
+      ++n;
+    } else {
+      act[i1] = KEEP;
+    }
+  }
+  // unpaired candidates (also those left when the budget ran out)
+  for (int j = b; j < e; ++j) {
+    const int i = perm[j];
+    if (act[i] == MERGE_PRIMARY && !paired[j]) act[i] = KEEP;
+  }
+  int projected = 0;
+  for (int j = b; j < e; ++j) {
+    const int a = act[perm[j]];
+    projected += (a == KEEP) ? 1 : (a == SPLIT) ? 2 : (a == MERGE_PRIMARY) ? 1 : 0;
+  }
+  while (projected < min_ppc) {
+    bool undone = false;
+    for (int j = b; j < e; ++j) {
+      const int pp = perm[j];
+      if (act[pp] == MERGE_PRIMARY) {
+        const int q = partner[pp];
+        if (q >= 0) act[q] = KEEP;
+        partner[pp] = -1;
+        act[pp] = KEEP;
+        --n;
+        projected += 1;
+        undone = true;
+        break;
+      }
+    }
+    if (!undone) break;
+  }
+  return n;
+}
+
+__global__ void k_ms_count_cand(const int* act, int cap, Scalars* S) {
+  if (!S->active) return;
+  __shared__ long long sm;
+  if (threadIdx.x == 0) sm = 0;
+  __syncthreads();
+  long long c = 0, s = 0;
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    c += (act[i] == MERGE_PRIMARY);
+    s += (act[i] == SPLIT);
+  }
+  atomicAdd((unsigned long long*)&sm, (unsigned long long)c);
+  atomicAdd((unsigned long long*)&S->ms_counts[0], (unsigned long long)s);
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd((unsigned long long*)&S->ms_counts[2], (unsigned long long)sm);
+}
+
+__global__ void k_ms_reset_counts(Scalars* S) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    S->ms_counts[0] = S->ms_counts[1] = S->ms_counts[2] = S->ms_counts[3] = 0;
+  }
+}
+
+// all cells in parallel when the merge budget cannot bind
+__global__ void k_ms_pair_parallel(const int* start, int ncells,
+                                   const int* perm, int* act, int* partner,
+                                   int* paired, Particles p, MsCfg c,
+                                   Scalars* S) {
+  if (!S->active) return;
+  if (S->ms_counts[2] / 2 >= c.max_ops) return;  // budget may bind
+  const double max_dv2 = c.max_dv * c.max_dv;
+  long long local = 0;
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < ncells;
+       cell += gridDim.x * blockDim.x) {
+    const int b = start[cell], e = start[cell + 1];
+    if (e - b < 1) continue;
+    local += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.min_ppc,
+                       0x7fffffffffffffffLL);
+  }
+  if (local) atomicAdd((unsigned long long*)&S->ms_counts[1], (unsigned long long)local);
+}
+
+// one thread, cells in order, exact global n_merge budget
+__global__ void k_ms_pair_serial(const int* start, int ncells, const int* perm,
+                                 int* act, int* partner, int* paired,
+                                 Particles p, MsCfg c, Scalars* S) {
+  if (!S->active) return;
+  if (S->ms_counts[2] / 2 < c.max_ops) return;
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double max_dv2 = c.max_dv * c.max_dv;
+  long long n_merge = 0;
+  for (int cell = 0; cell < ncells; ++cell) {
+    const int b = start[cell], e = start[cell + 1];
+    if (e - b < 1) continue;
+    n_merge += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.min_ppc,
+                         c.max_ops - n_merge);
+  }
+  S->ms_counts[1] = n_merge;
+}
+
+__global__ void k_ms_weights(const int* act, int* w, int* partner, int cap,
+                             const Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap;
+       i += gridDim.x * blockDim.x) {
+    int v = 0;
+    if (i < np) {
+      const int a = act[i];
+      v = (a == KEEP) ? 1 : (a == SPLIT) ? 2 : (a == MERGE_PRIMARY) ? 1 : 0;
+    }
+    w[i] = v;
+  }
+}
+
+__global__ void k_ms_init_partner(int* partner, int cap, const Scalars* S) {
+  if (!S->active) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap;
+       i += gridDim.x * blockDim.x)
+    partner[i] = -1;
+}
+
+struct Fields {
+  double* f[kMsFields];
+  int* label;
+  int* level;
+};
+
+// field slots: 0 x, 1 y, 2 vpx, 3 vpy, 4 hp, 5 F11, 6 F12, 7 F22, 8 Mp,
+// 9 Vp, 10 H, 11 Ap, 12 mpx, 13 mpy, 14 Fbx, 15 Fby, 16 vpx_dx, 17 vpx_dy,
+// 18 vpy_dx, 19 vpy_dy, 20 xp, 21 yp
+__device__ __forceinline__ bool extensive(int k) {
+  return k == 8 || k == 9 || k == 11 || k == 12 || k == 13;
+}
+
+__global__ void k_ms_emit(Fields in, Fields out, const int* act,
+                          const int* partner, const int* offs, Geom G,
+                          long long cap, Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  const int nnew = offs[cap];
+  if (nnew > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
+    return;
+  }
+  const double eps = 1e-10;
+  const double Lx = G.ncols * G.hx, Ly = G.nrows * G.hy;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    const int a = act[i];
+    const int o = offs[i];
+    if (a == KEEP) {
+#pragma unroll
+      for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
+      out.label[o] = in.label[i];
+      out.level[o] = in.level[i];
+    } else if (a == SPLIT) {
+      const int o2 = o + 1;
+      const int level = in.level[i];
+      // principal_stretch_dir (merge_split_ops_cmes.h:93-110)
+      const double exx = in.f[16][i], eyy = in.f[19][i];
+      const double exy = 0.5 * (in.f[17][i] + in.f[18][i]);
+      const double tr = exx + eyy;
+      const double diff = 0.5 * (exx - eyy);
+      const double disc = sqrt(diff * diff + exy * exy);
+      const double l1 = 0.5 * tr + disc;
+      const double vx = l1 - eyy, vy = exy;
+      const double nrm = sqrt(vx * vx + vy * vy);
+      double ux = 1.0, uy = 0.0;
+      if (!(nrm < 1e-12)) {
+        ux = vx / nrm;
+        uy = vy / nrm;
+      }
+      const double r_i = sqrt(in.f[11][i]);
+      const double off = 0.25 * r_i;
+      const double cx = in.f[0][i], cy = in.f[1][i];
+      auto clampx = [&](double v) { return v < eps ? eps : (v > Lx - eps ? Lx - eps : v); };
+      auto clampy = [&](double v) { return v < eps ? eps : (v > Ly - eps ? Ly - eps : v); };
+      const double nx1 = clampx(cx + off * ux), ny1 = clampy(cy + off * uy);
+      const double nx2 = clampx(cx - off * ux), ny2 = clampy(cy - off * uy);
+#pragma unroll
+      for (int k = 0; k < kMsFields; ++k) {
+        const double val = in.f[k][i] / (extensive(k) ? 2.0 : 1.0);
+        out.f[k][o] = val;
+        out.f[k][o2] = val;
+      }
+      const double h = out.f[4][o];
+      out.f[11][o] = out.f[9][o] / h;
+      out.f[11][o2] = out.f[9][o2] / h;
+      out.f[0][o] = nx1; out.f[1][o] = ny1;
+      out.f[0][o2] = nx2; out.f[1][o2] = ny2;
+      out.f[20][o] = nx1; out.f[21][o] = ny1;
+      out.f[20][o2] = nx2; out.f[21][o2] = ny2;
+      out.f[12][o] = out.f[8][o] * out.f[2][o];
+      out.f[12][o2] = out.f[8][o2] * out.f[2][o2];
+      out.f[13][o] = out.f[8][o] * out.f[3][o];
+      out.f[13][o2] = out.f[8][o2] * out.f[3][o2];
+      out.level[o] = level - 1;
+      out.level[o2] = level - 1;
+      out.label[o] = -1;
+      out.label[o2] = -1;
+    } else if (a == MERGE_PRIMARY) {
+      const int j = partner[i];
+      const int level = in.level[i];
+      const double M1 = in.f[8][i], M2 = in.f[8][j];
+      const double Mt = M1 + M2;
+      const double nx = (M1 * in.f[0][i] + M2 * in.f[0][j]) / Mt;
+      const double ny = (M1 * in.f[1][i] + M2 * in.f[1][j]) / Mt;
+#pragma unroll
+      for (int k = 0; k < kMsFields; ++k)
+        out.f[k][o] = extensive(k) ? (in.f[k][i] + in.f[k][j])
+                                   : (M1 * in.f[k][i] + M2 * in.f[k][j]) / Mt;
+      out.f[4][o] = out.f[9][o] / out.f[11][o];  // hp = Vp / Ap
+      out.f[0][o] = nx;
+      out.f[1][o] = ny;
+      out.f[20][o] = nx;
+      out.f[21][o] = ny;
+      out.f[12][o] = out.f[8][o] * out.f[2][o];
+      out.f[13][o] = out.f[8][o] * out.f[3][o];
+      out.level[o] = level + 1;
+      out.label[o] = -1;
+    }
+  }
+}
+
+__global__ void k_ms_copy_back(Fields from, Fields to, const int* offs,
+                               long long cap, Scalars* S) {
+  if (!S->active) return;
+  const int nnew = offs[cap];
+  if (nnew > cap) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnew;
+       i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < kMsFields; ++k) to.f[k][i] = from.f[k][i];
+    to.label[i] = from.label[i];
+    to.level[i] = from.level[i];
+  }
+}
+
+__global__ void k_ms_finish(const int* offs, long long cap, Scalars* S) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (!S->active) return;
+  const int nnew = offs[cap];
+  S->ms_counts[2] = S->np;
+  if (nnew > cap) {
+    S->ms_counts[3] = S->np;
+    return;
+  }
+  S->np = nnew;
+  S->ms_counts[3] = nnew;
+  S->fresh = 1;
+}
+
+int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return int(b);
+}
+
+// exclusive scan of a[0..n) -> out[0..n] (a is zeroed), n = cap
+int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
+                 const Scalars* S, cudaStream_t st) {
+  k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, S);
+  k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(tile_sum, ntiles, S);
+  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, S);
+  return 3;
+}
+
+}  // namespace
+
+int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
+               int ncells, Geom G, Phys P, const dampm_ms_params& cfg,
+               Scalars* S, long long cap, cudaStream_t st, int use_step_dt,
+               double dt) {
+  MsCfg c{};
+  c.alpha = cfg.alpha;
+  c.beta = cfg.beta;
+  c.split_hp_min = cfg.split_hp_min;
+  c.shear_split = cfg.shear_split;
+  c.hp_min = cfg.hp_min;
+  c.max_dv = cfg.max_dv;
+  c.min_level = cfg.min_level;
+  c.max_level = cfg.max_level;
+  c.min_ppc = cfg.min_particles_per_cell;
+  c.max_ops = (long long)(int)cfg.max_ops;
+  c.dt_host = dt;
+  c.use_step_dt = use_step_dt;
+  int n = 0;
+  const int gp = grid_for(cap, 256);
+  const int ic = int(cap);
+  k_ms_reset_counts<<<1, 1, 0, st>>>(S);
+  k_ms_materialize<<<gp, 256, 0, st>>>(p, P, S);
+  n += 2;
+  k_ms_mark<<<gp, 256, 0, st>>>(p, G, c, m.act, ic, S);
+  k_ms_init_partner<<<gp, 256, 0, st>>>(m.partner, ic, S);
+  k_ms_split_flags<<<gp, 256, 0, st>>>(perm, m.act, m.flag, ic, S);
+  n += 3;
+  n += scan_enqueue(m.flag, m.rank, ic, m.tile_sum, m.ntiles, S, st);
+  k_ms_split_cap<<<gp, 256, 0, st>>>(perm, m.rank, m.act, c, S);
+  k_ms_count_cand<<<gp, 256, 0, st>>>(m.act, ic, S);
+  k_ms_pair_parallel<<<grid_for(ncells, 128), 128, 0, st>>>(
+      start, ncells, perm, m.act, m.partner, m.paired, p, c, S);
+  k_ms_pair_serial<<<1, 1, 0, st>>>(start, ncells, perm, m.act, m.partner,
+                                    m.paired, p, c, S);
+  k_ms_weights<<<gp, 256, 0, st>>>(m.act, m.w, m.partner, ic, S);
+  n += 5;
+  n += scan_enqueue(m.w, m.offs, ic, m.tile_sum, m.ntiles, S, st);
+  Fields in{}, out{};
+  double* pf[kMsFields] = {p.x,   p.y,   p.vpx, p.vpy, p.hp,     p.F11,
+                           p.F12, p.F22, p.Mp,  p.Vp,  p.H,      p.Ap,
+                           p.mpx, p.mpy, p.Fbx, p.Fby, p.vpx_dx, p.vpx_dy,
+                           p.vpy_dx, p.vpy_dy, p.xp, p.yp};
+  for (int k = 0; k < kMsFields; ++k) {
+    in.f[k] = pf[k];
+    out.f[k] = m.sd[k];
+  }
+  in.label = p.label;
+  in.level = p.level;
+  out.label = m.slabel;
+  out.level = m.slevel;
+  k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
+  k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
+  k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
+  n += 3;
+  return n;
+}
+
+}  // namespace dampm

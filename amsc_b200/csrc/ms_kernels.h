@@ -1,0 +1,53 @@
+// ms_kernels.h -- adaptive merge/split on the device
+// (main/merge_split_ops_cmes.h:116-447).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/dampm_cuda.h"
+#include "dampm_kernels.h"
+
+namespace dampm {
+
+// particle fields carried through a merge/split emit (doubles)
+constexpr int kMsFields = 22;
+
+struct MsBuffers {
+  int *act = nullptr, *partner = nullptr, *w = nullptr, *offs = nullptr;
+  int *flag = nullptr, *rank = nullptr, *paired = nullptr, *tile_sum = nullptr;
+  int ntiles = 0;
+  long long cap = 0;
+  double* stage = nullptr;  // one field of scratch (also a download staging area)
+  double* sd[kMsFields] = {};
+  int *slabel = nullptr, *slevel = nullptr;
+};
+
+template <class Alloc>
+int ms_alloc(MsBuffers& m, long long cap, int /*ncells*/, Alloc alloc) {
+  m.cap = cap;
+  m.ntiles = int((cap + kScanTile - 1) / kScanTile);
+  int** ints[] = {&m.act, &m.partner, &m.w, &m.offs, &m.flag, &m.rank,
+                        &m.paired, &m.slabel, &m.slevel};
+  for (int** q : ints) {
+    int rc = alloc((void**)q, sizeof(int) * size_t(cap + 1));
+    if (rc) return rc;
+  }
+  int rc = alloc((void**)&m.tile_sum, sizeof(int) * size_t(m.ntiles + 1));
+  if (rc) return rc;
+  rc = alloc((void**)&m.stage, sizeof(double) * size_t(cap));
+  if (rc) return rc;
+  for (int k = 0; k < kMsFields; ++k) {
+    rc = alloc((void**)&m.sd[k], sizeof(double) * size_t(cap));
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+// Enqueues one adaptive_merge_split on the current binning (start/perm must
+// describe the current positions).  dt comes from the step's device scalar
+// when use_step_dt, else `dt`.  Returns the number of kernel launches.
+int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
+               int ncells, Geom G, Phys P, const dampm_ms_params& cfg,
+               Scalars* S, long long cap, cudaStream_t stream, int use_step_dt,
+               double dt);
+
+}  // namespace dampm

@@ -1,0 +1,137 @@
+"""DATA: the solver input of dampm, mirroring ``struct DATA``.
+
+Reference: main/mpm_data.h:6-122.  Required keys are read with ``j.at`` and
+raise when missing (:64-97); optional keys fall back to the defaults of
+:99-112.  DATA.json files hold only numbers and flat number arrays, written
+with ``%.17g`` by the scenario generators (data/dambreak/dambreak.m:146-165),
+so a round trip through :func:`to_json` / :func:`from_json` is exact.
+
+Node arrays (Z, dZdx, dZdy) are in quadgrid order: node (r, c) at
+r + c*(Ney+1), i.e. Octave's column-major ``Z(:)`` of a meshgrid with y
+varying fastest.
+"""
+from __future__ import annotations
+
+import json
+from dataclasses import dataclass, field, fields
+from typing import Dict
+
+import numpy as np
+
+PARTICLE_KEYS = ("x", "y", "Mp", "Ap", "vpx", "vpy", "hp", "mom_px", "mom_py", "Vp")
+NODE_KEYS = ("Z", "dZdx", "dZdy")
+# required scalar keys (main/mpm_data.h:70-97) and their types
+REQUIRED_SCALARS = {
+    "Nex": int, "Ney": int, "hx": float, "hy": float, "rho": float, "g": float,
+    "T": float, "xi": float, "mu": float, "phi": float, "tauy": float,
+    "BINGHAM_ON": float, "FRICTION_ON": float, "CFL": float, "BC_FLAG": int,
+    "MERGE_SPLIT_ON": int, "eq_level": float,
+}
+# optional keys and defaults (main/mpm_data.h:99-112)
+OPTIONAL_DEFAULTS = {
+    "DT_FIXED": 0.0, "NSTEPS": 0,
+    "ms_alpha": 0.9, "ms_beta": 0.30, "ms_split_hp_min": 0.0,
+    "ms_shear_split": 1e30, "ms_hp_min": 0.05, "ms_max_dv": 0.01,
+    "ms_min_level": -2, "ms_max_level": 2, "ms_min_particles_per_cell": 2,
+    "ms_call_interval": 10, "ms_max_ops": 1e9,
+}
+_INT_KEYS = {"Nex", "Ney", "BC_FLAG", "MERGE_SPLIT_ON", "NSTEPS", "ms_min_level",
+             "ms_max_level", "ms_min_particles_per_cell", "ms_call_interval"}
+
+
+class DataError(KeyError):
+    pass
+
+
+@dataclass
+class DATA:
+    """Flat scenario description; arrays are float64 numpy arrays."""
+
+    arrays: Dict[str, np.ndarray] = field(default_factory=dict)
+    scalars: Dict[str, float] = field(default_factory=dict)
+
+    # -- convenience accessors ------------------------------------------------
+    def __getattr__(self, name):
+        if name in ("arrays", "scalars"):
+            raise AttributeError(name)
+        a = self.__dict__.get("arrays", {})
+        s = self.__dict__.get("scalars", {})
+        if name in a:
+            return a[name]
+        if name in s:
+            return s[name]
+        raise AttributeError(name)
+
+    @property
+    def np(self) -> int:
+        return int(self.arrays["x"].shape[0])
+
+    @property
+    def nnodes(self) -> int:
+        return (int(self.scalars["Nex"]) + 1) * (int(self.scalars["Ney"]) + 1)
+
+    def copy(self) -> "DATA":
+        return DATA({k: v.copy() for k, v in self.arrays.items()}, dict(self.scalars))
+
+    def validate(self) -> None:
+        for k in PARTICLE_KEYS:
+            if k not in self.arrays:
+                raise DataError(f"DATA: missing key '{k}'")
+        for k in NODE_KEYS:
+            if k not in self.arrays:
+                raise DataError(f"DATA: missing key '{k}'")
+        for k in REQUIRED_SCALARS:
+            if k not in self.scalars:
+                raise DataError(f"DATA: missing key '{k}'")
+        n = self.np
+        for k in PARTICLE_KEYS:
+            if self.arrays[k].shape != (n,):
+                raise DataError(f"DATA: '{k}' has {self.arrays[k].shape[0]} values, expected {n}")
+        nn = self.nnodes
+        for k in NODE_KEYS:
+            if self.arrays[k].shape != (nn,):
+                raise DataError(f"DATA: '{k}' has {self.arrays[k].shape[0]} values, expected {nn}")
+
+
+def from_dict(j: dict) -> DATA:
+    """``from_json`` of main/mpm_data.h:61-114."""
+    arrays, scalars = {}, {}
+    for k in PARTICLE_KEYS + NODE_KEYS:
+        if k not in j:
+            raise DataError(f"DATA: missing key '{k}'")
+        arrays[k] = np.ascontiguousarray(np.asarray(j[k], dtype=np.float64).reshape(-1))
+    for k, typ in REQUIRED_SCALARS.items():
+        if k not in j:
+            raise DataError(f"DATA: missing key '{k}'")
+        scalars[k] = int(j[k]) if typ is int else float(j[k])
+    for k, dflt in OPTIONAL_DEFAULTS.items():
+        v = j.get(k, dflt)
+        scalars[k] = int(v) if k in _INT_KEYS else float(v)
+    d = DATA(arrays, scalars)
+    d.validate()
+    return d
+
+
+def from_json(path: str) -> DATA:
+    """``DATA::DATA(const char*)`` (main/mpm_data.h:116-122)."""
+    with open(path, "r") as f:
+        return from_dict(json.load(f))
+
+
+def _fmt(v) -> str:
+    return "%.17g" % float(v)
+
+
+def to_json(d: DATA, path: str) -> None:
+    """Writes DATA.json the way the Octave generators' ``v2j`` does."""
+    d.validate()
+    with open(path, "w") as f:
+        f.write("{\n")
+        items = []
+        for k in PARTICLE_KEYS + NODE_KEYS:
+            a = d.arrays[k]
+            items.append('"%s": [%s]' % (k, ",".join(_fmt(v) for v in a.tolist())))
+        for k, v in d.scalars.items():
+            items.append('"%s": %s' % (k, str(int(v)) if k in _INT_KEYS else _fmt(v)))
+        f.write(",\n".join(items))
+        f.write("\n}\n")

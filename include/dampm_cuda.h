@@ -1,0 +1,187 @@
+/*
+ * dampm_cuda.h -- C ABI of the B200 (sm_100a) depth-averaged MPM time step.
+ *
+ * Drop-in boundary for the step loop of dampm (lucadiprofio/AMSC).  It
+ * replaces, in the reference project:
+ *   - the 17 `gpu_kernels::` free functions (main/gpu_kernels.h:7-196) that
+ *     main/gpu_offload.cpp:410-540 launches once per step;
+ *   - the per-step host binning `particles_t::init_particle_mesh` and its
+ *     PCIe round trip (main/gpu_offload.cpp:546-558);
+ *   - the host CFL reduction (main/gpu_offload.cpp:285-300,
+ *     main/optim_par.cpp:285-308);
+ *   - the host merge/split `adaptive_merge_split` (main/merge_split_ops_cmes.h
+ *     :432-447, called from main/gpu_offload.cpp:321-401);
+ *   - the loop body of main/optim_par.cpp:281-668 (whose numbers the FP64
+ *     path reproduces).
+ *
+ * Conventions
+ *   - Plain C types only; host pointers are host memory, never retained.
+ *   - Every function returns 0 (DAMPM_OK) or a negative dampm_status code;
+ *     dampm_last_error() gives a one-line message.  Device-side problems
+ *     (non-finite depth, particle capacity exceeded) are reported through a
+ *     device status word read by dampm_sync()/dampm_status(); kernels never
+ *     trap.
+ *   - A context owns all of its device memory and is used from one host
+ *     thread at a time.  Work is enqueued on the stream given at creation
+ *     (NULL = a stream the context creates).
+ *   - Node arrays are in quadgrid order: node (r, c) at r + c*(Ney+1)
+ *     (main/gpu_kernels.cpp:7-16); the cell of (r, c) is r + c*Ney.
+ *   - Particle arrays passed in and out are in the reference's particle
+ *     index order (DATA order, then the compacted order that merge/split
+ *     produces, main/merge_split_ops_cmes.h:268-274).
+ */
+#ifndef DAMPM_CUDA_H
+#define DAMPM_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dampm_status {
+  DAMPM_OK = 0,
+  DAMPM_ERR_ARG = -1,      /* bad argument (null pointer, bad size, ...)   */
+  DAMPM_ERR_CUDA = -2,     /* CUDA runtime error                           */
+  DAMPM_ERR_STATE = -3,    /* call out of order (e.g. step before upload)  */
+  DAMPM_ERR_CAPACITY = -4, /* particle capacity exceeded (merge/split)     */
+  DAMPM_ERR_DEVICE = -5,   /* device status word flagged a problem         */
+  DAMPM_ERR_UNKNOWN_FIELD = -6
+};
+
+/* Grid of main/mpm_data.h:14-17 (grid.set_sizes(Ney, Nex, hx, hy),
+ * main/optim_par.cpp:136). */
+typedef struct {
+  int Nex;
+  int Ney;
+  double hx;
+  double hy;
+} dampm_grid;
+
+/* Scalar physics/run parameters of struct DATA (main/mpm_data.h:21-44). */
+typedef struct {
+  double g, T, rho, xi, mu, phi, tauy;
+  double BINGHAM_ON, FRICTION_ON, CFL;
+  int BC_FLAG;
+  int MERGE_SPLIT_ON;
+  double eq_level;
+  double DT_FIXED; /* > 0: fixed dt for NSTEPS steps; else CFL until T     */
+  int NSTEPS;
+} dampm_params;
+
+/* ms_* parameters (main/mpm_data.h:46-56 defaults at :102-112; used as
+ * ms_config, main/merge_split_ops_cmes.h:14-37, main/gpu_offload.cpp:308-319).
+ */
+typedef struct {
+  double alpha, beta, split_hp_min, shear_split, hp_min, max_dv;
+  int min_level, max_level, min_particles_per_cell, call_interval;
+  double max_ops;
+} dampm_ms_params;
+
+typedef struct dampm_ctx dampm_ctx;
+
+/* Precision of particle storage and arithmetic. */
+enum dampm_precision { DAMPM_FP64 = 0, DAMPM_FP32 = 1 };
+
+/* Creates a context for one scenario.  `capacity` is the largest particle
+ * count the context may hold (merge/split may grow it); 0 = chosen at upload
+ * (2x the uploaded count).  Replaces the `target data` region set-up of
+ * main/gpu_offload.cpp:258-271. */
+int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
+                     const dampm_ms_params* ms, int precision,
+                     long long capacity, void* cuda_stream, dampm_ctx** out);
+
+int dampm_ctx_destroy(dampm_ctx* ctx);
+
+/* Terrain on the nodes, quadgrid node order, (Nex+1)*(Ney+1) values each.
+ * Replaces vars["Z"/"dZdx"/"dZdy"] = data.* (main/optim_par.cpp:235-237). */
+int dampm_upload_terrain(dampm_ctx* ctx, const double* Z, const double* dZdx,
+                         const double* dZdy);
+
+/* Particles in DATA order, then the initialisation of
+ * main/optim_par.cpp:147-264 on the device (Zp, H, hpZ, initial stress,
+ * label = index, level = 0).  Resets it = 0, t = 0. */
+int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
+                           const double* y, const double* Mp, const double* Ap,
+                           const double* vpx, const double* vpy,
+                           const double* hp, const double* mom_px,
+                           const double* mom_py, const double* Vp);
+
+/* Enqueues `nsteps` passes of the loop body (dt, it++, merge/split at the
+ * gpu_offload cadence when MERGE_SPLIT_ON and enabled, sort, P2G + nodal
+ * update, G2P + rheology, t += dt).  A pass whose loop condition
+ * (fixed ? it < NSTEPS : t < T) fails on the device does nothing, so this
+ * never overshoots.  Asynchronous: returns once the work is enqueued. */
+int dampm_step(dampm_ctx* ctx, int nsteps);
+
+/* Runs until the loop condition fails (or max_steps passes), synchronising
+ * every `chunk` steps.  *steps_done (may be NULL) receives the count. */
+int dampm_run(dampm_ctx* ctx, long long max_steps, int chunk,
+              long long* steps_done);
+
+/* Waits for the stream and checks the device status word. */
+int dampm_sync(dampm_ctx* ctx);
+
+/* Loop state: iteration, time, last dt, particle count (synchronises). */
+int dampm_status(dampm_ctx* ctx, int* it, double* t, double* dt_last,
+                 long long* np);
+
+/* Enables merge/split at the gpu_offload cadence (main/gpu_offload.cpp:321)
+ * when MERGE_SPLIT_ON != 0.  Off by default: main/optim_par.cpp reads the
+ * flag but never splits or merges. */
+int dampm_enable_merge_split(dampm_ctx* ctx, int enable);
+
+/* One standalone adaptive_merge_split(dt) on the current state
+ * (main/merge_split_ops_cmes.h:432-447).  counts (may be NULL) receives
+ * {splits, merges, np_before, np_after}. */
+int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]);
+
+/* Copies one particle field to host memory in reference index order.
+ * Names: x, y, Mp, Vp, H, hp, vpx, vpy, F_11, F_12, F_21, F_22, Ap, mom_px,
+ * mom_py, Fb_x, Fb_y, label, level (as double), and, after a step run with
+ * dampm_record_outputs(ctx, 1): vpx_dx, vpx_dy, vpy_dx, vpy_dy, apx, apy, Zp,
+ * hpZ, dZxp, dZyp, Fpx, Fpy, Fric_px, Fric_py, vpxL, vpyL, xp, yp.
+ * `out` must hold the current particle count. */
+int dampm_download(dampm_ctx* ctx, const char* field, double* out);
+
+/* Copies one nodal field ((Nex+1)*(Ney+1) values) of the last step:
+ * vvxL, vvyL always; Mv, mom_vx, mom_vy, avx, avy, vvx, vvy, Ftot_vx,
+ * Ftot_vy, F_ext_vx, F_ext_vy, F_int_vx, F_int_vy, FPxv, FPyv, Fric_x,
+ * Fric_y, HV after a step run with dampm_record_outputs(ctx, 1); Z, dZdx,
+ * dZdy always. */
+int dampm_download_nodal(dampm_ctx* ctx, const char* field, double* out);
+
+/* When on, the following steps also materialise the output-only and
+ * intermediate fields listed above (the nc_particles / nc_grid columns). */
+int dampm_record_outputs(dampm_ctx* ctx, int enable);
+
+/* Conservation ledger of the last step (main/optim_par.cpp:395-425):
+ * {sum Mp, sum mom_px, sum mom_py, sum Mv, sum mom_vx, sum mom_vy,
+ *  err_mass, err_mom, t}. */
+int dampm_ledgers(dampm_ctx* ctx, double out[9]);
+
+/* Overwrites / reads the whole persistent particle state (checkpoint and
+ * host round trip).  Arrays in reference index order, np values each:
+ * x, y, vpx, vpy, hp, F_11, F_12, F_22, Mp, Vp, H.  set_state marks the
+ * next step as reading Ap/mom/Fb from the supplied fresh arrays when they
+ * are non-NULL, else recomputing them as the step does. */
+int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
+                    const double* Ap, const double* mom_px,
+                    const double* mom_py, const double* Fb_x,
+                    const double* Fb_y);
+int dampm_get_state(dampm_ctx* ctx, double* const* fields);
+
+/* Number of this library's kernel launches enqueued by the last dampm_step
+ * call (for launch accounting). */
+long long dampm_last_launch_count(dampm_ctx* ctx);
+
+/* Wall time of the kernels of the last dampm_step call, measured with CUDA
+ * events on the context stream (ms, synchronises); per kernel class:
+ * out[0] sort, out[1] p2g, out[2] g2p, out[3] other, out[4] total. */
+int dampm_last_timings(dampm_ctx* ctx, int enable_events, double out[5]);
+
+const char* dampm_last_error(dampm_ctx* ctx);
+const char* dampm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DAMPM_CUDA_H */
