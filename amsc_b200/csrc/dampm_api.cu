@@ -34,6 +34,9 @@ struct dampm_ctx {
   int ntiles = 0;
   double* led_part = nullptr;
   int n_led = 0;
+  int strips = 0, chunks = 0;
+  int *ulist = nullptr, *ucount = nullptr;
+  int p2g_grid = 0;
   Scalars* S = nullptr;
   Scalars* Sh = nullptr;  // pinned host mirror
   MsBuffers msb{};
@@ -193,10 +196,21 @@ int enqueue_pass(dampm_ctx* ctx) {
   ev_mark(ctx, 0);
   enqueue_sort(ctx);
   ev_mark(ctx, 1);
-  dim3 pg((ctx->grid.Ney + 1 + kTR - 1) / kTR, (ctx->grid.Nex + 1 + kLC - 1) / kLC);
-  k_p2g<<<pg, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
+  k_units_reset<<<1, 1, 0, ctx->stream>>>(ctx->ucount, ctx->S);
+  k_units<<<grid_for((long long)ctx->strips * ctx->chunks, 256), 256, 0, ctx->stream>>>(
+      ctx->start, ctx->strips, ctx->chunks, ctx->ulist, ctx->ucount, ctx->led_part,
+      ctx->G, ctx->S);
+  if (ctx->record) {
+    Nodes& n = ctx->nodes;
+    double* nf[] = {n.vvxL, n.vvyL, n.Mv,  n.mvx,  n.mvy,   n.avx,   n.avy, n.vvx,
+                    n.vvy,  n.FPxv, n.FPyv, n.Fricx, n.Fricy, n.Fintx, n.Finty};
+    for (double* q : nf)
+      cudaMemsetAsync(q, 0, sizeof(double) * ctx->nn, ctx->stream);
+  }
+  k_p2g<<<ctx->p2g_grid, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
       ctx->p, ctx->perm, ctx->start, ctx->Z, ctx->nodes, ctx->led_part, ctx->G,
-      ctx->P, ctx->S, ctx->record ? 1 : 0);
+      ctx->P, ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount, ctx->strips);
+  ctx->launches += 2;
   ev_mark(ctx, 3);
   k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->n_led, ctx->S);
   ev_mark(ctx, 2);
@@ -306,6 +320,11 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   ctx->G.hy = grid->hy;
   ctx->G.Lx = grid->Nex * grid->hx;
   ctx->G.Ly = grid->Ney * grid->hy;
+  {
+    int e;
+    ctx->G.hx_pow2 = std::frexp(grid->hx, &e) == 0.5 ? 1 : 0;
+    ctx->G.hy_pow2 = std::frexp(grid->hy, &e) == 0.5 ? 1 : 0;
+  }
   ctx->P = make_phys(*params);
   ctx->nn = int(nn);
   ctx->nc = grid->Nex * grid->Ney;
@@ -329,11 +348,12 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   rc = rc ? rc : dalloc(ctx, &ctx->count, ctx->nc);
   rc = rc ? rc : dalloc(ctx, &ctx->start, size_t(ctx->nc) + 1);
   rc = rc ? rc : dalloc(ctx, &ctx->tile_sum, size_t(ctx->ntiles) + 1);
-  const int strips = (grid->Ney + 1 + kTR - 1) / kTR;
-  const int chunks = (grid->Nex + 1 + kLC - 1) / kLC;
-  if (chunks > 65535) rc = rc ? rc : fail(ctx, DAMPM_ERR_ARG, "grid too wide");
-  ctx->n_led = strips * chunks;
+  ctx->strips = (grid->Ney + 1 + kTR - 1) / kTR;
+  ctx->chunks = (grid->Nex + 1 + kLC - 1) / kLC;
+  ctx->n_led = ctx->strips * ctx->chunks;
   rc = rc ? rc : dalloc(ctx, &ctx->led_part, size_t(ctx->n_led) * 6);
+  rc = rc ? rc : dalloc(ctx, &ctx->ulist, size_t(ctx->n_led));
+  rc = rc ? rc : dalloc(ctx, &ctx->ucount, 1);
   rc = rc ? rc : dalloc(ctx, &ctx->S, 1);
   if (rc == DAMPM_OK) {
     if (cudaMallocHost(&ctx->Sh, sizeof(Scalars)) != cudaSuccess) rc = DAMPM_ERR_CUDA;
@@ -347,6 +367,12 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
     if (cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smem)) != cudaSuccess)
       rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+    int per_sm = 0, nsm = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g, kP2GThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    ctx->p2g_grid = std::max(1, std::min(nsm * per_sm, ctx->n_led));
   }
   if (rc != DAMPM_OK) {
     dampm_ctx_destroy(ctx);

@@ -17,6 +17,7 @@ struct Geom {
   int ncols;   // Nex
   double hx, hy;
   double Lx, Ly;  // Nex*hx, Ney*hy (main/optim_par.cpp:557-558)
+  int hx_pow2, hy_pow2;  // h is a power of two: v/h == v*(1/h) exactly
 };
 
 // Scalars of struct DATA used inside the step (main/mpm_data.h:21-44).
@@ -88,6 +89,17 @@ __device__ __forceinline__ void local_xy(double x, double y, int c, int r,
                                          double& eta) {
   xi = (x - c * hx) / hx;
   eta = (y - r * hy) / hy;
+}
+
+// Same values as local_xy; when h is a power of two the quotient by h equals
+// the product with 1/h exactly, and the division is skipped.
+__device__ __forceinline__ void local_xy_g(double x, double y, int c, int r,
+                                           const Geom& G, double ihx,
+                                           double ihy, double& xi,
+                                           double& eta) {
+  const double dx = x - c * G.hx, dy = y - r * G.hy;
+  xi = G.hx_pow2 ? dx * ihx : dx / G.hx;
+  eta = G.hy_pow2 ? dy * ihy : dy / G.hy;
 }
 
 // shp (main/gpu_kernels.cpp:33-41)

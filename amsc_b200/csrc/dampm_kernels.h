@@ -6,12 +6,14 @@
 
 namespace dampm {
 
-// P2G tiling: kTR node rows per strip, kLC node columns per chunk, particle
-// records staged in shared memory kCap at a time, 2*kTR threads per CTA.
-constexpr int kTR = 64;
-constexpr int kLC = 8;
-constexpr int kCap = 256;
-constexpr int kP2GThreads = 2 * kTR;
+// P2G tiling: kTR node rows per strip (one lane per row in each of the four
+// quantity-group warps), kLC node
+// columns per chunk, particle records staged in shared memory kCap at a time.
+constexpr int kTR = 32;
+constexpr int kLC = 16;
+constexpr int kP2GThreads = 128;
+constexpr int kCap = 544;
+constexpr int kP2GMinBlocks = 2;
 constexpr int kG2PThreads = 256;
 constexpr int kScanTile = 4096;
 constexpr int kScanThreads = 1024;
@@ -58,9 +60,13 @@ __global__ void k_scatter(const int* key, const int* slot, const int* start,
                           int* perm, const Scalars* S);
 __global__ void k_segment_order(const int* start, int ncells, int* perm,
                                 const Scalars* S);
+__global__ void k_units(const int* cstart, int strips, int chunks, int* ulist,
+                        int* ucount, double* led_part, Geom G, const Scalars* S);
+__global__ void k_units_reset(int* ucount, const Scalars* S);
 __global__ void k_p2g(Particles p, const int* perm, const int* cstart,
                       const double* Z, Nodes nodes, double* led_part, Geom G,
-                      Phys P, const Scalars* S, int record);
+                      Phys P, const Scalars* S, int record, const int* ulist,
+                      const int* ucount, int strips);
 __global__ void k_ledger_final(const double* led_part, int nparts, Scalars* S);
 __global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
                       Phys P, Scalars* S, int record, int want_grad);

@@ -313,254 +313,454 @@ __global__ void k_segment_order(const int* __restrict__ start, int ncells,
 // ---------------------------------------------------------------------------
 // P2G + NODAL
 //
-// A CTA owns the node rows [r0, r0+kTR) of one strip and the node columns
-// [cA, cB) of one chunk.  It walks the cell columns cA-1 .. cB-1.  For cell
-// column cc the particles of cells (rlo..rhi, cc) are one contiguous range of
-// the sorted order; records are computed once per particle into shared memory
-// in batches of kCap.  Thread (row r, side):
-//   side 0 finishes node (r, cc): it carries the chain over cells
-//          (r-1, cc-1), (r, cc-1) handed over from the previous column and
-//          adds cells (r-1, cc) [local node 1] then (r, cc) [local node 0];
-//   side 1 starts node (r, cc+1) with cells (r-1, cc) [local node 3] then
-//          (r, cc) [local node 2].
-// These are exactly the node's contributions in quadgrid's cell-sweep order,
-// so every nodal sum is the reference's sequential sum, bit for bit.
+// Work unit: node rows [r0, r0+kTR) of one strip x node columns [cA, cB) of
+// one chunk; the unit walks the cell columns cA-1 .. cB-1.  For cell column cc
+// the particles of cells (rlo..rhi, cc) are one contiguous range of the sorted
+// order.  Per column:
+//   gather  : the particle fields of the range (through the sorted index) and
+//             the column's terrain strip are copied into shared staging with
+//             cp.async, one column ahead -- the gathers of column cc+1 fly
+//             while column cc is computed;
+//   records : local coordinates and the nine transferred quantities per
+//             particle, computed once from the staging (SoA, swizzled);
+//   chains  : node row r is served by lane r of each of the four warps, which
+//             walk the particles of cells (r-1, cc) then (r, cc) and extend two
+//             chains per quantity:
+//               fin   : node (r, cc)   -- local node 1 of cell (r-1,cc), then
+//                       0 of (r,cc); it already holds cells (r-1,cc-1),
+//                       (r,cc-1) from the previous column;
+//               start : node (r, cc+1) -- local node 3 of cell (r-1,cc), then
+//                       2 of (r,cc).
+//             That is each node's contributions in quadgrid's cell-sweep
+//             order, so every nodal sum equals the reference's sequential sum
+//             bit for bit.  The warps split the quantities (warp-uniform
+//             code): g0 {Mv, mom_x, mom_y}, g1 {FPx, FPy, Fric_x},
+//             g2 {Fric_y, Fint_x}, g3 {Fint_y};
+//   nodal   : warp 0 collects the finished chains and applies the nodal
+//             update (momentum, velocity, walls) to node column cc.
+// A column whose range exceeds kCap (pile-ups) is processed in synchronous
+// batches instead.
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int kNQ = 9;  // Mv, mom_x, mom_y, FPx, FPy, Fric_x, Fric_y, Fint_x, Fint_y
 
 struct P2GSmem {
+  // records
   double xi[kCap], eta[kCap], Mp[kCap], mpx[kCap], mpy[kCap], Fpx[kCap],
       Fpy[kCap], Frx[kCap], Fry[kCap], F11[kCap], F12[kCap], F22[kCap],
       Vp[kCap];
-  int rowstart[kTR + 2];
-  double hand[kNQ][kTR];
+  // gather staging (cp.async destination)
+  double gx[kCap], gy[kCap], gMp[kCap], gVp[kCap], gH[kCap], ghp[kCap],
+      gvx[kCap], gvy[kCap], gF11[kCap], gF12[kCap], gF22[kCap];
+  int gkey[kCap];
+  int gidx[kCap];
+  double zs[2][kTR + 2];  // Z at node rows rlo.., node columns cc and cc+1
+  int rowstart[3][kTR + 2];
+  double xfin[6][kTR];  // finished chains of warps 1-3, read by warp 0
+  double xst[6][kTR];
   double led[6][kP2GThreads / 32];
 };
 
-__device__ __forceinline__ void add_contrib(double (&acc)[kNQ],
-                                            const P2GSmem& s, int j, int k,
+__device__ __forceinline__ int swz(int j) { return j ^ ((j >> 4) & 15); }
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// (x - c*h)/h; when h is a power of two the quotient equals the product with
+// 1/h exactly, so the division is skipped.
+__device__ __forceinline__ double local1(double x, int c, double h, double ih,
+                                         bool pow2) {
+  const double d = x - c * h;
+  return pow2 ? d * ih : d / h;
+}
+
+// Nodal momentum, velocity and wall conditions of node (r, nc) from its nine
+// P2G sums (main/optim_par.cpp:467-529); also accumulates the node ledger.
+__device__ __forceinline__ void nodal_update(
+    double Mv, double momx, double momy, double FPx, double FPy, double Frx,
+    double Fry, double Fix, double Fiy, int r, int nc, const Geom& G,
+    const Phys& P, double dt, const Nodes& nodes, int record, double& ln0,
+    double& ln1, double& ln2) {
+  const int nrows = G.nrows, ncols = G.ncols;
+  const int n = r + nc * (nrows + 1);
+  const double Fextx = FPx + Frx;
+  const double Fexty = FPy + Fry;
+  const double Ftx = Fextx - Fix;
+  const double Fty = Fexty - Fiy;
+  ln0 += Mv;
+  ln1 += momx;
+  ln2 += momy;
+  momx = dt * Ftx + momx;
+  momy = dt * Fty + momy;
+  const bool act = Mv > 1.e-2;
+  double avx = act ? Ftx / Mv : 0.0;
+  double avy = act ? Fty / Mv : 0.0;
+  double vvx = act ? momx / Mv : 0.0;
+  double vvy = act ? momy / Mv : 0.0;
+  double vvxL = dt * avx + vvx;
+  double vvyL = dt * avy + vvy;
+  if (P.BC) {  // cells on the walls zero their 4 nodes (main/optim_par.cpp:503-529)
+    if (nc == 0 || nc == 1 || nc == ncols - 1 || nc == ncols) {
+      avx = 0.0; vvx = 0.0; vvxL = 0.0; momx = 0.0;
+    }
+    if (r == 0 || r == 1 || r == nrows - 1 || r == nrows) {
+      avy = 0.0; vvy = 0.0; vvyL = 0.0; momy = 0.0;
+    }
+  }
+  nodes.vvxL[n] = vvxL;
+  nodes.vvyL[n] = vvyL;
+  if (record) {
+    nodes.Mv[n] = Mv;
+    nodes.mvx[n] = momx;
+    nodes.mvy[n] = momy;
+    nodes.avx[n] = avx;
+    nodes.avy[n] = avy;
+    nodes.vvx[n] = vvx;
+    nodes.vvy[n] = vvy;
+    nodes.FPxv[n] = FPx;
+    nodes.FPyv[n] = FPy;
+    nodes.Fricx[n] = Frx;
+    nodes.Fricy[n] = Fry;
+    nodes.Fintx[n] = Fix;
+    nodes.Finty[n] = Fiy;
+  }
+}
+
+// one particle contribution to the chains of quantity group kG:
+//   upper = cell r-1 (fin: local 1, start: local 3)
+//   lower = cell r   (fin: local 0, start: local 2)
+template <int kG>
+__device__ __forceinline__ void chain_step(double (&fn)[3], double (&st)[3],
+                                           const P2GSmem& s, int l, bool upper,
+                                           double ihx, double mihx, double ihy,
+                                           double mihy) {
+  const double xi = s.xi[l], eta = s.eta[l];
+  const double omx = 1.0 - xi;
+  const double fb = upper ? eta : (1.0 - eta);
+  const double Nf = omx * fb, Ns = xi * fb;
+  if (kG == 0) {
+    const double q0 = s.Mp[l], q1 = s.mpx[l], q2 = s.mpy[l];
+    fn[0] += Nf * q0; fn[1] += Nf * q1; fn[2] += Nf * q2;
+    st[0] += Ns * q0; st[1] += Ns * q1; st[2] += Ns * q2;
+  } else if (kG == 1) {
+    const double q0 = s.Fpx[l], q1 = s.Fpy[l], q2 = s.Frx[l];
+    fn[0] += Nf * q0; fn[1] += Nf * q1; fn[2] += Nf * q2;
+    st[0] += Ns * q0; st[1] += Ns * q1; st[2] += Ns * q2;
+  } else {
+    // upper: fin local 1 -> Nx = mihx*eta,     Ny = (1-xi)*ihy
+    //        start local 3 -> Nx = ihx*eta,    Ny = xi*ihy
+    // lower: fin local 0 -> Nx = mihx*(1-eta), Ny = (1-xi)*mihy
+    //        start local 2 -> Nx = ihx*(1-eta), Ny = xi*mihy
+    const double Nxf = mihx * fb, Nxs = ihx * fb;
+    const double gy = upper ? ihy : mihy;
+    const double Nyf = omx * gy, Nys = xi * gy;
+    const double f11 = s.F11[l], f12 = s.F12[l], f22 = s.F22[l], vp = s.Vp[l];
+    if (kG == 2) {
+      const double q0 = s.Fry[l];
+      fn[0] += Nf * q0;
+      st[0] += Ns * q0;
+      fn[1] += (Nxf * f11 + Nyf * f12) * vp;
+      st[1] += (Nxs * f11 + Nys * f12) * vp;
+    } else {
+      fn[0] += (Nxf * f12 + Nyf * f22) * vp;
+      st[0] += (Nxs * f12 + Nys * f22) * vp;
+    }
+  }
+}
+
+template <int kG>
+__device__ __forceinline__ void chain_range(double (&fn)[3], double (&st)[3],
+                                            const P2GSmem& s, int a0, int a1,
+                                            int b0, int b1, int bb, int be,
                                             double ihx, double mihx,
                                             double ihy, double mihy) {
-  const double xi = s.xi[j], eta = s.eta[j];
-  const double N = shp(xi, eta, k);
-  const double Nx = shg_x(eta, k, ihx, mihx);
-  const double Ny = shg_y(xi, k, ihy, mihy);
-  acc[0] += N * s.Mp[j];
-  acc[1] += N * s.mpx[j];
-  acc[2] += N * s.mpy[j];
-  acc[3] += N * s.Fpx[j];
-  acc[4] += N * s.Fpy[j];
-  acc[5] += N * s.Frx[j];
-  acc[6] += N * s.Fry[j];
-  const double f12 = s.F12[j], vp = s.Vp[j];
-  acc[7] += (Nx * s.F11[j] + Ny * f12) * vp;
-  acc[8] += (Nx * f12 + Ny * s.F22[j]) * vp;
+  for (int j = max(a0, bb); j < min(a1, be); ++j)
+    chain_step<kG>(fn, st, s, swz(j - bb), true, ihx, mihx, ihy, mihy);
+  for (int j = max(b0, bb); j < min(b1, be); ++j)
+    chain_step<kG>(fn, st, s, swz(j - bb), false, ihx, mihx, ihy, mihy);
 }
+
+struct RecArgs {
+  double hx, hy, ihx, mihx, ihy, mihy;
+  bool px2, py2, fresh;
+  int record;
+};
+
+// record of one particle from its gathered fields; z[k] = Z at local node k
+__device__ __forceinline__ void make_record(
+    P2GSmem& s, int lj, int i, int cc, int pr, double x, double y, double Mp,
+    double Vp, double H, double hp, double vx, double vy, double F11,
+    double F12, double F22, const double (&z)[4], const Particles& p,
+    const Phys& P, const RecArgs& a, bool owned, double& lp0, double& lp1,
+    double& lp2) {
+  const double xi = local1(x, cc, a.hx, a.ihx, a.px2);
+  const double eta = local1(y, pr, a.hy, a.ihy, a.py2);
+  // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
+  double dzx = 0.0, dzy = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    dzx += shg_x(eta, k, a.ihx, a.mihx) * z[k];
+    dzy += shg_y(xi, k, a.ihy, a.mihy) * z[k];
+  }
+  // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
+  const double wb = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
+  const double Fpx = -P.g * Vp * P.rho * dzx * wb;
+  const double Fpy = -P.g * Vp * P.rho * dzy * wb;
+  double Ap, fbx, fby, mpx, mpy;
+  if (a.fresh) {
+    Ap = p.Ap[i];
+    fbx = p.Fbx[i];
+    fby = p.Fby[i];
+    mpx = p.mpx[i];
+    mpy = p.mpy[i];
+  } else {
+    // the values the reference stored at the end of the previous step
+    // (main/optim_par.cpp:600-626)
+    Ap = hp > 1.e-2 ? Vp / hp : 0.0;
+    voellmy(P, vx, vy, hp, fbx, fby);
+    mpx = vx * Mp;
+    mpy = vy * Mp;
+  }
+  const int l = swz(lj);
+  s.xi[l] = xi;
+  s.eta[l] = eta;
+  s.Mp[l] = Mp;
+  s.mpx[l] = mpx;
+  s.mpy[l] = mpy;
+  s.Fpx[l] = Fpx;
+  s.Fpy[l] = Fpy;
+  s.Frx[l] = Ap * fbx;
+  s.Fry[l] = Ap * fby;
+  s.F11[l] = F11;
+  s.F12[l] = F12;
+  s.F22[l] = F22;
+  s.Vp[l] = Vp;
+  if (a.record) {
+    p.dZxp[i] = dzx;
+    p.dZyp[i] = dzy;
+    p.Fpx[i] = Fpx;
+    p.Fpy[i] = Fpy;
+    p.Frx[i] = Ap * fbx;
+    p.Fry[i] = Ap * fby;
+  }
+  if (owned) {  // particle ledger, once per particle
+    lp0 += Mp;
+    lp1 += mpx;
+    lp2 += mpy;
+  }
+}
+
+// Issues the cp.async gathers of the range [j0, j1) (<= kCap particles) and
+// of the terrain strip of column cc.
+__device__ __forceinline__ void issue_gather(P2GSmem& s, const Particles& p,
+                                             const int* __restrict__ perm,
+                                             const double* __restrict__ Z,
+                                             int j0, int j1, int cc, int rlo,
+                                             int rhi, int nrows, int ncols) {
+  for (int j = j0 + threadIdx.x; j < j1; j += kP2GThreads) {
+    const int i = perm[j];
+    const int l = j - j0;
+    s.gidx[l] = i;
+    cp_async8(&s.gx[l], p.x + i);
+    cp_async8(&s.gy[l], p.y + i);
+    cp_async8(&s.gMp[l], p.Mp + i);
+    cp_async8(&s.gVp[l], p.Vp + i);
+    cp_async8(&s.gH[l], p.H + i);
+    cp_async8(&s.ghp[l], p.hp + i);
+    cp_async8(&s.gvx[l], p.vpx + i);
+    cp_async8(&s.gvy[l], p.vpy + i);
+    cp_async8(&s.gF11[l], p.F11 + i);
+    cp_async8(&s.gF12[l], p.F12 + i);
+    cp_async8(&s.gF22[l], p.F22 + i);
+    cp_async4(&s.gkey[l], p.key + i);
+  }
+  const int nz = rhi + 2 - rlo;  // node rows rlo .. rhi+1
+  for (int q = threadIdx.x; q < 2 * nz; q += kP2GThreads) {
+    const int col = q / nz, rr = q - col * nz;
+    const int nc = min(cc + col, ncols);
+    cp_async8(&s.zs[col][rr], Z + (rlo + rr) + nc * (nrows + 1));
+  }
+  cp_async_commit();
+}
+
 }  // namespace
 
-__global__ void __launch_bounds__(kP2GThreads)
-    k_p2g(Particles p, const int* __restrict__ perm,
-          const int* __restrict__ cstart, const double* __restrict__ Z,
-          Nodes nodes, double* __restrict__ led_part, Geom G, Phys P,
-          const Scalars* S, int record) {
-  if (!S->active) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  P2GSmem& s = *reinterpret_cast<P2GSmem*>(smem_raw);
-
+__device__ __forceinline__ void p2g_unit(
+    const Particles& p, const int* __restrict__ perm,
+    const int* __restrict__ cstart, const double* __restrict__ Z,
+    const Nodes& nodes, double* __restrict__ led_part, const Geom& G,
+    const Phys& P, const Scalars* S, int record, P2GSmem& s, int unit,
+    int strips) {
   const int nrows = G.nrows, ncols = G.ncols;
-  const int r0 = blockIdx.x * kTR;
-  const int cA = blockIdx.y * kLC;
+  const int r0 = (unit % strips) * kTR;
+  const int cA = (unit / strips) * kLC;
   const int cB = min(cA + kLC, ncols + 1);
   const int rlo = max(r0 - 1, 0);
   const int rhi = min(r0 + kTR - 1, nrows - 1);
   const int ccFirst = max(cA - 1, 0);
   const int ccLast = min(cB - 1, ncols - 1);
+  const int nrs = rhi - rlo + 2;  // row starts per column
   const int tid = threadIdx.x;
-  const int row = tid % kTR, side = tid / kTR;
+  const int warp = tid >> 5, lane = tid & 31;
+  // chain lanes: warp = quantity group (warp-uniform code), lane = node row
+  const int grp = warp;
+  const int row = lane;
   const int r = r0 + row;
+  const bool row_ok = (r <= nrows);
   const double dt = S->dt;
-  const bool fresh = S->fresh != 0;
-  const double hx = G.hx, hy = G.hy;
-  const double ihx = 1.0 / hx, mihx = -1.0 / hx;
-  const double ihy = 1.0 / hy, mihy = -1.0 / hy;
+  RecArgs ra;
+  ra.hx = G.hx;
+  ra.hy = G.hy;
+  ra.ihx = 1.0 / G.hx;
+  ra.mihx = -1.0 / G.hx;
+  ra.ihy = 1.0 / G.hy;
+  ra.mihy = -1.0 / G.hy;
+  ra.px2 = G.hx_pow2 != 0;
+  ra.py2 = G.hy_pow2 != 0;
+  ra.fresh = S->fresh != 0;
+  ra.record = record;
 
-  // any particle in the cell block this CTA touches?
-  int any = 0;
-  if (tid == 0) {
-    for (int cc = ccFirst; cc <= ccLast; ++cc)
-      any |= (cstart[rhi + cc * nrows + 1] - cstart[rlo + cc * nrows]) != 0;
-  }
-  any = __syncthreads_or(any);
   double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
-  if (any || record) {
-    for (int q = tid; q < kNQ * kTR; q += kP2GThreads)
-      (&s.hand[0][0])[q] = 0.0;
-    __syncthreads();
+  double fn[3] = {0, 0, 0}, st[3] = {0, 0, 0};
 
-    for (int cc = ccFirst; cc <= ccLast; ++cc) {
-      const int cbase = cc * nrows;
-      for (int q = tid; q < kTR + 2; q += kP2GThreads) {
-        const int rr = rlo + q;
-        s.rowstart[q] = cstart[min(rr, rhi + 1) + cbase];
-      }
-      __syncthreads();
-      const int seg0 = s.rowstart[0];
-      const int seg1 = s.rowstart[rhi - rlo + 1];
-      // per-thread ranges (global sorted positions) of cells r-1 and r
-      int a0 = 0, a1 = 0, b0 = 0, b1 = 0;  // cell r-1: [a0,a1), cell r: [b0,b1)
-      if (r - 1 >= rlo && r - 1 <= rhi) {
-        a0 = s.rowstart[r - 1 - rlo];
-        a1 = s.rowstart[r - rlo];
-      }
-      if (r >= rlo && r <= rhi) {
-        b0 = s.rowstart[r - rlo];
-        b1 = s.rowstart[r - rlo + 1];
-      }
-      const bool fin_active = (side == 0) && (cc >= cA) && (r <= nrows);
-      const bool start_active = (side == 1) && (cc + 1 < cB) && (r <= nrows);
-      double acc[kNQ];
-#pragma unroll
-      for (int q = 0; q < kNQ; ++q) acc[q] = (side == 0) ? s.hand[q][row] : 0.0;
-      __syncthreads();  // hand[] consumed before it is rewritten
+  // prologue: row starts of the first two columns, gather of the first
+  for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
+    const int k = q / nrs, rr = q - k * nrs;
+    const int cc = ccFirst + k;
+    if (cc <= ccLast) s.rowstart[cc % 3][rr] = cstart[rlo + rr + cc * nrows];
+  }
+  __syncthreads();
+  {
+    const int* R = s.rowstart[ccFirst % 3];
+    if (R[nrs - 1] - R[0] <= kCap)
+      issue_gather(s, p, perm, Z, R[0], R[nrs - 1], ccFirst, rlo, rhi, nrows, ncols);
+  }
 
+  for (int cc = ccFirst; cc <= ccLast; ++cc) {
+    const int cbase = cc * nrows;
+    const int* R = s.rowstart[cc % 3];
+    const int seg0 = R[0], seg1 = R[nrs - 1];
+    const bool fits = (seg1 - seg0) <= kCap;
+    // next column's range (its row starts are in shared memory already)
+    const bool has_next = cc + 1 <= ccLast;
+    int nseg0 = 0, nseg1 = 0;
+    if (has_next) {
+      nseg0 = s.rowstart[(cc + 1) % 3][0];
+      nseg1 = s.rowstart[(cc + 1) % 3][nrs - 1];
+    }
+    const bool next_fits = has_next && (nseg1 - nseg0) <= kCap;
+    // row starts two columns ahead: loaded now, stored at the end
+    int rs2 = 0;
+    const bool has_next2 = cc + 2 <= ccLast && tid < nrs;
+    if (has_next2) rs2 = cstart[rlo + tid + (cc + 2) * nrows];
+    // my rows' particle ranges: cell r-1 [a0,a1), cell r [b0,b1)
+    int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    if (row_ok && r - 1 >= rlo && r - 1 <= rhi) {
+      a0 = R[r - 1 - rlo];
+      a1 = R[r - rlo];
+    }
+    if (row_ok && r >= rlo && r <= rhi) {
+      b0 = R[r - rlo];
+      b1 = R[r - rlo + 1];
+    }
+
+    if (fits) {
+      cp_async_wait_all();
+      __syncthreads();  // gathers of column cc visible to all threads
+      for (int j = seg0 + tid; j < seg1; j += kP2GThreads) {
+        const int lj = j - seg0;
+        const int pr = s.gkey[lj] - cbase;
+        const int zr = pr - rlo;
+        const double z[4] = {s.zs[0][zr], s.zs[0][zr + 1], s.zs[1][zr], s.zs[1][zr + 1]};
+        make_record(s, lj, s.gidx[lj], cc, pr, s.gx[lj], s.gy[lj], s.gMp[lj], s.gVp[lj],
+                    s.gH[lj], s.ghp[lj], s.gvx[lj], s.gvy[lj], s.gF11[lj], s.gF12[lj],
+                    s.gF22[lj], z, p, P, ra, pr >= r0 && pr < r0 + kTR && cc >= cA, lp0,
+                    lp1, lp2);
+      }
+      __syncthreads();  // records complete, staging free
+      if (next_fits)
+        issue_gather(s, p, perm, Z, nseg0, nseg1, cc + 1, rlo, rhi, nrows, ncols);
+      switch (grp) {
+        case 0: chain_range<0>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+        case 1: chain_range<1>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+        case 2: chain_range<2>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+        default: chain_range<3>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+      }
+    } else {
+      // a pile-up column: synchronous batches of kCap particles
       for (int bb = seg0; bb < seg1; bb += kCap) {
         const int be = min(bb + kCap, seg1);
-        // ---- particle records -------------------------------------------
         for (int j = bb + tid; j < be; j += kP2GThreads) {
           const int i = perm[j];
-          const int lj = j - bb;
-          const int pr = p.key[i] - cbase;  // cell row
-          const double x = p.x[i], y = p.y[i];
-          double xi, eta;
-          local_xy(x, y, cc, pr, hx, hy, xi, eta);
-          const double Mp = p.Mp[i], Vp = p.Vp[i], H = p.H[i], hp = p.hp[i];
-          const double vx = p.vpx[i], vy = p.vpy[i];
-          // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
-          double dzx = 0.0, dzy = 0.0;
+          const int pr = p.key[i] - cbase;
+          double z[4];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const double zn = Z[node_of(k, cc, pr, nrows)];
-            dzx += shg_x(eta, k, ihx, mihx) * zn;
-            dzy += shg_y(xi, k, ihy, mihy) * zn;
-          }
-          // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
-          const double wb = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
-          const double Fpx = -P.g * Vp * P.rho * dzx * wb;
-          const double Fpy = -P.g * Vp * P.rho * dzy * wb;
-          double Ap, fbx, fby, mpx, mpy;
-          if (fresh) {
-            Ap = p.Ap[i];
-            fbx = p.Fbx[i];
-            fby = p.Fby[i];
-            mpx = p.mpx[i];
-            mpy = p.mpy[i];
-          } else {
-            // values the reference stored at the end of the previous step
-            // (main/optim_par.cpp:600-626)
-            Ap = hp > 1.e-2 ? Vp / hp : 0.0;
-            voellmy(P, vx, vy, hp, fbx, fby);
-            mpx = vx * Mp;
-            mpy = vy * Mp;
-          }
-          s.xi[lj] = xi;
-          s.eta[lj] = eta;
-          s.Mp[lj] = Mp;
-          s.mpx[lj] = mpx;
-          s.mpy[lj] = mpy;
-          s.Fpx[lj] = Fpx;
-          s.Fpy[lj] = Fpy;
-          s.Frx[lj] = Ap * fbx;
-          s.Fry[lj] = Ap * fby;
-          s.F11[lj] = p.F11[i];
-          s.F12[lj] = p.F12[i];
-          s.F22[lj] = p.F22[i];
-          s.Vp[lj] = Vp;
-          if (record) {
-            p.dZxp[i] = dzx;
-            p.dZyp[i] = dzy;
-            p.Fpx[i] = Fpx;
-            p.Fpy[i] = Fpy;
-            p.Frx[i] = Ap * fbx;
-            p.Fry[i] = Ap * fby;
-          }
-          // particle ledger, once per particle (owning CTA only)
-          if (pr >= r0 && pr < r0 + kTR && cc >= cA) {
-            lp0 += Mp;
-            lp1 += mpx;
-            lp2 += mpy;
-          }
+          for (int k = 0; k < 4; ++k) z[k] = Z[node_of(k, cc, pr, nrows)];
+          make_record(s, j - bb, i, cc, pr, p.x[i], p.y[i], p.Mp[i], p.Vp[i], p.H[i],
+                      p.hp[i], p.vpx[i], p.vpy[i], p.F11[i], p.F12[i], p.F22[i], z, p,
+                      P, ra, pr >= r0 && pr < r0 + kTR && cc >= cA, lp0, lp1, lp2);
         }
         __syncthreads();
-        // ---- node chains --------------------------------------------------
-        if (fin_active || start_active) {
-          const int kA = fin_active ? 1 : 3;  // local node as seen from cell r-1
-          const int kB = fin_active ? 0 : 2;  // ... from cell r
-          for (int j = max(a0, bb); j < min(a1, be); ++j)
-            add_contrib(acc, s, j - bb, kA, ihx, mihx, ihy, mihy);
-          for (int j = max(b0, bb); j < min(b1, be); ++j)
-            add_contrib(acc, s, j - bb, kB, ihx, mihx, ihy, mihy);
+        switch (grp) {
+          case 0: chain_range<0>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+          case 1: chain_range<1>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+          case 2: chain_range<2>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+          default: chain_range<3>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
         }
         __syncthreads();
       }
-
-      // ---- finished node (r, cc) [side 0] or (r, ncols) [side 1, last] ----
-      const bool last_col = (side == 1) && (cc == ncols - 1) && (cB == ncols + 1) &&
-                            (r <= nrows);
-      if (fin_active || last_col) {
-        const int nc = fin_active ? cc : ncols;
-        const int n = r + nc * (nrows + 1);
-        const double Mv = acc[0];
-        double momx = acc[1], momy = acc[2];
-        const double Fextx = acc[3] + acc[5];
-        const double Fexty = acc[4] + acc[6];
-        const double Ftx = Fextx - acc[7];
-        const double Fty = Fexty - acc[8];
-        ln0 += Mv;
-        ln1 += momx;
-        ln2 += momy;
-        momx = dt * Ftx + momx;
-        momy = dt * Fty + momy;
-        const bool act = Mv > 1.e-2;
-        double avx = act ? Ftx / Mv : 0.0;
-        double avy = act ? Fty / Mv : 0.0;
-        double vvx = act ? momx / Mv : 0.0;
-        double vvy = act ? momy / Mv : 0.0;
-        double vvxL = dt * avx + vvx;
-        double vvyL = dt * avy + vvy;
-        if (P.BC) {
-          if (nc == 0 || nc == 1 || nc == ncols - 1 || nc == ncols) {
-            avx = 0.0; vvx = 0.0; vvxL = 0.0; momx = 0.0;
-          }
-          if (r == 0 || r == 1 || r == nrows - 1 || r == nrows) {
-            avy = 0.0; vvy = 0.0; vvyL = 0.0; momy = 0.0;
-          }
-        }
-        nodes.vvxL[n] = vvxL;
-        nodes.vvyL[n] = vvyL;
-        if (record) {
-          nodes.Mv[n] = Mv;
-          nodes.mvx[n] = momx;
-          nodes.mvy[n] = momy;
-          nodes.avx[n] = avx;
-          nodes.avy[n] = avy;
-          nodes.vvx[n] = vvx;
-          nodes.vvy[n] = vvy;
-          nodes.FPxv[n] = acc[3];
-          nodes.FPyv[n] = acc[4];
-          nodes.Fricx[n] = acc[5];
-          nodes.Fricy[n] = acc[6];
-          nodes.Fintx[n] = acc[7];
-          nodes.Finty[n] = acc[8];
-        }
-      }
-      if (start_active) {
-#pragma unroll
-        for (int q = 0; q < kNQ; ++q) s.hand[q][row] = acc[q];
-      }
-      __syncthreads();
+      if (next_fits)
+        issue_gather(s, p, perm, Z, nseg0, nseg1, cc + 1, rlo, rhi, nrows, ncols);
     }
+
+    // ---- nodal update of the finished nodes (warp 0) ---------------------
+    // g1: FPx FPy Frx | g2: Fry Fix | g3: Fiy
+    if (grp == 1) {
+      s.xfin[0][row] = fn[0]; s.xfin[1][row] = fn[1]; s.xfin[2][row] = fn[2];
+      s.xst[0][row] = st[0]; s.xst[1][row] = st[1]; s.xst[2][row] = st[2];
+    } else if (grp == 2) {
+      s.xfin[3][row] = fn[0]; s.xfin[4][row] = fn[1];
+      s.xst[3][row] = st[0]; s.xst[4][row] = st[1];
+    } else if (grp == 3) {
+      s.xfin[5][row] = fn[0];
+      s.xst[5][row] = st[0];
+    }
+    if (has_next2) s.rowstart[(cc + 2) % 3][tid] = rs2;
+    __syncthreads();
+    if (grp == 0) {
+      const bool do_fin = (cc >= cA) && row_ok;
+      const bool do_last = (cc == ncols - 1) && (cB == ncols + 1) && row_ok;
+      if (do_fin)
+        nodal_update(fn[0], fn[1], fn[2], s.xfin[0][row], s.xfin[1][row],
+                     s.xfin[2][row], s.xfin[3][row], s.xfin[4][row], s.xfin[5][row],
+                     r, cc, G, P, dt, nodes, record, ln0, ln1, ln2);
+      if (do_last)
+        nodal_update(st[0], st[1], st[2], s.xst[0][row], s.xst[1][row],
+                     s.xst[2][row], s.xst[3][row], s.xst[4][row], s.xst[5][row], r,
+                     ncols, G, P, dt, nodes, record, ln0, ln1, ln2);
+    }
+    // the started chains of node (r, cc+1) continue in the next column
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      fn[q] = st[q];
+      st[q] = 0.0;
+    }
+    // a non-fitting next column gathers synchronously: nothing in flight
+    if (has_next && !next_fits) cp_async_wait_all();
+    __syncthreads();
   }
+  cp_async_wait_all();
   // ---- ledger partials: fixed-order block reduction ----------------------
   {
     double v[6] = {lp0, lp1, lp2, ln0, ln1, ln2};
@@ -568,15 +768,64 @@ __global__ void __launch_bounds__(kP2GThreads)
     for (int q = 0; q < 6; ++q) {
       double x = v[q];
       for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if ((tid & 31) == 0) s.led[q][tid >> 5] = x;
+      if (lane == 0) s.led[q][warp] = x;
     }
     __syncthreads();
     if (tid < 6) {
       double x = 0.0;
       for (int w = 0; w < kP2GThreads / 32; ++w) x += s.led[tid][w];
-      led_part[(size_t)(blockIdx.y * gridDim.x + blockIdx.x) * 6 + tid] = x;
+      led_part[(size_t)unit * 6 + tid] = x;
+    }
+    __syncthreads();
+  }
+}
+
+// Lists the P2G units (strip, chunk) whose cell block holds particles; the
+// others have nothing to transfer (their ledger partials are zeroed here).
+// List order is irrelevant: units write disjoint nodes and their ledger
+// partials go to the slot of the unit, reduced in unit order.
+__global__ void k_units(const int* __restrict__ cstart, int strips, int chunks,
+                        int* __restrict__ ulist, int* __restrict__ ucount,
+                        double* __restrict__ led_part, Geom G, const Scalars* S) {
+  if (!S->active) return;
+  const int nrows = G.nrows, ncols = G.ncols;
+  const int nu = strips * chunks;
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nu;
+       u += gridDim.x * blockDim.x) {
+    const int strip = u % strips, chunk = u / strips;
+    const int r0 = strip * kTR, cA = chunk * kLC;
+    const int cB = min(cA + kLC, ncols + 1);
+    const int rlo = max(r0 - 1, 0), rhi = min(r0 + kTR - 1, nrows - 1);
+    const int c0 = max(cA - 1, 0), c1 = min(cB - 1, ncols - 1);
+    int n = 0;
+    for (int cc = c0; cc <= c1; ++cc)
+      n += cstart[rhi + cc * nrows + 1] - cstart[rlo + cc * nrows];
+    if (n > 0) {
+      ulist[atomicAdd(ucount, 1)] = u;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) led_part[(size_t)u * 6 + q] = 0.0;
     }
   }
+}
+
+__global__ void k_units_reset(int* ucount, const Scalars* S) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) *ucount = 0;
+}
+
+__global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
+    k_p2g(Particles p, const int* __restrict__ perm,
+          const int* __restrict__ cstart, const double* __restrict__ Z,
+          Nodes nodes, double* __restrict__ led_part, Geom G, Phys P,
+          const Scalars* S, int record, const int* __restrict__ ulist,
+          const int* __restrict__ ucount, int strips) {
+  if (!S->active) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  P2GSmem& s = *reinterpret_cast<P2GSmem*>(smem_raw);
+  const int nunits = *ucount;
+  for (int ui = blockIdx.x; ui < nunits; ui += gridDim.x)
+    p2g_unit(p, perm, cstart, Z, nodes, led_part, G, P, S, record, s, ulist[ui],
+             strips);
 }
 
 __global__ void k_ledger_final(const double* __restrict__ led_part, int nparts,
@@ -648,7 +897,7 @@ __global__ void __launch_bounds__(kG2PThreads)
     }
     double x = p.x[i], y = p.y[i];
     double xi, eta;
-    local_xy(x, y, c, r, hx, hy, xi, eta);
+    local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
     double vxL = 0.0, vyL = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -675,7 +924,7 @@ __global__ void __launch_bounds__(kG2PThreads)
     if (y < eps) y = eps;
     if (y > G.Ly - eps) y = G.Ly - eps;
     // g2pd {vvxL, vvyL} at the new position, old cell (main/optim_par.cpp:578)
-    local_xy(x, y, c, r, hx, hy, xi, eta);
+    local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
     double vxdx = 0.0, vydx = 0.0, vxdy = 0.0, vydy = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {

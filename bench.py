@@ -1,0 +1,320 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 MPM time step (particle-steps/s).
+
+Workload: the 2048x2048 mudflow (hx = 0.5 m, seeded bumpy slope, ~4.02M
+particles, Bingham + Voellmy, adaptive CFL 0.4), plain FP64.  A step is one
+pass of the reference loop body over all particles.  The particle state
+(11 x 8 B x Np = 354 MB) is larger than the 126 MB L2, so no flush is done
+between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0.  Multi-GPU runs are independent replicas (one
+scenario per GPU, weak scaling): the single-scenario step has no exchange.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+WORKLOAD = "mudflow 2048x2048 cells, hx=0.5 m, ~4.02M particles, Bingham+Voellmy, CFL 0.4"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_profile():
+    """dram bytes per launch from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"dampm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = max(mx, float(parts[2]))
+                except ValueError:
+                    continue
+                for k, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(k)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def _allreduce(x: float, world: int, op: str = "max") -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _touched_nodes(d, key_cells: np.ndarray) -> int:
+    """Nodes written by P2G's active strips: corners of occupied cells."""
+    nrows = int(d.scalars["Ney"])
+    cells = np.unique(key_cells)
+    r = cells % nrows
+    c = cells // nrows
+    nodes = set()
+    NR = nrows + 1
+    for dr in (0, 1):
+        for dc in (0, 1):
+            nodes.update(((r + dr) + (c + dc) * NR).tolist())
+    return len(nodes)
+
+
+def cpu_baseline_port(d, seconds: float = 15.0):
+    """The CPU restatement of optim_par (OpenMP, all host cores) on a bounded
+    sample of the same workload: as many steps as fit in ~`seconds`."""
+    from oracle.oracle import Oracle
+    threads = os.cpu_count() or 1
+    o = Oracle(d, threads=threads)
+    o.run(1)  # warm-up (first-touch of the nodal arrays)
+    n = 0
+    t0 = time.perf_counter()
+    while n < 1 or (time.perf_counter() - t0 < seconds and n < 50):
+        o.run(1)
+        n += 1
+    el = time.perf_counter() - t0
+    np_ = o.np
+    o.close()
+    return {"value": np_ * n / el, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{n} steps of the full workload ({np_} particles) after 1 warm-up step, "
+                      f"{el:.1f} s"}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference algorithm on the host cores (the
+    oracle restatement of main/optim_par.cpp; the reference binary itself
+    needs the absent quadgrid submodule), same workload, bounded sample."""
+    if rank != 0:
+        return 0
+    from amsc_b200 import scenarios
+    d = scenarios.mudflow(N=2048)
+    from oracle.oracle import Oracle
+    threads = os.cpu_count() or 1
+    o = Oracle(d, threads=threads)
+    for _ in range(max(args.warmup, 1)):
+        o.run(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.run(1)
+    el = time.perf_counter() - t0
+    v = o.np * args.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": o.np, "grid": "2048x2048",
+                       "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} timed steps after {max(args.warmup, 1)} "
+                                       f"warm-up steps of the full workload"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = _dist_init()
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        _barrier(world)
+        return rc
+
+    import torch
+    torch.cuda.set_device(local)
+    from amsc_b200 import scenarios
+    from amsc_b200.dampm import STATE_FIELDS, Solver
+
+    d = scenarios.mudflow(N=2048, seed=12345 + rank)
+    np_ = d.np
+    s = Solver(d)
+    # warm-up
+    s.step(args.warmup)
+    s.sync()
+    keys_cells = None
+    # timed region: K steps, device-timed with CUDA events on the library stream
+    sampler = ClockSampler(local)
+    _barrier(world)
+    s.sync()
+    s.timings(True)
+    sampler.start()
+    s.step(args.steps)
+    s.sync()
+    clocks = sampler.stop()
+    tm = s.timings(False)
+    launches = s.last_launch_count()
+    el_ms = _allreduce(float(tm[4]), world)
+    total_particles = _allreduce(float(np_), world, "sum")
+    value = total_particles * args.steps / (el_ms * 1e-3)
+    ms_per_step = el_ms / args.steps
+    st = s.status()
+
+    # roofline of the dominant kernel (P2G), algorithmic bytes per launch:
+    # 96 B per particle (11 f64 fields, sorted index, cell key) + 24 B per
+    # written node (vvxL, vvyL, Z)
+    x = s.download("x")
+    y = s.download("y")
+    h = float(d.scalars["hx"])
+    nrows = int(d.scalars["Ney"])
+    kc = (np.clip(np.floor(y / h), 0, nrows - 1).astype(np.int64) +
+          np.clip(np.floor(x / h), 0, int(d.scalars["Nex"]) - 1).astype(np.int64) * nrows)
+    n_nodes = _touched_nodes(d, kc)
+    np_now = st["np"]
+    p2g_bytes = 96 * np_now + 24 * n_nodes
+    g2p_bytes = 104 * np_now + 16 * n_nodes
+    p2g_ms = tm[1] / args.steps
+    g2p_ms = tm[2] / args.steps
+    peak, peak_kind = _peaks()
+    dom = "p2g" if p2g_ms >= g2p_ms else "g2p"
+    dom_bytes, dom_ms = (p2g_bytes, p2g_ms) if dom == "p2g" else (g2p_bytes, g2p_ms)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = _traffic_profile().get(dom)
+
+    # end to end through the C ABI with host buffers: per step the persistent
+    # state goes host->device from pinned memory (dampm_set_state), the step
+    # runs, and the state comes back (dampm_get_state)
+    pin = {k: torch.empty(np_now, dtype=torch.float64, pin_memory=True).numpy()
+           for k in STATE_FIELDS}
+    s.get_state(pin)
+    e2e_steps = max(args.e2e_steps, 1)
+    _barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.set_state(pin)
+        s.step(1)
+        s.get_state(pin)
+    e2e_s = _allreduce(time.perf_counter() - t0, world)
+    e2e_value = total_particles * e2e_steps / e2e_s
+    state_bytes = 8 * len(STATE_FIELDS) * np_now
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_port(d)
+        except Exception as e:  # reported, not fatal
+            cpu = {"error": str(e)}
+    s.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": np_, "grid": "2048x2048",
+                       "precision": "fp64", "parallelism": f"replicas{world}",
+                       "l2": "state 354 MB > 126 MB L2, no flush",
+                       "seed": 12345},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": dom_bytes,
+                         "kernel_ms": dom_ms},
+            "kernels_ms_per_step": {"sort": tm[0] / args.steps, "p2g": p2g_ms,
+                                    "g2p": g2p_ms, "other": tm[3] / args.steps},
+            "e2e": {"value": e2e_value, "unit": METRIC,
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "state": {"it": st["it"], "t": st["t"], "dt": st["dt"]},
+        }
+        print(json.dumps(line), flush=True)
+    _barrier(world)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
