@@ -36,6 +36,7 @@ struct dampm_ctx {
   int n_led = 0;
   int strips = 0, chunks = 0;
   int *ulist = nullptr, *ucount = nullptr;
+  int *clist = nullptr, *clist_n = nullptr;  // cells with >= 2 particles
   int p2g_grid = 0;
   Scalars* S = nullptr;
   Scalars* Sh = nullptr;  // pinned host mirror
@@ -136,7 +137,7 @@ int alloc_particles(dampm_ctx* ctx, long long cap) {
                   &p.F11,   &p.F12,   &p.F22,    &p.Mp,     &p.Vp,
                   &p.H,     &p.Ap,    &p.mpx,    &p.mpy,    &p.Fbx,
                   &p.Fby,   &p.vpx_dx, &p.vpx_dy, &p.vpy_dx, &p.vpy_dy,
-                  &p.xp,    &p.yp};
+                  &p.xp,    &p.yp,    &p.qfx,    &p.qfy,    &p.qwb};
   for (double** q : f) {
     int rc = dalloc(ctx, q, cap);
     if (rc) return rc;
@@ -163,13 +164,14 @@ void enqueue_sort(dampm_ctx* ctx) {
                                                               ctx->tile_sum, ctx->S);
   k_scan_tile_sums<<<1, kScanThreads, 0, ctx->stream>>>(ctx->tile_sum, ctx->ntiles,
                                                         ctx->S);
+  k_list_reset<<<1, 1, 0, ctx->stream>>>(ctx->clist_n, ctx->S);
   k_scan_apply<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(
-      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->S);
+      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S);
   k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->slot, ctx->start,
                                          ctx->perm, ctx->S);
-  k_segment_order<<<grid_for(ctx->nc, 256), 256, 0, ctx->stream>>>(
-      ctx->start, ctx->nc, ctx->perm, ctx->S);
-  ctx->launches += 6;
+  k_segment_order<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,
+                                                   ctx->clist_n, ctx->perm, ctx->S);
+  ctx->launches += 7;
 }
 
 int enqueue_pass(dampm_ctx* ctx) {
@@ -345,7 +347,9 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvxL, nn);
   rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvyL, nn);
   ctx->ntiles = (ctx->nc + kScanTile - 1) / kScanTile;
-  rc = rc ? rc : dalloc(ctx, &ctx->count, ctx->nc);
+  rc = rc ? rc : dalloc(ctx, &ctx->count, size_t(ctx->nc) + 4);
+  rc = rc ? rc : dalloc(ctx, &ctx->clist, size_t(ctx->nc) + 4);
+  rc = rc ? rc : dalloc(ctx, &ctx->clist_n, 4);
   rc = rc ? rc : dalloc(ctx, &ctx->start, size_t(ctx->nc) + 1);
   rc = rc ? rc : dalloc(ctx, &ctx->tile_sum, size_t(ctx->ntiles) + 1);
   ctx->strips = (grid->Ney + 1 + kTR - 1) / kTR;
@@ -449,6 +453,7 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
   if (np > 0) {
     k_init_particles<<<grid_for(np, 256), 256, 0, ctx->stream>>>(
         p, ctx->Z, ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np));
+    k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, 0);
     CK(cudaGetLastError());
   }
   ctx->it_host = 0;
@@ -584,8 +589,8 @@ int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
   else if (f == "label") isrc = p.label;
   else if (f == "level") isrc = p.level;
   else if (f == "Ap") { if (fresh) src = p.Ap; else derived = 0; }
-  else if (f == "mom_px") { if (fresh) src = p.mpx; else derived = 1; }
-  else if (f == "mom_py") { if (fresh) src = p.mpy; else derived = 2; }
+  else if (f == "mom_px") src = p.mpx;
+  else if (f == "mom_py") src = p.mpy;
   else if (f == "Fb_x") { if (fresh) src = p.Fbx; else derived = 3; }
   else if (f == "Fb_y") { if (fresh) src = p.Fby; else derived = 4; }
   else if (ctx->record_alloc) {
@@ -692,6 +697,7 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
                      ctx->stream));
   k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.x, p.y, p.key, ctx->G, ctx->S);
   k_reduce_state<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->S);
+  k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, fresh ? 0 : 1);
   CK(cudaGetLastError());
   return DAMPM_OK;
 }

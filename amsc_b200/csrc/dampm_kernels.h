@@ -23,9 +23,14 @@ struct Particles {
   // persistent state
   double *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
   int *label, *level, *key;
-  // values stored by the reference at the end of a step; read by the next
-  // P2G only when Scalars::fresh is set (after upload or merge/split)
-  double *Ap, *mpx, *mpy, *Fbx, *Fby;
+  // inputs of the next P2G, as the reference stores them at the end of a
+  // step (main/optim_par.cpp:600-626): momentum mom = v*Mp, friction force
+  // Fric = Ap*Fb and the well-balance factor 1 - H/hp; written by G2P (or
+  // by k_prep after an upload, a state upload or a merge/split)
+  double *mpx, *mpy, *qfx, *qfy, *qwb;
+  // Ap and Fb as stored at upload / merge/split (valid while Scalars::fresh
+  // is set; otherwise they are derived from the state)
+  double *Ap, *Fbx, *Fby;
   // velocity gradients (merge/split input, outputs)
   double *vpx_dx, *vpx_dy, *vpy_dx, *vpy_dy;
   // output-only fields (allocated when outputs are recorded)
@@ -49,17 +54,20 @@ __global__ void k_init_particles(Particles p, const double* Z,
 __global__ void k_keys(const double* x, const double* y, int* key, Geom G,
                        const Scalars* S);
 __global__ void k_reduce_state(Particles p, Scalars* S);
+__global__ void k_prep(Particles p, Phys P, const Scalars* S, int derive);
 __global__ void k_count(const int* key, int* count, int* slot,
                         const Scalars* S);
 __global__ void k_scan_tiles(const int* count, int n, int* tile_sum,
                              const Scalars* S);
 __global__ void k_scan_tile_sums(int* tile_sum, int ntiles, const Scalars* S);
 __global__ void k_scan_apply(int* count, int n, const int* tile_sum,
-                             int* start, const Scalars* S);
+                             int* start, int* list, int* list_n,
+                             const Scalars* S);
+__global__ void k_list_reset(int* list_n, const Scalars* S);
 __global__ void k_scatter(const int* key, const int* slot, const int* start,
                           int* perm, const Scalars* S);
-__global__ void k_segment_order(const int* start, int ncells, int* perm,
-                                const Scalars* S);
+__global__ void k_segment_order(const int* start, const int* list,
+                                const int* list_n, int* perm, const Scalars* S);
 __global__ void k_units(const int* cstart, int strips, int chunks, int* ulist,
                         int* ucount, double* led_part, Geom G, const Scalars* S);
 __global__ void k_units_reset(int* ucount, const Scalars* S);

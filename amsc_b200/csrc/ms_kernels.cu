@@ -394,7 +394,7 @@ int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
                  const Scalars* S, cudaStream_t st) {
   k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, S);
   k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(tile_sum, ntiles, S);
-  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, S);
+  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, nullptr, nullptr, S);
   return 3;
 }
 
@@ -453,7 +453,8 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
   k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
-  n += 3;
+  k_prep<<<gp, 256, 0, st>>>(p, P, S, 0);
+  n += 4;
   return n;
 }
 

@@ -159,6 +159,33 @@ __global__ void k_reduce_state(Particles p, Scalars* S) {
   }
 }
 
+// Inputs of the next P2G from the stored Ap/Fb/mom (derive == 0: after an
+// upload or a merge/split) or from the state alone (derive != 0), exactly as
+// the reference computes them at the end of a step
+// (main/optim_par.cpp:447-459,600-626).
+__global__ void k_prep(Particles p, Phys P, const Scalars* S, int derive) {
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    const double hp = p.hp[i];
+    double Ap, fbx, fby;
+    if (derive) {
+      Ap = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
+      voellmy(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
+      p.mpx[i] = p.vpx[i] * p.Mp[i];
+      p.mpy[i] = p.vpy[i] * p.Mp[i];
+    } else {
+      Ap = p.Ap[i];
+      fbx = p.Fbx[i];
+      fby = p.Fby[i];
+    }
+    p.qfx[i] = Ap * fbx;
+    p.qfy[i] = Ap * fby;
+    const double H = p.H[i];
+    p.qwb[i] = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // SORT: stable counting sort by cell, (cell, particle index) order
 // (init_particle_mesh + cell_start/cell_ptcls, main/gpu_offload.cpp:243-249)
@@ -172,110 +199,118 @@ __global__ void k_count(const int* __restrict__ key, int* __restrict__ count,
     slot[i] = atomicAdd(&count[key[i]], 1);
 }
 
-// exclusive scan of count[0..n) into start[0..n]; count is zeroed on the way
-// (ready for the next step).  Three phases over tiles of kScanTile items.
-__global__ void k_scan_tiles(const int* __restrict__ count, int n,
-                             int* __restrict__ tile_sum, const Scalars* S) {
+// Exclusive scan of count[0..n) into start[0..n] in two passes over tiles of
+// kScanTile = 4 x kScanThreads items (each thread one int4): tile totals,
+// then per tile a block scan plus the scanned total of the preceding tiles.
+// count is zeroed on the way (ready for the next step).  When `list` is
+// given, cells holding two or more particles are appended to it (the cells
+// whose order k_segment_order has to establish).
+__device__ __forceinline__ int block_incl_scan(int v, int* wsum) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    int ws = (lane < nw) ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += t;
+    }
+    if (lane < nw) wsum[lane] = ws;  // inclusive warp totals
+  }
+  __syncthreads();
+  return incl + (w > 0 ? wsum[w - 1] : 0);
+}
+
+__device__ __forceinline__ int4 load_count4(const int* count, int i0, int n) {
+  if (i0 + 3 < n && (i0 & 3) == 0) return *reinterpret_cast<const int4*>(count + i0);
+  int4 c;
+  c.x = (i0 < n) ? count[i0] : 0;
+  c.y = (i0 + 1 < n) ? count[i0 + 1] : 0;
+  c.z = (i0 + 2 < n) ? count[i0 + 2] : 0;
+  c.w = (i0 + 3 < n) ? count[i0 + 3] : 0;
+  return c;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_tiles(const int* __restrict__ count, int n, int* __restrict__ tile_sum,
+                 const Scalars* S) {
   if (!S->active) return;
   __shared__ int wsum[32];
-  const int base = blockIdx.x * kScanTile;
-  int s = 0;
-  for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
-    const int i = base + k;
-    if (i < n) s += count[i];
-  }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
+  const int i0 = blockIdx.x * kScanTile + threadIdx.x * 4;
+  const int4 c = load_count4(count, i0, n);
+  int v = c.x + c.y + c.z + c.w;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x < 32) {
-    int v = (threadIdx.x < (blockDim.x >> 5)) ? wsum[threadIdx.x] : 0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) tile_sum[blockIdx.x] = v;
+    int t = (threadIdx.x < (blockDim.x >> 5)) ? wsum[threadIdx.x] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = t;
   }
 }
 
 // single block: exclusive scan of the tile sums in place; total at [ntiles]
-__global__ void k_scan_tile_sums(int* __restrict__ tile_sum, int ntiles,
-                                 const Scalars* S) {
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_tile_sums(int* __restrict__ tile_sum, int ntiles, const Scalars* S) {
   if (!S->active) return;
   __shared__ int wsum[32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
+  int carry = 0;
   for (int base = 0; base < ntiles; base += blockDim.x) {
     const int i = base + threadIdx.x;
     const int v = (i < ntiles) ? tile_sum[i] : 0;
-    int incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) wsum[w] = incl;
+    const int incl = block_incl_scan(v, wsum);
+    if (i < ntiles) tile_sum[i] = carry + incl - v;
+    const int total = wsum[(blockDim.x >> 5) - 1];
     __syncthreads();
-    if (w == 0) {
-      int ws = (lane < nw) ? wsum[lane] : 0;
-      int wi = ws;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, wi, o);
-        if (lane >= o) wi += t;
-      }
-      if (lane < nw) wsum[lane] = wi - ws;  // exclusive warp offsets
-    }
-    __syncthreads();
-    const int excl = carry + wsum[w] + incl - v;
-    if (i < ntiles) tile_sum[i] = excl;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-    __syncthreads();
+    carry += total;
   }
   if (threadIdx.x == 0) tile_sum[ntiles] = carry;
 }
 
-__global__ void k_scan_apply(int* __restrict__ count, int n,
-                             const int* __restrict__ tile_sum,
-                             int* __restrict__ start, const Scalars* S) {
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_apply(int* __restrict__ count, int n, const int* __restrict__ tile_sum,
+                 int* __restrict__ start, int* __restrict__ list,
+                 int* __restrict__ list_n, const Scalars* S) {
   if (!S->active) return;
   __shared__ int wsum[32];
-  __shared__ int carry;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  const int base = blockIdx.x * kScanTile;
-  if (threadIdx.x == 0) carry = tile_sum[blockIdx.x];
-  __syncthreads();
-  for (int off = 0; off < kScanTile; off += blockDim.x) {
-    const int i = base + off + threadIdx.x;
-    int v = 0;
-    if (i < n) {
-      v = count[i];
-      count[i] = 0;
-    }
-    int incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) wsum[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-      int ws = (lane < nw) ? wsum[lane] : 0;
-      int wi = ws;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, wi, o);
-        if (lane >= o) wi += t;
+  const int i0 = blockIdx.x * kScanTile + threadIdx.x * 4;
+  const int4 c = load_count4(count, i0, n);
+  const int v = c.x + c.y + c.z + c.w;
+  const int incl = block_incl_scan(v, wsum);
+  const int e0 = tile_sum[blockIdx.x] + incl - v;
+  int4 o;
+  o.x = e0;
+  o.y = e0 + c.x;
+  o.z = o.y + c.y;
+  o.w = o.z + c.z;
+  if (i0 + 3 < n && (i0 & 3) == 0) {
+    *reinterpret_cast<int4*>(start + i0) = o;
+    *reinterpret_cast<int4*>(count + i0) = make_int4(0, 0, 0, 0);
+  } else {
+    const int ov[4] = {o.x, o.y, o.z, o.w};
+    for (int k = 0; k < 4; ++k)
+      if (i0 + k < n) {
+        start[i0 + k] = ov[k];
+        count[i0 + k] = 0;
       }
-      if (lane < nw) wsum[lane] = wi - ws;
-    }
-    __syncthreads();
-    const int excl = carry + wsum[w] + incl - v;
-    if (i < n) start[i] = excl;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-    __syncthreads();
   }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
-    start[n] = tile_sum[gridDim.x];
+  if (list) {
+    const int cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (cv[k] >= 2) list[atomicAdd(list_n, 1)] = i0 + k;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[n] = tile_sum[gridDim.x];
 }
 
 __global__ void k_scatter(const int* __restrict__ key,
@@ -289,23 +324,50 @@ __global__ void k_scatter(const int* __restrict__ key,
     perm[start[key[i]] + slot[i]] = i;
 }
 
-// Orders each cell's segment by ascending particle index (the atomics of
-// k_count hand out slots in arbitrary order).  One thread per cell.
-__global__ void k_segment_order(const int* __restrict__ start, int ncells,
+__global__ void k_list_reset(int* list_n, const Scalars* S) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) *list_n = 0;
+}
+
+// Orders each listed cell's segment by ascending particle index (the atomics
+// of k_count hand out slots in arbitrary order).  One warp per cell: a
+// register bitonic sort for up to 32 particles, an insertion sort by lane 0
+// for larger cells.  Particle indices are unique, so the order is total.
+__global__ void k_segment_order(const int* __restrict__ start,
+                                const int* __restrict__ list,
+                                const int* __restrict__ list_n,
                                 int* __restrict__ perm, const Scalars* S) {
   if (!S->active) return;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
-       c += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nl = *list_n;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nl;
+       w += (gridDim.x * blockDim.x) >> 5) {
+    const int c = list[w];
     const int b = start[c], e = start[c + 1];
-    if (e - b < 2) continue;
-    for (int j = b + 1; j < e; ++j) {
-      const int v = perm[j];
-      int k = j - 1;
-      while (k >= b && perm[k] > v) {
-        perm[k + 1] = perm[k];
-        --k;
+    const int m = e - b;
+    if (m <= 32) {
+      int v = (lane < m) ? perm[b + lane] : 0x7fffffff;
+#pragma unroll
+      for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          const int o = __shfl_xor_sync(0xffffffffu, v, j);
+          const bool up = ((lane & k) == 0);
+          const bool lower = ((lane & j) == 0);
+          // keep the min in the lower lane of an ascending pair
+          v = (lower == up) ? min(v, o) : max(v, o);
+        }
       }
-      perm[k + 1] = v;
+      if (lane < m) perm[b + lane] = v;
+    } else if (lane == 0) {
+      for (int j = b + 1; j < e; ++j) {
+        const int v = perm[j];
+        int k = j - 1;
+        while (k >= b && perm[k] > v) {
+          perm[k + 1] = perm[k];
+          --k;
+        }
+        perm[k + 1] = v;
+      }
     }
   }
 }
@@ -349,8 +411,8 @@ struct P2GSmem {
       Fpy[kCap], Frx[kCap], Fry[kCap], F11[kCap], F12[kCap], F22[kCap],
       Vp[kCap];
   // gather staging (cp.async destination)
-  double gx[kCap], gy[kCap], gMp[kCap], gVp[kCap], gH[kCap], ghp[kCap],
-      gvx[kCap], gvy[kCap], gF11[kCap], gF12[kCap], gF22[kCap];
+  double gx[kCap], gy[kCap], gMp[kCap], gVp[kCap], gmx[kCap], gmy[kCap],
+      gfx[kCap], gfy[kCap], gwb[kCap], gF11[kCap], gF12[kCap], gF22[kCap];
   int gkey[kCap];
   int gidx[kCap];
   double zs[2][kTR + 2];  // Z at node rows rlo.., node columns cc and cc+1
@@ -493,17 +555,17 @@ __device__ __forceinline__ void chain_range(double (&fn)[3], double (&st)[3],
 
 struct RecArgs {
   double hx, hy, ihx, mihx, ihy, mihy;
-  bool px2, py2, fresh;
+  bool px2, py2;
   int record;
 };
 
 // record of one particle from its gathered fields; z[k] = Z at local node k
 __device__ __forceinline__ void make_record(
     P2GSmem& s, int lj, int i, int cc, int pr, double x, double y, double Mp,
-    double Vp, double H, double hp, double vx, double vy, double F11,
-    double F12, double F22, const double (&z)[4], const Particles& p,
-    const Phys& P, const RecArgs& a, bool owned, double& lp0, double& lp1,
-    double& lp2) {
+    double Vp, double mpx, double mpy, double qfx, double qfy, double wb,
+    double F11, double F12, double F22, const double (&z)[4],
+    const Particles& p, const Phys& P, const RecArgs& a, bool owned,
+    double& lp0, double& lp1, double& lp2) {
   const double xi = local1(x, cc, a.hx, a.ihx, a.px2);
   const double eta = local1(y, pr, a.hy, a.ihy, a.py2);
   // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
@@ -514,24 +576,8 @@ __device__ __forceinline__ void make_record(
     dzy += shg_y(xi, k, a.ihy, a.mihy) * z[k];
   }
   // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
-  const double wb = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
   const double Fpx = -P.g * Vp * P.rho * dzx * wb;
   const double Fpy = -P.g * Vp * P.rho * dzy * wb;
-  double Ap, fbx, fby, mpx, mpy;
-  if (a.fresh) {
-    Ap = p.Ap[i];
-    fbx = p.Fbx[i];
-    fby = p.Fby[i];
-    mpx = p.mpx[i];
-    mpy = p.mpy[i];
-  } else {
-    // the values the reference stored at the end of the previous step
-    // (main/optim_par.cpp:600-626)
-    Ap = hp > 1.e-2 ? Vp / hp : 0.0;
-    voellmy(P, vx, vy, hp, fbx, fby);
-    mpx = vx * Mp;
-    mpy = vy * Mp;
-  }
   const int l = swz(lj);
   s.xi[l] = xi;
   s.eta[l] = eta;
@@ -540,8 +586,8 @@ __device__ __forceinline__ void make_record(
   s.mpy[l] = mpy;
   s.Fpx[l] = Fpx;
   s.Fpy[l] = Fpy;
-  s.Frx[l] = Ap * fbx;
-  s.Fry[l] = Ap * fby;
+  s.Frx[l] = qfx;
+  s.Fry[l] = qfy;
   s.F11[l] = F11;
   s.F12[l] = F12;
   s.F22[l] = F22;
@@ -551,8 +597,8 @@ __device__ __forceinline__ void make_record(
     p.dZyp[i] = dzy;
     p.Fpx[i] = Fpx;
     p.Fpy[i] = Fpy;
-    p.Frx[i] = Ap * fbx;
-    p.Fry[i] = Ap * fby;
+    p.Frx[i] = qfx;
+    p.Fry[i] = qfy;
   }
   if (owned) {  // particle ledger, once per particle
     lp0 += Mp;
@@ -561,25 +607,43 @@ __device__ __forceinline__ void make_record(
   }
 }
 
-// Issues the cp.async gathers of the range [j0, j1) (<= kCap particles) and
-// of the terrain strip of column cc.
+constexpr int kPf = (kCap + kP2GThreads - 1) / kP2GThreads;
+
+// Loads the sorted indices of the range [j0, j1) into registers (issued a
+// batch ahead so that the gathers that depend on them do not wait).
+__device__ __forceinline__ void load_perm(int (&pf)[kPf],
+                                          const int* __restrict__ perm, int j0,
+                                          int j1) {
+#pragma unroll
+  for (int u = 0; u < kPf; ++u) {
+    const int j = j0 + threadIdx.x + u * kP2GThreads;
+    pf[u] = (j < j1) ? perm[j] : 0;
+  }
+}
+
+// Issues the cp.async gathers of the range [j0, j1) (<= kCap particles,
+// sorted indices in pf) and of the terrain strip of column cc.
 __device__ __forceinline__ void issue_gather(P2GSmem& s, const Particles& p,
-                                             const int* __restrict__ perm,
+                                             const int (&pf)[kPf],
                                              const double* __restrict__ Z,
                                              int j0, int j1, int cc, int rlo,
                                              int rhi, int nrows, int ncols) {
-  for (int j = j0 + threadIdx.x; j < j1; j += kP2GThreads) {
-    const int i = perm[j];
+#pragma unroll
+  for (int u = 0; u < kPf; ++u) {
+    const int j = j0 + threadIdx.x + u * kP2GThreads;
+    if (j >= j1) break;
+    const int i = pf[u];
     const int l = j - j0;
     s.gidx[l] = i;
     cp_async8(&s.gx[l], p.x + i);
     cp_async8(&s.gy[l], p.y + i);
     cp_async8(&s.gMp[l], p.Mp + i);
     cp_async8(&s.gVp[l], p.Vp + i);
-    cp_async8(&s.gH[l], p.H + i);
-    cp_async8(&s.ghp[l], p.hp + i);
-    cp_async8(&s.gvx[l], p.vpx + i);
-    cp_async8(&s.gvy[l], p.vpy + i);
+    cp_async8(&s.gmx[l], p.mpx + i);
+    cp_async8(&s.gmy[l], p.mpy + i);
+    cp_async8(&s.gfx[l], p.qfx + i);
+    cp_async8(&s.gfy[l], p.qfy + i);
+    cp_async8(&s.gwb[l], p.qwb + i);
     cp_async8(&s.gF11[l], p.F11 + i);
     cp_async8(&s.gF12[l], p.F12 + i);
     cp_async8(&s.gF22[l], p.F22 + i);
@@ -628,137 +692,128 @@ __device__ __forceinline__ void p2g_unit(
   ra.mihy = -1.0 / G.hy;
   ra.px2 = G.hx_pow2 != 0;
   ra.py2 = G.hy_pow2 != 0;
-  ra.fresh = S->fresh != 0;
   ra.record = record;
 
   double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
   double fn[3] = {0, 0, 0}, st[3] = {0, 0, 0};
 
-  // prologue: row starts of the first two columns, gather of the first
+  // The unit is processed as a sequence of batches: each cell column's range
+  // split into pieces of at most kCap particles.  The gathers of batch k+1
+  // are issued (cp.async) before the chains of batch k run.
+  //
+  // prologue: row starts of the first two columns, gather of the first batch
   for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
     const int k = q / nrs, rr = q - k * nrs;
     const int cc = ccFirst + k;
     if (cc <= ccLast) s.rowstart[cc % 3][rr] = cstart[rlo + rr + cc * nrows];
   }
   __syncthreads();
-  {
-    const int* R = s.rowstart[ccFirst % 3];
-    if (R[nrs - 1] - R[0] <= kCap)
-      issue_gather(s, p, perm, Z, R[0], R[nrs - 1], ccFirst, rlo, rhi, nrows, ncols);
-  }
+  int pf[kPf];
+  int cc = ccFirst;
+  int bb = s.rowstart[cc % 3][0];
+  int be = min(bb + kCap, s.rowstart[cc % 3][nrs - 1]);
+  load_perm(pf, perm, bb, be);
+  issue_gather(s, p, pf, Z, bb, be, cc, rlo, rhi, nrows, ncols);
+  int a0 = 0, a1 = 0, b0 = 0, b1 = 0;  // my rows' ranges in column cc
 
-  for (int cc = ccFirst; cc <= ccLast; ++cc) {
+  while (true) {
     const int cbase = cc * nrows;
     const int* R = s.rowstart[cc % 3];
     const int seg0 = R[0], seg1 = R[nrs - 1];
-    const bool fits = (seg1 - seg0) <= kCap;
-    // next column's range (its row starts are in shared memory already)
-    const bool has_next = cc + 1 <= ccLast;
-    int nseg0 = 0, nseg1 = 0;
+    const bool first_of_col = (bb == seg0);
+    const bool last_of_col = (be == seg1);
+    // the next batch: rest of this column, else the first of the next one
+    int ncc = cc, nbb = be, nbe = 0;
+    bool has_next = true;
+    if (last_of_col) {
+      ncc = cc + 1;
+      if (ncc > ccLast) {
+        has_next = false;
+      } else {
+        nbb = s.rowstart[ncc % 3][0];
+      }
+    }
     if (has_next) {
-      nseg0 = s.rowstart[(cc + 1) % 3][0];
-      nseg1 = s.rowstart[(cc + 1) % 3][nrs - 1];
+      const int nseg1 = s.rowstart[ncc % 3][nrs - 1];
+      nbe = min(nbb + kCap, nseg1);
+      load_perm(pf, perm, nbb, nbe);
     }
-    const bool next_fits = has_next && (nseg1 - nseg0) <= kCap;
-    // row starts two columns ahead: loaded now, stored at the end
+    // row starts two columns ahead: loaded now, stored at the column's end
     int rs2 = 0;
-    const bool has_next2 = cc + 2 <= ccLast && tid < nrs;
-    if (has_next2) rs2 = cstart[rlo + tid + (cc + 2) * nrows];
-    // my rows' particle ranges: cell r-1 [a0,a1), cell r [b0,b1)
-    int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-    if (row_ok && r - 1 >= rlo && r - 1 <= rhi) {
-      a0 = R[r - 1 - rlo];
-      a1 = R[r - rlo];
-    }
-    if (row_ok && r >= rlo && r <= rhi) {
-      b0 = R[r - rlo];
-      b1 = R[r - rlo + 1];
+    const bool has_rs2 = last_of_col && cc + 2 <= ccLast && tid < nrs;
+    if (has_rs2) rs2 = cstart[rlo + tid + (cc + 2) * nrows];
+    if (first_of_col) {
+      a0 = a1 = b0 = b1 = 0;
+      if (row_ok && r - 1 >= rlo && r - 1 <= rhi) {
+        a0 = R[r - 1 - rlo];
+        a1 = R[r - rlo];
+      }
+      if (row_ok && r >= rlo && r <= rhi) {
+        b0 = R[r - rlo];
+        b1 = R[r - rlo + 1];
+      }
     }
 
-    if (fits) {
-      cp_async_wait_all();
-      __syncthreads();  // gathers of column cc visible to all threads
-      for (int j = seg0 + tid; j < seg1; j += kP2GThreads) {
-        const int lj = j - seg0;
-        const int pr = s.gkey[lj] - cbase;
-        const int zr = pr - rlo;
-        const double z[4] = {s.zs[0][zr], s.zs[0][zr + 1], s.zs[1][zr], s.zs[1][zr + 1]};
-        make_record(s, lj, s.gidx[lj], cc, pr, s.gx[lj], s.gy[lj], s.gMp[lj], s.gVp[lj],
-                    s.gH[lj], s.ghp[lj], s.gvx[lj], s.gvy[lj], s.gF11[lj], s.gF12[lj],
-                    s.gF22[lj], z, p, P, ra, pr >= r0 && pr < r0 + kTR && cc >= cA, lp0,
-                    lp1, lp2);
-      }
-      __syncthreads();  // records complete, staging free
-      if (next_fits)
-        issue_gather(s, p, perm, Z, nseg0, nseg1, cc + 1, rlo, rhi, nrows, ncols);
-      switch (grp) {
-        case 0: chain_range<0>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-        case 1: chain_range<1>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-        case 2: chain_range<2>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-        default: chain_range<3>(fn, st, s, a0, a1, b0, b1, seg0, seg1, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-      }
-    } else {
-      // a pile-up column: synchronous batches of kCap particles
-      for (int bb = seg0; bb < seg1; bb += kCap) {
-        const int be = min(bb + kCap, seg1);
-        for (int j = bb + tid; j < be; j += kP2GThreads) {
-          const int i = perm[j];
-          const int pr = p.key[i] - cbase;
-          double z[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) z[k] = Z[node_of(k, cc, pr, nrows)];
-          make_record(s, j - bb, i, cc, pr, p.x[i], p.y[i], p.Mp[i], p.Vp[i], p.H[i],
-                      p.hp[i], p.vpx[i], p.vpy[i], p.F11[i], p.F12[i], p.F22[i], z, p,
-                      P, ra, pr >= r0 && pr < r0 + kTR && cc >= cA, lp0, lp1, lp2);
-        }
-        __syncthreads();
-        switch (grp) {
-          case 0: chain_range<0>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-          case 1: chain_range<1>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-          case 2: chain_range<2>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-          default: chain_range<3>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-        }
-        __syncthreads();
-      }
-      if (next_fits)
-        issue_gather(s, p, perm, Z, nseg0, nseg1, cc + 1, rlo, rhi, nrows, ncols);
+    cp_async_wait_all();
+    __syncthreads();  // gathers of this batch visible to all threads
+    for (int j = bb + tid; j < be; j += kP2GThreads) {
+      const int lj = j - bb;
+      const int pr = s.gkey[lj] - cbase;
+      const int zr = pr - rlo;
+      const double z[4] = {s.zs[0][zr], s.zs[0][zr + 1], s.zs[1][zr], s.zs[1][zr + 1]};
+      make_record(s, lj, s.gidx[lj], cc, pr, s.gx[lj], s.gy[lj], s.gMp[lj], s.gVp[lj],
+                  s.gmx[lj], s.gmy[lj], s.gfx[lj], s.gfy[lj], s.gwb[lj], s.gF11[lj],
+                  s.gF12[lj], s.gF22[lj], z, p, P, ra,
+                  pr >= r0 && pr < r0 + kTR && cc >= cA, lp0, lp1, lp2);
+    }
+    __syncthreads();  // records complete, staging free
+    if (has_next) issue_gather(s, p, pf, Z, nbb, nbe, ncc, rlo, rhi, nrows, ncols);
+    switch (grp) {
+      case 0: chain_range<0>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+      case 1: chain_range<1>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+      case 2: chain_range<2>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
+      default: chain_range<3>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
     }
 
-    // ---- nodal update of the finished nodes (warp 0) ---------------------
-    // g1: FPx FPy Frx | g2: Fry Fix | g3: Fiy
-    if (grp == 1) {
-      s.xfin[0][row] = fn[0]; s.xfin[1][row] = fn[1]; s.xfin[2][row] = fn[2];
-      s.xst[0][row] = st[0]; s.xst[1][row] = st[1]; s.xst[2][row] = st[2];
-    } else if (grp == 2) {
-      s.xfin[3][row] = fn[0]; s.xfin[4][row] = fn[1];
-      s.xst[3][row] = st[0]; s.xst[4][row] = st[1];
-    } else if (grp == 3) {
-      s.xfin[5][row] = fn[0];
-      s.xst[5][row] = st[0];
-    }
-    if (has_next2) s.rowstart[(cc + 2) % 3][tid] = rs2;
-    __syncthreads();
-    if (grp == 0) {
-      const bool do_fin = (cc >= cA) && row_ok;
-      const bool do_last = (cc == ncols - 1) && (cB == ncols + 1) && row_ok;
-      if (do_fin)
-        nodal_update(fn[0], fn[1], fn[2], s.xfin[0][row], s.xfin[1][row],
-                     s.xfin[2][row], s.xfin[3][row], s.xfin[4][row], s.xfin[5][row],
-                     r, cc, G, P, dt, nodes, record, ln0, ln1, ln2);
-      if (do_last)
-        nodal_update(st[0], st[1], st[2], s.xst[0][row], s.xst[1][row],
-                     s.xst[2][row], s.xst[3][row], s.xst[4][row], s.xst[5][row], r,
-                     ncols, G, P, dt, nodes, record, ln0, ln1, ln2);
-    }
-    // the started chains of node (r, cc+1) continue in the next column
+    if (last_of_col) {
+      // ---- nodal update of the finished nodes (warp 0) -------------------
+      // g1: FPx FPy Frx | g2: Fry Fix | g3: Fiy
+      if (grp == 1) {
+        s.xfin[0][row] = fn[0]; s.xfin[1][row] = fn[1]; s.xfin[2][row] = fn[2];
+        s.xst[0][row] = st[0]; s.xst[1][row] = st[1]; s.xst[2][row] = st[2];
+      } else if (grp == 2) {
+        s.xfin[3][row] = fn[0]; s.xfin[4][row] = fn[1];
+        s.xst[3][row] = st[0]; s.xst[4][row] = st[1];
+      } else if (grp == 3) {
+        s.xfin[5][row] = fn[0];
+        s.xst[5][row] = st[0];
+      }
+      if (has_rs2) s.rowstart[(cc + 2) % 3][tid] = rs2;
+      __syncthreads();
+      if (grp == 0) {
+        const bool do_fin = (cc >= cA) && row_ok;
+        const bool do_last = (cc == ncols - 1) && (cB == ncols + 1) && row_ok;
+        if (do_fin)
+          nodal_update(fn[0], fn[1], fn[2], s.xfin[0][row], s.xfin[1][row],
+                       s.xfin[2][row], s.xfin[3][row], s.xfin[4][row], s.xfin[5][row],
+                       r, cc, G, P, dt, nodes, record, ln0, ln1, ln2);
+        if (do_last)
+          nodal_update(st[0], st[1], st[2], s.xst[0][row], s.xst[1][row],
+                       s.xst[2][row], s.xst[3][row], s.xst[4][row], s.xst[5][row], r,
+                       ncols, G, P, dt, nodes, record, ln0, ln1, ln2);
+      }
+      // the started chains of node (r, cc+1) continue in the next column
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      fn[q] = st[q];
-      st[q] = 0.0;
+      for (int q = 0; q < 3; ++q) {
+        fn[q] = st[q];
+        st[q] = 0.0;
+      }
     }
-    // a non-fitting next column gathers synchronously: nothing in flight
-    if (has_next && !next_fits) cp_async_wait_all();
     __syncthreads();
+    if (!has_next) break;
+    cc = ncc;
+    bb = nbb;
+    be = nbe;
   }
   cp_async_wait_all();
   // ---- ledger partials: fixed-order block reduction ----------------------
@@ -868,7 +923,7 @@ __global__ void k_ledger_final(const double* __restrict__ led_part, int nparts,
 // cell of the step start, height update, Bingham stress, next cell key and
 // the CFL max-reductions (main/optim_par.cpp:532-651).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kG2PThreads)
+__global__ void __launch_bounds__(kG2PThreads, 2)
     k_g2p(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
           Phys P, Scalars* S, int record, int want_grad) {
   if (!S->active) return;
@@ -941,8 +996,8 @@ __global__ void __launch_bounds__(kG2PThreads)
     hp = hp / (1 + dt * div);
     hp = hp < 1e-2 ? 1e-2 : hp;
     double F11, F12, F22;
-    bingham_stress(P, vpx, vpy, hp, p.H[i], vxdx, vydy, vxdy, vydx, F11, F12,
-                   F22);
+    const double H = p.H[i];
+    bingham_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
     p.x[i] = x;
     p.y[i] = y;
     p.vpx[i] = vpx;
@@ -959,6 +1014,20 @@ __global__ void __launch_bounds__(kG2PThreads)
       p.vpy_dx[i] = vydx;
       p.vpy_dy[i] = vydy;
     }
+    // what the reference stores for the next step (main/optim_par.cpp:
+    // 600-626): momentum, area, basal friction; with the well-balance factor
+    // of the next gravity term (:450)
+    {
+      const double Mp = p.Mp[i], Vp = p.Vp[i];
+      p.mpx[i] = vpx * Mp;
+      p.mpy[i] = vpy * Mp;
+      const double Ap = hp > 1.e-2 ? Vp / hp : 0.0;
+      double fbx, fby;
+      voellmy(P, vpx, vpy, hp, fbx, fby);
+      p.qfx[i] = Ap * fbx;
+      p.qfy[i] = Ap * fby;
+      p.qwb[i] = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
+    }
     if (record) {
       // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
       double zp = 0.0;
@@ -966,16 +1035,6 @@ __global__ void __launch_bounds__(kG2PThreads)
       for (int k = 0; k < 4; ++k) zp += shp(xi, eta, k) * Z[nd[k]];
       p.Zp[i] = zp;
       p.hpZ[i] = hp + zp;
-      p.mpx[i] = vpx * p.Mp[i];
-      p.mpy[i] = vpy * p.Mp[i];
-      const double Vp = p.Vp[i];
-      p.Ap[i] = hp > 1.e-2 ? Vp / hp : 0.0;
-      double fbx, fby;
-      voellmy(P, vpx, vpy, hp, fbx, fby);
-      p.Fbx[i] = fbx;
-      p.Fby[i] = fby;
-      // HV: p2g hp with the same (stale) cell, atomics are fine here since
-      // the field is output-only (main/optim_par.cpp:650)
     }
     m0 = max(m0, ordered_key(fabs(vpx)));
     m1 = max(m1, ordered_key(fabs(vpy)));
