@@ -1,0 +1,116 @@
+"""TEST INFRASTRUCTURE ONLY -- drives the reference project's own programs
+built by ``make ref`` in oracle/ (``_ref/optim_par``, ``_ref/ms_harness``).
+
+``run_optim_par`` writes DATA.json into a scratch directory, runs the
+reference's main/optim_par.cpp there and parses what it writes: the
+``nc_particles_<it>.csv`` files (state at the start of step ``it``, i.e.
+after it-1 steps, main/optim_par.cpp:311-337), ``conservation_errors.csv``
+and the PERF line.  ``run_merge_split`` runs the reference's
+adaptive_merge_split (main/merge_split_ops_cmes.h) on a given state.
+"""
+from __future__ import annotations
+
+import csv
+import os
+import struct
+import subprocess
+import tempfile
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+OPTIM_PAR = os.path.join(REF_DIR, "optim_par")
+MS_HARNESS = os.path.join(REF_DIR, "ms_harness")
+
+
+def available() -> bool:
+    return os.path.exists(OPTIM_PAR) and os.path.exists(MS_HARNESS)
+
+
+def build(ref_root: str = "/root/reference") -> bool:
+    """Builds _ref/ from the reference sources when they are present."""
+    if not os.path.isdir(os.path.join(ref_root, "main")):
+        return available()
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
+    return available()
+
+
+def read_csv(path: str) -> Dict[str, np.ndarray]:
+    with open(path, newline="") as f:
+        rows = list(csv.reader(f))
+    header = [c.strip().strip('"').strip() for c in rows[0]]
+    data = np.array([[float(v) for v in r] for r in rows[1:] if r], dtype=np.float64)
+    return {name: data[:, k].copy() for k, name in enumerate(header)}
+
+
+def run_optim_par(d, workdir: Optional[str] = None, timeout: float = 600.0):
+    """Runs the reference CPU solver on DATA `d`; returns (csvs, errors, perf)
+    where csvs maps it -> {column: array}."""
+    from amsc_b200.data import to_json
+    own = workdir is None
+    wd = workdir or tempfile.mkdtemp(prefix="dampm_ref_")
+    to_json(d, os.path.join(wd, "DATA.json"))
+    out = subprocess.run([OPTIM_PAR], cwd=wd, capture_output=True, text=True,
+                         timeout=timeout, check=True)
+    csvs = {}
+    for fn in os.listdir(wd):
+        if fn.startswith("nc_particles_") and fn.endswith(".csv"):
+            csvs[int(fn[len("nc_particles_"):-4])] = read_csv(os.path.join(wd, fn))
+    errs = np.loadtxt(os.path.join(wd, "conservation_errors.csv"), delimiter=",",
+                      skiprows=1, ndmin=2)
+    perf = [l for l in out.stdout.splitlines() if l.startswith("PERF")]
+    if own:
+        for fn in os.listdir(wd):
+            os.unlink(os.path.join(wd, fn))
+        os.rmdir(wd)
+    return csvs, errs, (perf[0] if perf else "")
+
+
+def run_merge_split(grid: dict, ms: dict, dt: float, dprops: Dict[str, np.ndarray],
+                    x: np.ndarray, y: np.ndarray, level: np.ndarray, label: np.ndarray):
+    """Runs the reference's adaptive_merge_split on the given state."""
+    np_ = x.shape[0]
+    with tempfile.TemporaryDirectory(prefix="dampm_ms_") as wd:
+        fin = os.path.join(wd, "in.bin")
+        fout = os.path.join(wd, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<ii", grid["Nex"], grid["Ney"]))
+            f.write(struct.pack("<ddd", grid["hx"], grid["hy"], dt))
+            f.write(struct.pack("<dddddd", ms["alpha"], ms["beta"], ms["split_hp_min"],
+                                ms["shear_split"], ms["hp_min"], ms["max_dv"]))
+            f.write(struct.pack("<iiii", ms["min_level"], ms["max_level"],
+                                ms["min_particles_per_cell"], ms["call_interval"]))
+            f.write(struct.pack("<d", ms["max_ops"]))
+            f.write(struct.pack("<ii", np_, len(dprops)))
+            for k, v in dprops.items():
+                kb = k.encode()
+                f.write(struct.pack("<i", len(kb)))
+                f.write(kb)
+                f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(x, dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(y, dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(level, dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(label, dtype="<i4").tobytes())
+        subprocess.run([MS_HARNESS, fin, fout], check=True, capture_output=True)
+        raw = open(fout, "rb").read()
+    pos = 0
+    (n,) = struct.unpack_from("<i", raw, pos)
+    pos += 4
+    out = {}
+    for _ in range(len(dprops)):
+        (ln,) = struct.unpack_from("<i", raw, pos)
+        pos += 4
+        name = raw[pos:pos + ln].decode()
+        pos += ln
+        out[name] = np.frombuffer(raw, dtype="<f8", count=n, offset=pos).copy()
+        pos += 8 * n
+    out["x"] = np.frombuffer(raw, dtype="<f8", count=n, offset=pos).copy()
+    pos += 8 * n
+    out["y"] = np.frombuffer(raw, dtype="<f8", count=n, offset=pos).copy()
+    pos += 8 * n
+    out["level"] = np.frombuffer(raw, dtype="<i4", count=n, offset=pos).astype(np.float64)
+    pos += 4 * n
+    out["label"] = np.frombuffer(raw, dtype="<i4", count=n, offset=pos).astype(np.float64)
+    return out

@@ -1,0 +1,124 @@
+"""Recorded outputs, state round trips and edge cases on the GPU."""
+import numpy as np
+import pytest
+
+from amsc_b200 import scenarios
+from amsc_b200.dampm import STATE_FIELDS, Solver
+from oracle.oracle import Oracle
+
+OUT_FIELDS = ("apx", "apy", "Zp", "hpZ", "dZxp", "dZyp", "Fpx", "Fpy", "Fric_px",
+              "Fric_py", "vpx_dx", "vpx_dy", "vpy_dx", "vpy_dy", "vpxL", "vpyL")
+NODAL = ("Mv", "mom_vx", "mom_vy", "avx", "avy", "vvx", "vvy", "vvxL", "vvyL", "FPxv",
+         "FPyv", "Fric_x", "Fric_y", "F_int_vx", "F_int_vy")
+
+
+@pytest.mark.gpu
+def test_recorded_fields_bitwise(cuda_lib):
+    d = scenarios.bench_slab(1000)
+    o = Oracle(d, threads=4)
+    o.run(7)
+    with Solver(d, record=True) as s:
+        s.step(7)
+        for k in OUT_FIELDS:
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+        for k in NODAL:
+            np.testing.assert_array_equal(s.download_nodal(k), o.nodal(k), err_msg=k)
+
+
+@pytest.mark.gpu
+def test_state_round_trip(cuda_lib):
+    """get_state -> set_state -> step equals stepping through."""
+    d = scenarios.bench_slab(3000)
+    o = Oracle(d, threads=4)
+    o.run(10)
+    with Solver(d) as s:
+        s.step(5)
+        st = s.get_state()
+        s.set_state(st)
+        s.step(5)
+        for k in STATE_FIELDS:
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+
+
+@pytest.mark.gpu
+def test_mudflow_small_adaptive(cuda_lib):
+    """The mudflow workload scaled to 256x256 (Bingham + Voellmy, bumpy
+    terrain, adaptive CFL): 40 steps bitwise."""
+    d = scenarios.mudflow(N=256)
+    o = Oracle(d, threads=8)
+    o.run(40)
+    with Solver(d) as s:
+        s.step(40)
+        st = s.status()
+        assert st["it"] == o.it and st["t"] == o.t
+        for k in ("x", "y", "vpx", "vpy", "hp", "F_11", "F_12", "F_22"):
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+        led = s.ledgers()
+        assert led[6] < 1e-10 and led[7] < 1e-10
+
+
+@pytest.mark.gpu
+def test_edge_pileup_and_walls(cuda_lib):
+    """A pile-up (one cell with 60 particles: cells above 32 particles take
+    the serial per-cell ordering, columns above the P2G batch size are split
+    into batches), particles on the domain walls and an odd grid."""
+    d = scenarios.dam_break_flat(nsteps=20)
+    x, y = d.arrays["x"].copy(), d.arrays["y"].copy()
+    x[:60] = 2.126 + 1e-3 * np.arange(60) / 60
+    y[:60] = 7.9 + 1e-3 * np.arange(60) / 60
+    x[60:700] = 3.9  # one column with ~640 particles
+    y[60:700] = np.linspace(0.01, 15.99, 640)
+    x[700], y[700] = 0.0, 0.0
+    x[701], y[701] = 16.0, 16.0
+    d.arrays["x"], d.arrays["y"] = x, y
+    o = Oracle(d, threads=4)
+    o.run(20)
+    with Solver(d) as s:
+        s.step(20)
+        for k in ("x", "y", "vpx", "vpy", "hp", "F_11", "F_22"):
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+
+
+@pytest.mark.gpu
+def test_odd_grid_and_non_pow2_spacing(cuda_lib):
+    """Lake at rest (hx = 0.2, not a power of two; BC off) on a 50x50 grid and
+    a 37x23 rectangular grid."""
+    d = scenarios.well_balance(T=0.05)
+    o = Oracle(d, threads=4)
+    o.run(1 << 20)
+    with Solver(d) as s:
+        s.run()
+        for k in ("x", "y", "vpx", "vpy", "hp"):
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+    d = scenarios.bench_slab(1000, nsteps=15)
+    d.scalars.update({"Nex": 37, "Ney": 23})
+    n = (37 + 1) * (23 + 1)
+    for k in ("Z", "dZdx", "dZdy"):
+        d.arrays[k] = np.linspace(0, 1, n) if k == "Z" else np.zeros(n)
+    keep = (d.arrays["x"] < 36.5) & (d.arrays["y"] < 22.5)
+    for k in ("x", "y", "Mp", "Ap", "vpx", "vpy", "hp", "mom_px", "mom_py", "Vp"):
+        d.arrays[k] = d.arrays[k][keep]
+    o = Oracle(d, threads=4)
+    o.run(15)
+    with Solver(d) as s:
+        s.step(15)
+        for k in ("x", "y", "vpx", "vpy", "hp", "F_11", "F_22"):
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+
+
+@pytest.mark.gpu
+def test_empty_and_single_particle(cuda_lib):
+    d = scenarios.dam_break_flat(nsteps=5)
+    for k in ("x", "y", "Mp", "Ap", "vpx", "vpy", "hp", "mom_px", "mom_py", "Vp"):
+        d.arrays[k] = d.arrays[k][:1]
+    o = Oracle(d, threads=1)
+    o.run(5)
+    with Solver(d) as s:
+        s.step(5)
+        for k in ("x", "y", "vpx", "hp"):
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+    for k in ("x", "y", "Mp", "Ap", "vpx", "vpy", "hp", "mom_px", "mom_py", "Vp"):
+        d.arrays[k] = d.arrays[k][:0]
+    with Solver(d) as s:
+        s.step(5)
+        assert s.status()["np"] == 0

@@ -1,0 +1,79 @@
+"""The CPU oracle against golden vectors made by the reference project's own
+programs (tests/golden/make_golden.py): main/optim_par.cpp and
+main/merge_split_ops_cmes.h compiled from the reference sources.  Bitwise."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from amsc_b200 import scenarios
+from oracle.oracle import Oracle
+
+G = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<f8").tobytes()).hexdigest()
+
+
+def test_bench1000_columns_bitwise():
+    gold = np.load(os.path.join(G, "optim_par_bench1000.npz"))
+    d = scenarios.bench_slab(1000, nsteps=20)
+    its = sorted({int(k.split("/")[0][2:]) for k in gold.files if k.startswith("it")})
+    assert its == [10, 20]
+    for it in its:
+        o = Oracle(d, threads=1)
+        o.run(it - 1)  # the CSV of iteration `it` is written before its step
+        for k in gold.files:
+            if not k.startswith(f"it{it}/"):
+                continue
+            name = k.split("/", 1)[1]
+            np.testing.assert_array_equal(o.get(name), gold[k], err_msg=f"it{it} {name}")
+    # conservation_errors.csv rows: time, err_mass, err_mom (every step)
+    o = Oracle(d, threads=1)
+    errs = gold["errors"]
+    for step in range(errs.shape[0]):
+        o.run(1)
+        led = o.ledger()
+        np.testing.assert_allclose([led[8], led[6], led[7]], errs[step], rtol=1e-5, atol=0)
+
+
+@pytest.mark.parametrize("case", ["dam_break", "conservation_bump"])
+def test_digests_bitwise(case):
+    import sys
+    sys.path.insert(0, G)
+    from make_golden import golden_cases
+    gold = json.load(open(os.path.join(G, "optim_par_digests.json")))[case]
+    d = golden_cases()[case]
+    for it in (10, 20):
+        o = Oracle(d, threads=2)
+        o.run(it - 1)
+        for key, dg in gold["columns"].items():
+            if key.startswith(f"it{it}/"):
+                assert digest(o.get(key.split("/", 1)[1])) == dg, key
+
+
+def test_merge_split_bitwise():
+    import sys
+    sys.path.insert(0, G)
+    from make_golden import ms_case
+    gold = json.load(open(os.path.join(G, "ms_bench1000.json")))
+    d, state, x, y, level, label, ms = ms_case()
+    inputs = dict(state, x=x, y=y, level=level.astype(np.float64), label=label.astype(np.float64))
+    for k, v in inputs.items():
+        assert digest(v) == gold["in"][k], f"input recipe changed: {k}"
+    for k, v in ms.items():
+        d.scalars["ms_" + k] = v
+    o = Oracle(d, threads=1)
+    for k, v in state.items():
+        o.set(k, v)
+    o.set("x", x)
+    o.set("y", y)
+    o.set("level", level.astype(np.float64))
+    counts = o.merge_split(gold["dt"])
+    assert counts[2] == gold["np_in"] and counts[3] == gold["np_out"]
+    assert counts[0] > 0 and counts[1] > 0  # splits and merges both happened
+    for k, dg in gold["out"].items():
+        assert digest(o.get(k)) == dg, k
