@@ -12,7 +12,7 @@ namespace dampm {
 constexpr int kTR = 32;
 constexpr int kLC = 16;
 constexpr int kP2GThreads = 128;
-constexpr int kCap = 544;
+constexpr int kCap = 512;
 constexpr int kP2GMinBlocks = 2;
 constexpr int kG2PThreads = 256;
 constexpr int kScanTile = 4096;

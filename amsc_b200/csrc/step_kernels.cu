@@ -923,7 +923,7 @@ __global__ void k_ledger_final(const double* __restrict__ led_part, int nparts,
 // cell of the step start, height update, Bingham stress, next cell key and
 // the CFL max-reductions (main/optim_par.cpp:532-651).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kG2PThreads, 2)
+__global__ void __launch_bounds__(kG2PThreads, 3)
     k_g2p(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
           Phys P, Scalars* S, int record, int want_grad) {
   if (!S->active) return;

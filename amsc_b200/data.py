@@ -122,6 +122,12 @@ def _fmt(v) -> str:
     return "%.17g" % float(v)
 
 
+def _fmt_array(a: np.ndarray) -> str:
+    # repr() of a Python float is the shortest string that parses back to
+    # the same double, so the round trip stays exact
+    return ",".join(map(repr, np.asarray(a, dtype=np.float64).tolist()))
+
+
 def to_json(d: DATA, path: str) -> None:
     """Writes DATA.json the way the Octave generators' ``v2j`` does."""
     d.validate()
@@ -130,7 +136,7 @@ def to_json(d: DATA, path: str) -> None:
         items = []
         for k in PARTICLE_KEYS + NODE_KEYS:
             a = d.arrays[k]
-            items.append('"%s": [%s]' % (k, ",".join(_fmt(v) for v in a.tolist())))
+            items.append('"%s": [%s]' % (k, _fmt_array(a)))
         for k, v in d.scalars.items():
             items.append('"%s": %s' % (k, str(int(v)) if k in _INT_KEYS else _fmt(v)))
         f.write(",\n".join(items))

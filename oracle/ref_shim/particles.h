@@ -119,6 +119,13 @@ class particles_t {
   void p2g(std::map<std::string, std::vector<double>>& vars,
            const std::vector<std::string>& pnames,
            const std::vector<std::string>& gnames) const {
+    const size_t nv = pnames.size();
+    std::vector<const double*> src(nv);
+    std::vector<double*> dst(nv);
+    for (size_t v = 0; v < nv; ++v) {
+      src[v] = dprops.at(pnames[v]).data();
+      dst[v] = vars[gnames[v]].data();
+    }
     for (auto const& kv : grd_to_ptcl)
       for (idx_t ip : kv.second) {
         double xi, eta;
@@ -127,8 +134,7 @@ class particles_t {
         for (int inode = 0; inode < 4; ++inode) {
           const double N = shp(xi, eta, inode);
           const idx_t n = gt(inode, r, c);
-          for (size_t v = 0; v < pnames.size(); ++v)
-            vars[gnames[v]][n] += N * dprops.at(pnames[v])[ip];
+          for (size_t v = 0; v < nv; ++v) dst[v][n] += N * src[v][ip];
         }
       }
   }
@@ -138,7 +144,15 @@ class particles_t {
             const std::vector<std::string>& xnames,
             const std::vector<std::string>& ynames, const std::string& wname,
             const std::vector<std::string>& gnames) const {
-    const std::vector<double>& w = dprops.at(wname);
+    const double* w = dprops.at(wname).data();
+    const size_t nv = gnames.size();
+    std::vector<const double*> sx(nv), sy(nv);
+    std::vector<double*> dst(nv);
+    for (size_t v = 0; v < nv; ++v) {
+      sx[v] = dprops.at(xnames[v]).data();
+      sy[v] = dprops.at(ynames[v]).data();
+      dst[v] = vars[gnames[v]].data();
+    }
     for (auto const& kv : grd_to_ptcl)
       for (idx_t ip : kv.second) {
         double xi, eta;
@@ -148,9 +162,8 @@ class particles_t {
           const double Nx = shg(xi, eta, 0, inode, grid.hx(), grid.hy());
           const double Ny = shg(xi, eta, 1, inode, grid.hx(), grid.hy());
           const idx_t n = gt(inode, r, c);
-          for (size_t v = 0; v < gnames.size(); ++v)
-            vars[gnames[v]][n] +=
-                (Nx * dprops.at(xnames[v])[ip] + Ny * dprops.at(ynames[v])[ip]) * w[ip];
+          for (size_t v = 0; v < nv; ++v)
+            dst[v][n] += (Nx * sx[v][ip] + Ny * sy[v][ip]) * w[ip];
         }
       }
   }
@@ -158,6 +171,13 @@ class particles_t {
   void g2p(std::map<std::string, std::vector<double>>& vars,
            const std::vector<std::string>& gnames,
            const std::vector<std::string>& pnames) {
+    const size_t nv = gnames.size();
+    std::vector<const double*> src(nv);
+    std::vector<double*> dst(nv);
+    for (size_t v = 0; v < nv; ++v) {
+      src[v] = vars[gnames[v]].data();
+      dst[v] = dprops[pnames[v]].data();
+    }
     for (idx_t ip = 0; ip < num_particles; ++ip) {
       double xi, eta;
       idx_t r, c;
@@ -165,8 +185,7 @@ class particles_t {
       for (int inode = 0; inode < 4; ++inode) {
         const double N = shp(xi, eta, inode);
         const idx_t n = gt(inode, r, c);
-        for (size_t v = 0; v < gnames.size(); ++v)
-          dprops[pnames[v]][ip] += N * vars[gnames[v]][n];
+        for (size_t v = 0; v < nv; ++v) dst[v][ip] += N * src[v][n];
       }
     }
   }
@@ -175,6 +194,14 @@ class particles_t {
             const std::vector<std::string>& gnames,
             const std::vector<std::string>& dxnames,
             const std::vector<std::string>& dynames) {
+    const size_t nv = gnames.size();
+    std::vector<const double*> src(nv);
+    std::vector<double*> ddx(nv), ddy(nv);
+    for (size_t v = 0; v < nv; ++v) {
+      src[v] = vars[gnames[v]].data();
+      ddx[v] = dprops[dxnames[v]].data();
+      ddy[v] = dprops[dynames[v]].data();
+    }
     for (idx_t ip = 0; ip < num_particles; ++ip) {
       double xi, eta;
       idx_t r, c;
@@ -183,9 +210,9 @@ class particles_t {
         const double Nx = shg(xi, eta, 0, inode, grid.hx(), grid.hy());
         const double Ny = shg(xi, eta, 1, inode, grid.hx(), grid.hy());
         const idx_t n = gt(inode, r, c);
-        for (size_t v = 0; v < gnames.size(); ++v) {
-          dprops[dxnames[v]][ip] += Nx * vars[gnames[v]][n];
-          dprops[dynames[v]][ip] += Ny * vars[gnames[v]][n];
+        for (size_t v = 0; v < nv; ++v) {
+          ddx[v][ip] += Nx * src[v][n];
+          ddy[v][ip] += Ny * src[v][n];
         }
       }
     }
