@@ -137,7 +137,8 @@ int alloc_particles(dampm_ctx* ctx, long long cap) {
                   &p.F11,   &p.F12,   &p.F22,    &p.Mp,     &p.Vp,
                   &p.H,     &p.Ap,    &p.mpx,    &p.mpy,    &p.Fbx,
                   &p.Fby,   &p.vpx_dx, &p.vpx_dy, &p.vpy_dx, &p.vpy_dy,
-                  &p.xp,    &p.yp,    &p.qfx,    &p.qfy,    &p.qwb};
+                  &p.xp,    &p.yp,    &p.qfx,    &p.qfy,    &p.qxi,
+                  &p.qeta,  &p.qgx,   &p.qgy};
   for (double** q : f) {
     int rc = dalloc(ctx, q, cap);
     if (rc) return rc;
@@ -189,7 +190,7 @@ int enqueue_pass(dampm_ctx* ctx) {
   if (ms_due) {
     enqueue_sort(ctx);
     ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc,
-                                ctx->G, ctx->P, ctx->ms, ctx->S, ctx->cap,
+                                ctx->G, ctx->P, ctx->Z, ctx->ms, ctx->S, ctx->cap,
                                 ctx->stream, /*use_step_dt=*/1, 0.0);
     k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(
         ctx->p.x, ctx->p.y, ctx->p.key, ctx->G, ctx->S);
@@ -210,8 +211,8 @@ int enqueue_pass(dampm_ctx* ctx) {
       cudaMemsetAsync(q, 0, sizeof(double) * ctx->nn, ctx->stream);
   }
   k_p2g<<<ctx->p2g_grid, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
-      ctx->p, ctx->perm, ctx->start, ctx->Z, ctx->nodes, ctx->led_part, ctx->G,
-      ctx->P, ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount, ctx->strips);
+      ctx->p, ctx->perm, ctx->start, ctx->nodes, ctx->led_part, ctx->G, ctx->P,
+      ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount, ctx->strips);
   ctx->launches += 2;
   ev_mark(ctx, 3);
   k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->n_led, ctx->S);
@@ -357,7 +358,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   ctx->n_led = ctx->strips * ctx->chunks;
   rc = rc ? rc : dalloc(ctx, &ctx->led_part, size_t(ctx->n_led) * 6);
   rc = rc ? rc : dalloc(ctx, &ctx->ulist, size_t(ctx->n_led));
-  rc = rc ? rc : dalloc(ctx, &ctx->ucount, 1);
+  rc = rc ? rc : dalloc(ctx, &ctx->ucount, 2);
   rc = rc ? rc : dalloc(ctx, &ctx->S, 1);
   if (rc == DAMPM_OK) {
     if (cudaMallocHost(&ctx->Sh, sizeof(Scalars)) != cudaSuccess) rc = DAMPM_ERR_CUDA;
@@ -453,7 +454,8 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
   if (np > 0) {
     k_init_particles<<<grid_for(np, 256), 256, 0, ctx->stream>>>(
         p, ctx->Z, ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np));
-    k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, 0);
+    k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->Z, ctx->G, ctx->P,
+                                                       ctx->S, 0);
     CK(cudaGetLastError());
   }
   ctx->it_host = 0;
@@ -542,7 +544,7 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
   CK(cudaStreamSynchronize(ctx->stream));
   enqueue_sort(ctx);
   ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
-             ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt);
+             ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt);
   k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.x, ctx->p.y,
                                                            ctx->p.key, ctx->G, ctx->S);
   CK(cudaGetLastError());
@@ -697,7 +699,8 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
                      ctx->stream));
   k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.x, p.y, p.key, ctx->G, ctx->S);
   k_reduce_state<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->S);
-  k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, fresh ? 0 : 1);
+  k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->Z, ctx->G, ctx->P,
+                                                     ctx->S, fresh ? 0 : 1);
   CK(cudaGetLastError());
   return DAMPM_OK;
 }

@@ -6,12 +6,12 @@
 
 namespace dampm {
 
-// P2G tiling: kTR node rows per strip (one lane per row in each of the four
-// quantity-group warps), kLC node
+// P2G tiling: kTR node rows per strip (one lane per row in each of the eight
+// warps: four quantity groups x {finishing, starting} chains), kLC node
 // columns per chunk, particle records staged in shared memory kCap at a time.
-constexpr int kTR = 32;
+constexpr int kTR = 30;
 constexpr int kLC = 16;
-constexpr int kP2GThreads = 128;
+constexpr int kP2GThreads = 256;
 constexpr int kCap = 512;
 constexpr int kP2GMinBlocks = 2;
 constexpr int kG2PThreads = 256;
@@ -23,11 +23,15 @@ struct Particles {
   // persistent state
   double *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
   int *label, *level, *key;
-  // inputs of the next P2G, as the reference stores them at the end of a
-  // step (main/optim_par.cpp:600-626): momentum mom = v*Mp, friction force
-  // Fric = Ap*Fb and the well-balance factor 1 - H/hp; written by G2P (or
-  // by k_prep after an upload, a state upload or a merge/split)
-  double *mpx, *mpy, *qfx, *qfy, *qwb;
+  // the record the next P2G transfers, written by G2P (or by k_prep after an
+  // upload, a state upload or a merge/split):
+  //   mpx, mpy  momentum v*Mp and qfx, qfy friction force Ap*Fb, as the
+  //             reference stores them at the end of a step
+  //             (main/optim_par.cpp:456-459,600-626);
+  //   qxi, qeta local coordinates in the cell of the next binning;
+  //   qgx, qgy  gravity force -g*Vp*rho*grad(Z)*(1 - H/hp) there
+  //             (main/optim_par.cpp:387,447-454).
+  double *mpx, *mpy, *qfx, *qfy, *qxi, *qeta, *qgx, *qgy;
   // Ap and Fb as stored at upload / merge/split (valid while Scalars::fresh
   // is set; otherwise they are derived from the state)
   double *Ap, *Fbx, *Fby;
@@ -54,7 +58,8 @@ __global__ void k_init_particles(Particles p, const double* Z,
 __global__ void k_keys(const double* x, const double* y, int* key, Geom G,
                        const Scalars* S);
 __global__ void k_reduce_state(Particles p, Scalars* S);
-__global__ void k_prep(Particles p, Phys P, const Scalars* S, int derive);
+__global__ void k_prep(Particles p, const double* Z, Geom G, Phys P,
+                       const Scalars* S, int derive);
 __global__ void k_count(const int* key, int* count, int* slot,
                         const Scalars* S);
 __global__ void k_scan_tiles(const int* count, int n, int* tile_sum,
@@ -72,8 +77,8 @@ __global__ void k_units(const int* cstart, int strips, int chunks, int* ulist,
                         int* ucount, double* led_part, Geom G, const Scalars* S);
 __global__ void k_units_reset(int* ucount, const Scalars* S);
 __global__ void k_p2g(Particles p, const int* perm, const int* cstart,
-                      const double* Z, Nodes nodes, double* led_part, Geom G,
-                      Phys P, const Scalars* S, int record, const int* ulist,
+                      Nodes nodes, double* led_part, Geom G, Phys P,
+                      const Scalars* S, int record, const int* ulist,
                       const int* ucount, int strips);
 __global__ void k_ledger_final(const double* led_part, int nparts, Scalars* S);
 __global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,

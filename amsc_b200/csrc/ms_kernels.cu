@@ -401,9 +401,9 @@ int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
 }  // namespace
 
 int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
-               int ncells, Geom G, Phys P, const dampm_ms_params& cfg,
-               Scalars* S, long long cap, cudaStream_t st, int use_step_dt,
-               double dt) {
+               int ncells, Geom G, Phys P, const double* Z,
+               const dampm_ms_params& cfg, Scalars* S, long long cap,
+               cudaStream_t st, int use_step_dt, double dt) {
   MsCfg c{};
   c.alpha = cfg.alpha;
   c.beta = cfg.beta;
@@ -453,7 +453,7 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
   k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
-  k_prep<<<gp, 256, 0, st>>>(p, P, S, 0);
+  k_prep<<<gp, 256, 0, st>>>(p, Z, G, P, S, 0);
   n += 4;
   return n;
 }

@@ -46,8 +46,8 @@ int ms_alloc(MsBuffers& m, long long cap, int /*ncells*/, Alloc alloc) {
 // describe the current positions).  dt comes from the step's device scalar
 // when use_step_dt, else `dt`.  Returns the number of kernel launches.
 int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
-               int ncells, Geom G, Phys P, const dampm_ms_params& cfg,
-               Scalars* S, long long cap, cudaStream_t stream, int use_step_dt,
-               double dt);
+               int ncells, Geom G, Phys P, const double* Z,
+               const dampm_ms_params& cfg, Scalars* S, long long cap,
+               cudaStream_t stream, int use_step_dt, double dt);
 
 }  // namespace dampm

@@ -159,11 +159,35 @@ __global__ void k_reduce_state(Particles p, Scalars* S) {
   }
 }
 
-// Inputs of the next P2G from the stored Ap/Fb/mom (derive == 0: after an
-// upload or a merge/split) or from the state alone (derive != 0), exactly as
-// the reference computes them at the end of a step
-// (main/optim_par.cpp:447-459,600-626).
-__global__ void k_prep(Particles p, Phys P, const Scalars* S, int derive) {
+// Record of the next P2G for every particle (see Particles): from the stored
+// Ap/Fb/mom (derive == 0: after an upload or a merge/split) or from the state
+// alone (derive != 0), exactly as the reference computes these values
+// (main/optim_par.cpp:387,447-459,600-626).
+__device__ __forceinline__ void next_record(const Geom& G, const Phys& P,
+                                            const double* __restrict__ Z,
+                                            double x, double y, double hp,
+                                            double H, double Vp, double& xi,
+                                            double& eta, double& gx, double& gy) {
+  const int r = cell_row(y, G.hy, G.nrows), c = cell_col(x, G.hx, G.ncols);
+  const double ihx = 1.0 / G.hx, mihx = -1.0 / G.hx;
+  const double ihy = 1.0 / G.hy, mihy = -1.0 / G.hy;
+  local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
+  // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
+  double dzx = 0.0, dzy = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double zn = Z[node_of(k, c, r, G.nrows)];
+    dzx += shg_x(eta, k, ihx, mihx) * zn;
+    dzy += shg_y(xi, k, ihy, mihy) * zn;
+  }
+  // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
+  const double wb = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
+  gx = -P.g * Vp * P.rho * dzx * wb;
+  gy = -P.g * Vp * P.rho * dzy * wb;
+}
+
+__global__ void k_prep(Particles p, const double* __restrict__ Z, Geom G,
+                       Phys P, const Scalars* S, int derive) {
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
@@ -181,8 +205,12 @@ __global__ void k_prep(Particles p, Phys P, const Scalars* S, int derive) {
     }
     p.qfx[i] = Ap * fbx;
     p.qfy[i] = Ap * fby;
-    const double H = p.H[i];
-    p.qwb[i] = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
+    double xi, eta, gx, gy;
+    next_record(G, P, Z, p.x[i], p.y[i], hp, p.H[i], p.Vp[i], xi, eta, gx, gy);
+    p.qxi[i] = xi;
+    p.qeta[i] = eta;
+    p.qgx[i] = gx;
+    p.qgy[i] = gy;
   }
 }
 
@@ -378,47 +406,35 @@ __global__ void k_segment_order(const int* __restrict__ start,
 // Work unit: node rows [r0, r0+kTR) of one strip x node columns [cA, cB) of
 // one chunk; the unit walks the cell columns cA-1 .. cB-1.  For cell column cc
 // the particles of cells (rlo..rhi, cc) are one contiguous range of the sorted
-// order.  Per column:
-//   gather  : the particle fields of the range (through the sorted index) and
-//             the column's terrain strip are copied into shared staging with
-//             cp.async, one column ahead -- the gathers of column cc+1 fly
-//             while column cc is computed;
-//   records : local coordinates and the nine transferred quantities per
-//             particle, computed once from the staging (SoA, swizzled);
-//   chains  : node row r is served by lane r of each of the four warps, which
-//             walk the particles of cells (r-1, cc) then (r, cc) and extend two
-//             chains per quantity:
-//               fin   : node (r, cc)   -- local node 1 of cell (r-1,cc), then
-//                       0 of (r,cc); it already holds cells (r-1,cc-1),
-//                       (r,cc-1) from the previous column;
-//               start : node (r, cc+1) -- local node 3 of cell (r-1,cc), then
-//                       2 of (r,cc).
-//             That is each node's contributions in quadgrid's cell-sweep
-//             order, so every nodal sum equals the reference's sequential sum
-//             bit for bit.  The warps split the quantities (warp-uniform
-//             code): g0 {Mv, mom_x, mom_y}, g1 {FPx, FPy, Fric_x},
-//             g2 {Fric_y, Fint_x}, g3 {Fint_y};
-//   nodal   : warp 0 collects the finished chains and applies the nodal
-//             update (momentum, velocity, walls) to node column cc.
-// A column whose range exceeds kCap (pile-ups) is processed in synchronous
-// batches instead.
+// order, processed in batches of at most kCap particles.  Each particle's
+// record (local coordinates and the nine transferred quantities, built by the
+// previous step's G2P) is copied with cp.async into one of two shared-memory
+// buffers: the copies of batch k+1 fly while batch k is transferred, and the
+// sorted indices of batch k+2 are loaded meanwhile.
+//
+// Node row r is served by lane r of eight warps: four quantity groups
+// (warp-uniform code) g0 {Mv, mom_x, mom_y}, g1 {FPx, FPy, Fric_x},
+// g2 {Fric_y, Fint_x}, g3 {Fint_y}, each for two chains:
+//   fin   (warps 0-3): node (r, cc)   -- local node 1 of cell (r-1,cc), then 0
+//         of (r,cc); it already holds cells (r-1,cc-1), (r,cc-1);
+//   start (warps 4-7): node (r, cc+1) -- local node 3 of cell (r-1,cc), then 2
+//         of (r,cc).
+// That is each node's contributions in quadgrid's cell-sweep order, so every
+// nodal sum equals the reference's sequential sum bit for bit.  At the end of
+// a column warp 0 applies the nodal update to node column cc and the started
+// chains move to the finishing warps.  Records are stored SoA with an XOR
+// swizzle of the low four index bits so that lanes of consecutive rows
+// (records ~ppc apart) hit distinct banks.
 // ---------------------------------------------------------------------------
 namespace {
 
+constexpr int kRec = 13;  // xi eta Mp mpx mpy FPx FPy Frx Fry F11 F12 F22 Vp
+constexpr int kPf = (kCap + kP2GThreads - 1) / kP2GThreads;
+
 struct P2GSmem {
-  // records
-  double xi[kCap], eta[kCap], Mp[kCap], mpx[kCap], mpy[kCap], Fpx[kCap],
-      Fpy[kCap], Frx[kCap], Fry[kCap], F11[kCap], F12[kCap], F22[kCap],
-      Vp[kCap];
-  // gather staging (cp.async destination)
-  double gx[kCap], gy[kCap], gMp[kCap], gVp[kCap], gmx[kCap], gmy[kCap],
-      gfx[kCap], gfy[kCap], gwb[kCap], gF11[kCap], gF12[kCap], gF22[kCap];
-  int gkey[kCap];
-  int gidx[kCap];
-  double zs[2][kTR + 2];  // Z at node rows rlo.., node columns cc and cc+1
+  double rec[2][kRec][kCap];
   int rowstart[3][kTR + 2];
-  double xfin[6][kTR];  // finished chains of warps 1-3, read by warp 0
-  double xst[6][kTR];
+  double xch[2][9][kTR];  // finished [0] / started [1] chains per quantity
   double led[6][kP2GThreads / 32];
 };
 
@@ -428,10 +444,6 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
@@ -439,12 +451,59 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// (x - c*h)/h; when h is a power of two the quotient equals the product with
-// 1/h exactly, so the division is skipped.
-__device__ __forceinline__ double local1(double x, int c, double h, double ih,
-                                         bool pow2) {
-  const double d = x - c * h;
-  return pow2 ? d * ih : d / h;
+struct Batch {
+  int cc, bb, be;
+  bool valid;
+};
+
+// the batch after b: the rest of its column, else the start of the next one
+__device__ __forceinline__ Batch next_batch(const Batch& b, const P2GSmem& s,
+                                            int nrs, int ccLast) {
+  Batch n{0, 0, 0, false};
+  if (!b.valid) return n;
+  const int seg1 = s.rowstart[b.cc % 3][nrs - 1];
+  if (b.be < seg1) return Batch{b.cc, b.be, min(b.be + kCap, seg1), true};
+  if (b.cc + 1 > ccLast) return n;
+  const int s0 = s.rowstart[(b.cc + 1) % 3][0];
+  const int s1 = s.rowstart[(b.cc + 1) % 3][nrs - 1];
+  return Batch{b.cc + 1, s0, min(s0 + kCap, s1), true};
+}
+
+__device__ __forceinline__ void load_perm(int (&pf)[kPf],
+                                          const int* __restrict__ perm,
+                                          const Batch& b) {
+#pragma unroll
+  for (int u = 0; u < kPf; ++u) {
+    const int j = b.bb + threadIdx.x + u * kP2GThreads;
+    pf[u] = (b.valid && j < b.be) ? perm[j] : 0;
+  }
+}
+
+__device__ __forceinline__ void issue_gather(P2GSmem& s, int buf,
+                                             const Particles& p,
+                                             const int (&pf)[kPf],
+                                             const Batch& b) {
+#pragma unroll
+  for (int u = 0; u < kPf; ++u) {
+    const int j = b.bb + threadIdx.x + u * kP2GThreads;
+    if (j >= b.be) break;
+    const int i = pf[u];
+    const int l = swz(j - b.bb);
+    cp_async8(&s.rec[buf][0][l], p.qxi + i);
+    cp_async8(&s.rec[buf][1][l], p.qeta + i);
+    cp_async8(&s.rec[buf][2][l], p.Mp + i);
+    cp_async8(&s.rec[buf][3][l], p.mpx + i);
+    cp_async8(&s.rec[buf][4][l], p.mpy + i);
+    cp_async8(&s.rec[buf][5][l], p.qgx + i);
+    cp_async8(&s.rec[buf][6][l], p.qgy + i);
+    cp_async8(&s.rec[buf][7][l], p.qfx + i);
+    cp_async8(&s.rec[buf][8][l], p.qfy + i);
+    cp_async8(&s.rec[buf][9][l], p.F11 + i);
+    cp_async8(&s.rec[buf][10][l], p.F12 + i);
+    cp_async8(&s.rec[buf][11][l], p.F22 + i);
+    cp_async8(&s.rec[buf][12][l], p.Vp + i);
+  }
+  cp_async_commit();
 }
 
 // Nodal momentum, velocity and wall conditions of node (r, nc) from its nine
@@ -499,341 +558,72 @@ __device__ __forceinline__ void nodal_update(
   }
 }
 
-// one particle contribution to the chains of quantity group kG:
-//   upper = cell r-1 (fin: local 1, start: local 3)
-//   lower = cell r   (fin: local 0, start: local 2)
-template <int kG>
-__device__ __forceinline__ void chain_step(double (&fn)[3], double (&st)[3],
-                                           const P2GSmem& s, int l, bool upper,
-                                           double ihx, double mihx, double ihy,
-                                           double mihy) {
-  const double xi = s.xi[l], eta = s.eta[l];
-  const double omx = 1.0 - xi;
+struct Shape {
+  double ihx, mihx, ihy, mihy;
+};
+
+// One particle's contribution to the chains of quantity group kG; kStart
+// selects the chain (fin: local 1/0, start: local 3/2), `upper` the cell
+// (r-1: local 1/3, r: local 0/2).  With fa = (1-xi) or xi, fb = eta or
+// (1-eta):  N = fa*fb,  Nx = (mihx or ihx)*fb,  Ny = fa*(ihy or mihy) --
+// shp/shg of main/gpu_kernels.cpp:33-59 for that local node.
+template <int kG, bool kStart>
+__device__ __forceinline__ void chain_step(double (&a)[3], const P2GSmem& s,
+                                           int buf, int l, bool upper,
+                                           const Shape& sh) {
+  const double xi = s.rec[buf][0][l], eta = s.rec[buf][1][l];
+  const double fa = kStart ? xi : (1.0 - xi);
   const double fb = upper ? eta : (1.0 - eta);
-  const double Nf = omx * fb, Ns = xi * fb;
+  const double N = fa * fb;
   if (kG == 0) {
-    const double q0 = s.Mp[l], q1 = s.mpx[l], q2 = s.mpy[l];
-    fn[0] += Nf * q0; fn[1] += Nf * q1; fn[2] += Nf * q2;
-    st[0] += Ns * q0; st[1] += Ns * q1; st[2] += Ns * q2;
+    const double q0 = s.rec[buf][2][l], q1 = s.rec[buf][3][l], q2 = s.rec[buf][4][l];
+    a[0] += N * q0;
+    a[1] += N * q1;
+    a[2] += N * q2;
   } else if (kG == 1) {
-    const double q0 = s.Fpx[l], q1 = s.Fpy[l], q2 = s.Frx[l];
-    fn[0] += Nf * q0; fn[1] += Nf * q1; fn[2] += Nf * q2;
-    st[0] += Ns * q0; st[1] += Ns * q1; st[2] += Ns * q2;
+    const double q0 = s.rec[buf][5][l], q1 = s.rec[buf][6][l], q2 = s.rec[buf][7][l];
+    a[0] += N * q0;
+    a[1] += N * q1;
+    a[2] += N * q2;
   } else {
-    // upper: fin local 1 -> Nx = mihx*eta,     Ny = (1-xi)*ihy
-    //        start local 3 -> Nx = ihx*eta,    Ny = xi*ihy
-    // lower: fin local 0 -> Nx = mihx*(1-eta), Ny = (1-xi)*mihy
-    //        start local 2 -> Nx = ihx*(1-eta), Ny = xi*mihy
-    const double Nxf = mihx * fb, Nxs = ihx * fb;
-    const double gy = upper ? ihy : mihy;
-    const double Nyf = omx * gy, Nys = xi * gy;
-    const double f11 = s.F11[l], f12 = s.F12[l], f22 = s.F22[l], vp = s.Vp[l];
+    const double Nx = (kStart ? sh.ihx : sh.mihx) * fb;
+    const double Ny = fa * (upper ? sh.ihy : sh.mihy);
+    const double f12 = s.rec[buf][10][l], vp = s.rec[buf][12][l];
     if (kG == 2) {
-      const double q0 = s.Fry[l];
-      fn[0] += Nf * q0;
-      st[0] += Ns * q0;
-      fn[1] += (Nxf * f11 + Nyf * f12) * vp;
-      st[1] += (Nxs * f11 + Nys * f12) * vp;
+      const double q0 = s.rec[buf][8][l], f11 = s.rec[buf][9][l];
+      a[0] += N * q0;
+      a[1] += (Nx * f11 + Ny * f12) * vp;
     } else {
-      fn[0] += (Nxf * f12 + Nyf * f22) * vp;
-      st[0] += (Nxs * f12 + Nys * f22) * vp;
+      const double f22 = s.rec[buf][11][l];
+      a[0] += (Nx * f12 + Ny * f22) * vp;
     }
   }
 }
 
-template <int kG>
-__device__ __forceinline__ void chain_range(double (&fn)[3], double (&st)[3],
-                                            const P2GSmem& s, int a0, int a1,
-                                            int b0, int b1, int bb, int be,
-                                            double ihx, double mihx,
-                                            double ihy, double mihy) {
-  for (int j = max(a0, bb); j < min(a1, be); ++j)
-    chain_step<kG>(fn, st, s, swz(j - bb), true, ihx, mihx, ihy, mihy);
-  for (int j = max(b0, bb); j < min(b1, be); ++j)
-    chain_step<kG>(fn, st, s, swz(j - bb), false, ihx, mihx, ihy, mihy);
-}
-
-struct RecArgs {
-  double hx, hy, ihx, mihx, ihy, mihy;
-  bool px2, py2;
-  int record;
-};
-
-// record of one particle from its gathered fields; z[k] = Z at local node k
-__device__ __forceinline__ void make_record(
-    P2GSmem& s, int lj, int i, int cc, int pr, double x, double y, double Mp,
-    double Vp, double mpx, double mpy, double qfx, double qfy, double wb,
-    double F11, double F12, double F22, const double (&z)[4],
-    const Particles& p, const Phys& P, const RecArgs& a, bool owned,
-    double& lp0, double& lp1, double& lp2) {
-  const double xi = local1(x, cc, a.hx, a.ihx, a.px2);
-  const double eta = local1(y, pr, a.hy, a.ihy, a.py2);
-  // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
-  double dzx = 0.0, dzy = 0.0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    dzx += shg_x(eta, k, a.ihx, a.mihx) * z[k];
-    dzy += shg_y(xi, k, a.ihy, a.mihy) * z[k];
+// The particles of cells (r-1, cc) and (r, cc) are the adjacent ranges
+// [a0, a1) and [a1, b1) of the sorted order: one walk in order.
+template <int kG, bool kStart>
+__device__ __forceinline__ void chain_range(double (&a)[3], const P2GSmem& s,
+                                            int buf, int a0, int a1, int b1,
+                                            int bb, int be, const Shape& sh,
+                                            bool own, double& lp0, double& lp1,
+                                            double& lp2) {
+  const int j1 = min(b1, be);
+  int j = max(a0, bb);
+#pragma unroll 2
+  for (; j < j1; ++j) {
+    const int l = swz(j - bb);
+    const bool upper = j < a1;
+    chain_step<kG, kStart>(a, s, buf, l, upper, sh);
+    if (kG == 0 && !kStart && own && !upper) {  // particle ledger, once each
+      lp0 += s.rec[buf][2][l];
+      lp1 += s.rec[buf][3][l];
+      lp2 += s.rec[buf][4][l];
+    }
   }
-  // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
-  const double Fpx = -P.g * Vp * P.rho * dzx * wb;
-  const double Fpy = -P.g * Vp * P.rho * dzy * wb;
-  const int l = swz(lj);
-  s.xi[l] = xi;
-  s.eta[l] = eta;
-  s.Mp[l] = Mp;
-  s.mpx[l] = mpx;
-  s.mpy[l] = mpy;
-  s.Fpx[l] = Fpx;
-  s.Fpy[l] = Fpy;
-  s.Frx[l] = qfx;
-  s.Fry[l] = qfy;
-  s.F11[l] = F11;
-  s.F12[l] = F12;
-  s.F22[l] = F22;
-  s.Vp[l] = Vp;
-  if (a.record) {
-    p.dZxp[i] = dzx;
-    p.dZyp[i] = dzy;
-    p.Fpx[i] = Fpx;
-    p.Fpy[i] = Fpy;
-    p.Frx[i] = qfx;
-    p.Fry[i] = qfy;
-  }
-  if (owned) {  // particle ledger, once per particle
-    lp0 += Mp;
-    lp1 += mpx;
-    lp2 += mpy;
-  }
-}
-
-constexpr int kPf = (kCap + kP2GThreads - 1) / kP2GThreads;
-
-// Loads the sorted indices of the range [j0, j1) into registers (issued a
-// batch ahead so that the gathers that depend on them do not wait).
-__device__ __forceinline__ void load_perm(int (&pf)[kPf],
-                                          const int* __restrict__ perm, int j0,
-                                          int j1) {
-#pragma unroll
-  for (int u = 0; u < kPf; ++u) {
-    const int j = j0 + threadIdx.x + u * kP2GThreads;
-    pf[u] = (j < j1) ? perm[j] : 0;
-  }
-}
-
-// Issues the cp.async gathers of the range [j0, j1) (<= kCap particles,
-// sorted indices in pf) and of the terrain strip of column cc.
-__device__ __forceinline__ void issue_gather(P2GSmem& s, const Particles& p,
-                                             const int (&pf)[kPf],
-                                             const double* __restrict__ Z,
-                                             int j0, int j1, int cc, int rlo,
-                                             int rhi, int nrows, int ncols) {
-#pragma unroll
-  for (int u = 0; u < kPf; ++u) {
-    const int j = j0 + threadIdx.x + u * kP2GThreads;
-    if (j >= j1) break;
-    const int i = pf[u];
-    const int l = j - j0;
-    s.gidx[l] = i;
-    cp_async8(&s.gx[l], p.x + i);
-    cp_async8(&s.gy[l], p.y + i);
-    cp_async8(&s.gMp[l], p.Mp + i);
-    cp_async8(&s.gVp[l], p.Vp + i);
-    cp_async8(&s.gmx[l], p.mpx + i);
-    cp_async8(&s.gmy[l], p.mpy + i);
-    cp_async8(&s.gfx[l], p.qfx + i);
-    cp_async8(&s.gfy[l], p.qfy + i);
-    cp_async8(&s.gwb[l], p.qwb + i);
-    cp_async8(&s.gF11[l], p.F11 + i);
-    cp_async8(&s.gF12[l], p.F12 + i);
-    cp_async8(&s.gF22[l], p.F22 + i);
-    cp_async4(&s.gkey[l], p.key + i);
-  }
-  const int nz = rhi + 2 - rlo;  // node rows rlo .. rhi+1
-  for (int q = threadIdx.x; q < 2 * nz; q += kP2GThreads) {
-    const int col = q / nz, rr = q - col * nz;
-    const int nc = min(cc + col, ncols);
-    cp_async8(&s.zs[col][rr], Z + (rlo + rr) + nc * (nrows + 1));
-  }
-  cp_async_commit();
 }
 
 }  // namespace
-
-__device__ __forceinline__ void p2g_unit(
-    const Particles& p, const int* __restrict__ perm,
-    const int* __restrict__ cstart, const double* __restrict__ Z,
-    const Nodes& nodes, double* __restrict__ led_part, const Geom& G,
-    const Phys& P, const Scalars* S, int record, P2GSmem& s, int unit,
-    int strips) {
-  const int nrows = G.nrows, ncols = G.ncols;
-  const int r0 = (unit % strips) * kTR;
-  const int cA = (unit / strips) * kLC;
-  const int cB = min(cA + kLC, ncols + 1);
-  const int rlo = max(r0 - 1, 0);
-  const int rhi = min(r0 + kTR - 1, nrows - 1);
-  const int ccFirst = max(cA - 1, 0);
-  const int ccLast = min(cB - 1, ncols - 1);
-  const int nrs = rhi - rlo + 2;  // row starts per column
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
-  // chain lanes: warp = quantity group (warp-uniform code), lane = node row
-  const int grp = warp;
-  const int row = lane;
-  const int r = r0 + row;
-  const bool row_ok = (r <= nrows);
-  const double dt = S->dt;
-  RecArgs ra;
-  ra.hx = G.hx;
-  ra.hy = G.hy;
-  ra.ihx = 1.0 / G.hx;
-  ra.mihx = -1.0 / G.hx;
-  ra.ihy = 1.0 / G.hy;
-  ra.mihy = -1.0 / G.hy;
-  ra.px2 = G.hx_pow2 != 0;
-  ra.py2 = G.hy_pow2 != 0;
-  ra.record = record;
-
-  double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
-  double fn[3] = {0, 0, 0}, st[3] = {0, 0, 0};
-
-  // The unit is processed as a sequence of batches: each cell column's range
-  // split into pieces of at most kCap particles.  The gathers of batch k+1
-  // are issued (cp.async) before the chains of batch k run.
-  //
-  // prologue: row starts of the first two columns, gather of the first batch
-  for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
-    const int k = q / nrs, rr = q - k * nrs;
-    const int cc = ccFirst + k;
-    if (cc <= ccLast) s.rowstart[cc % 3][rr] = cstart[rlo + rr + cc * nrows];
-  }
-  __syncthreads();
-  int pf[kPf];
-  int cc = ccFirst;
-  int bb = s.rowstart[cc % 3][0];
-  int be = min(bb + kCap, s.rowstart[cc % 3][nrs - 1]);
-  load_perm(pf, perm, bb, be);
-  issue_gather(s, p, pf, Z, bb, be, cc, rlo, rhi, nrows, ncols);
-  int a0 = 0, a1 = 0, b0 = 0, b1 = 0;  // my rows' ranges in column cc
-
-  while (true) {
-    const int cbase = cc * nrows;
-    const int* R = s.rowstart[cc % 3];
-    const int seg0 = R[0], seg1 = R[nrs - 1];
-    const bool first_of_col = (bb == seg0);
-    const bool last_of_col = (be == seg1);
-    // the next batch: rest of this column, else the first of the next one
-    int ncc = cc, nbb = be, nbe = 0;
-    bool has_next = true;
-    if (last_of_col) {
-      ncc = cc + 1;
-      if (ncc > ccLast) {
-        has_next = false;
-      } else {
-        nbb = s.rowstart[ncc % 3][0];
-      }
-    }
-    if (has_next) {
-      const int nseg1 = s.rowstart[ncc % 3][nrs - 1];
-      nbe = min(nbb + kCap, nseg1);
-      load_perm(pf, perm, nbb, nbe);
-    }
-    // row starts two columns ahead: loaded now, stored at the column's end
-    int rs2 = 0;
-    const bool has_rs2 = last_of_col && cc + 2 <= ccLast && tid < nrs;
-    if (has_rs2) rs2 = cstart[rlo + tid + (cc + 2) * nrows];
-    if (first_of_col) {
-      a0 = a1 = b0 = b1 = 0;
-      if (row_ok && r - 1 >= rlo && r - 1 <= rhi) {
-        a0 = R[r - 1 - rlo];
-        a1 = R[r - rlo];
-      }
-      if (row_ok && r >= rlo && r <= rhi) {
-        b0 = R[r - rlo];
-        b1 = R[r - rlo + 1];
-      }
-    }
-
-    cp_async_wait_all();
-    __syncthreads();  // gathers of this batch visible to all threads
-    for (int j = bb + tid; j < be; j += kP2GThreads) {
-      const int lj = j - bb;
-      const int pr = s.gkey[lj] - cbase;
-      const int zr = pr - rlo;
-      const double z[4] = {s.zs[0][zr], s.zs[0][zr + 1], s.zs[1][zr], s.zs[1][zr + 1]};
-      make_record(s, lj, s.gidx[lj], cc, pr, s.gx[lj], s.gy[lj], s.gMp[lj], s.gVp[lj],
-                  s.gmx[lj], s.gmy[lj], s.gfx[lj], s.gfy[lj], s.gwb[lj], s.gF11[lj],
-                  s.gF12[lj], s.gF22[lj], z, p, P, ra,
-                  pr >= r0 && pr < r0 + kTR && cc >= cA, lp0, lp1, lp2);
-    }
-    __syncthreads();  // records complete, staging free
-    if (has_next) issue_gather(s, p, pf, Z, nbb, nbe, ncc, rlo, rhi, nrows, ncols);
-    switch (grp) {
-      case 0: chain_range<0>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-      case 1: chain_range<1>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-      case 2: chain_range<2>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-      default: chain_range<3>(fn, st, s, a0, a1, b0, b1, bb, be, ra.ihx, ra.mihx, ra.ihy, ra.mihy); break;
-    }
-
-    if (last_of_col) {
-      // ---- nodal update of the finished nodes (warp 0) -------------------
-      // g1: FPx FPy Frx | g2: Fry Fix | g3: Fiy
-      if (grp == 1) {
-        s.xfin[0][row] = fn[0]; s.xfin[1][row] = fn[1]; s.xfin[2][row] = fn[2];
-        s.xst[0][row] = st[0]; s.xst[1][row] = st[1]; s.xst[2][row] = st[2];
-      } else if (grp == 2) {
-        s.xfin[3][row] = fn[0]; s.xfin[4][row] = fn[1];
-        s.xst[3][row] = st[0]; s.xst[4][row] = st[1];
-      } else if (grp == 3) {
-        s.xfin[5][row] = fn[0];
-        s.xst[5][row] = st[0];
-      }
-      if (has_rs2) s.rowstart[(cc + 2) % 3][tid] = rs2;
-      __syncthreads();
-      if (grp == 0) {
-        const bool do_fin = (cc >= cA) && row_ok;
-        const bool do_last = (cc == ncols - 1) && (cB == ncols + 1) && row_ok;
-        if (do_fin)
-          nodal_update(fn[0], fn[1], fn[2], s.xfin[0][row], s.xfin[1][row],
-                       s.xfin[2][row], s.xfin[3][row], s.xfin[4][row], s.xfin[5][row],
-                       r, cc, G, P, dt, nodes, record, ln0, ln1, ln2);
-        if (do_last)
-          nodal_update(st[0], st[1], st[2], s.xst[0][row], s.xst[1][row],
-                       s.xst[2][row], s.xst[3][row], s.xst[4][row], s.xst[5][row], r,
-                       ncols, G, P, dt, nodes, record, ln0, ln1, ln2);
-      }
-      // the started chains of node (r, cc+1) continue in the next column
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        fn[q] = st[q];
-        st[q] = 0.0;
-      }
-    }
-    __syncthreads();
-    if (!has_next) break;
-    cc = ncc;
-    bb = nbb;
-    be = nbe;
-  }
-  cp_async_wait_all();
-  // ---- ledger partials: fixed-order block reduction ----------------------
-  {
-    double v[6] = {lp0, lp1, lp2, ln0, ln1, ln2};
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      double x = v[q];
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) s.led[q][warp] = x;
-    }
-    __syncthreads();
-    if (tid < 6) {
-      double x = 0.0;
-      for (int w = 0; w < kP2GThreads / 32; ++w) x += s.led[tid][w];
-      led_part[(size_t)unit * 6 + tid] = x;
-    }
-    __syncthreads();
-  }
-}
 
 // Lists the P2G units (strip, chunk) whose cell block holds particles; the
 // others have nothing to transfer (their ledger partials are zeroed here).
@@ -864,23 +654,174 @@ __global__ void k_units(const int* __restrict__ cstart, int strips, int chunks,
   }
 }
 
+// ucount[0]: listed units, ucount[1]: P2G's work cursor
 __global__ void k_units_reset(int* ucount, const Scalars* S) {
-  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) *ucount = 0;
+  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) {
+    ucount[0] = 0;
+    ucount[1] = 0;
+  }
+}
+
+__device__ __forceinline__ void p2g_unit(
+    const Particles& p, const int* __restrict__ perm,
+    const int* __restrict__ cstart, const Nodes& nodes,
+    double* __restrict__ led_part, const Geom& G, const Phys& P,
+    const Scalars* S, int record, P2GSmem& s, int unit, int strips) {
+  const int nrows = G.nrows, ncols = G.ncols;
+  const int r0 = (unit % strips) * kTR;
+  const int cA = (unit / strips) * kLC;
+  const int cB = min(cA + kLC, ncols + 1);
+  const int rlo = max(r0 - 1, 0);
+  const int rhi = min(r0 + kTR - 1, nrows - 1);
+  const int ccFirst = max(cA - 1, 0);
+  const int ccLast = min(cB - 1, ncols - 1);
+  const int nrs = rhi - rlo + 2;  // row starts per column
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int grp = warp & 3;          // quantity group (warp-uniform)
+  const bool start = warp >= 4;      // chains of node column cc+1
+  const int row = lane;
+  const int r = r0 + row;
+  const bool lane_ok = row < kTR;  // lanes kTR..31 idle
+  const bool row_ok = lane_ok && (r <= nrows);
+  const double dt = S->dt;
+  const Shape sh{1.0 / G.hx, -1.0 / G.hx, 1.0 / G.hy, -1.0 / G.hy};
+  // exchange slots of each group's quantities: g0 0-2, g1 3-5, g2 6-7, g3 8
+  const int slot0 = grp == 0 ? 0 : grp == 1 ? 3 : grp == 2 ? 6 : 8;
+  const int nq = grp < 2 ? 3 : grp == 2 ? 2 : 1;
+
+  double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
+  double acc[3] = {0, 0, 0};
+
+  // prologue: row starts of the first two columns; gather of batch 0; sorted
+  // indices of batch 1
+  for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
+    const int k = q / nrs, rr = q - k * nrs;
+    const int cc = ccFirst + k;
+    if (cc <= ccLast) s.rowstart[cc % 3][rr] = cstart[rlo + rr + cc * nrows];
+  }
+  __syncthreads();
+  int pf[kPf];
+  Batch cur;
+  cur.cc = ccFirst;
+  cur.bb = s.rowstart[ccFirst % 3][0];
+  cur.be = min(cur.bb + kCap, s.rowstart[ccFirst % 3][nrs - 1]);
+  cur.valid = true;
+  load_perm(pf, perm, cur);
+  issue_gather(s, 0, p, pf, cur);
+  Batch nxt = next_batch(cur, s, nrs, ccLast);
+  load_perm(pf, perm, nxt);
+  int buf = 0;
+  int a0 = 0, a1 = 0, b1 = 0;  // my rows' ranges in the current column
+
+  while (true) {
+    const int* R = s.rowstart[cur.cc % 3];
+    const bool first_of_col = (cur.bb == R[0]);
+    const bool last_of_col = (cur.be == R[nrs - 1]);
+    int rs2 = 0;
+    const bool has_rs2 = last_of_col && cur.cc + 2 <= ccLast && tid < nrs;
+    if (has_rs2) rs2 = cstart[rlo + tid + (cur.cc + 2) * nrows];
+    if (first_of_col) {
+      // cell r-1: [a0, a1), cell r: [a1, b1) (empty where the cell is absent)
+      a0 = a1 = b1 = 0;
+      if (row_ok && r >= rlo && r <= rhi + 1) {
+        const int k = r - rlo;  // row start of cell r (= end of cell r-1)
+        a1 = R[k];
+        a0 = (r - 1 >= rlo) ? R[k - 1] : a1;
+        b1 = (r <= rhi) ? R[k + 1] : a1;
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();  // batch `cur` is in buffer `buf`
+    if (nxt.valid) issue_gather(s, buf ^ 1, p, pf, nxt);
+    const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA;
+    if (!start) {
+      switch (grp) {
+        case 0: chain_range<0, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        case 1: chain_range<1, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        case 2: chain_range<2, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        default: chain_range<3, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      }
+    } else {
+      switch (grp) {
+        case 0: chain_range<0, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        case 1: chain_range<1, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        case 2: chain_range<2, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        default: chain_range<3, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      }
+    }
+    if (last_of_col) {
+      // ---- nodal update of node column cc; started chains move over -------
+      if (lane_ok)
+        for (int q = 0; q < nq; ++q) s.xch[start ? 1 : 0][slot0 + q][row] = acc[q];
+      if (has_rs2) s.rowstart[(cur.cc + 2) % 3][tid] = rs2;
+      __syncthreads();
+      if (warp == 0 && row_ok) {
+        const double (*X)[kTR] = s.xch[0];
+        const double (*Y)[kTR] = s.xch[1];
+        if (cur.cc >= cA)
+          nodal_update(acc[0], acc[1], acc[2], X[3][row], X[4][row], X[5][row],
+                       X[6][row], X[7][row], X[8][row], r, cur.cc, G, P, dt, nodes,
+                       record, ln0, ln1, ln2);
+        if (cur.cc == ncols - 1 && cB == ncols + 1)
+          nodal_update(Y[0][row], Y[1][row], Y[2][row], Y[3][row], Y[4][row], Y[5][row],
+                       Y[6][row], Y[7][row], Y[8][row], r, ncols, G, P, dt, nodes,
+                       record, ln0, ln1, ln2);
+      }
+      for (int q = 0; q < 3; ++q)
+        acc[q] = (lane_ok && !start && q < nq) ? s.xch[1][slot0 + q][row] : 0.0;
+    }
+    // sorted indices two batches ahead (the row starts they need are stored)
+    const Batch n2 = next_batch(nxt, s, nrs, ccLast);
+    load_perm(pf, perm, n2);
+    __syncthreads();  // buffer `buf` and the exchange slots are free again
+    if (!nxt.valid) break;
+    cur = nxt;
+    nxt = n2;
+    buf ^= 1;
+  }
+  cp_async_wait_all();
+  // ---- ledger partials: fixed-order block reduction ----------------------
+  {
+    double v[6] = {lp0, lp1, lp2, ln0, ln1, ln2};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      double x = v[q];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) s.led[q][warp] = x;
+    }
+    __syncthreads();
+    if (tid < 6) {
+      double x = 0.0;
+      for (int w = 0; w < kP2GThreads / 32; ++w) x += s.led[tid][w];
+      led_part[(size_t)unit * 6 + tid] = x;
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     k_p2g(Particles p, const int* __restrict__ perm,
-          const int* __restrict__ cstart, const double* __restrict__ Z,
-          Nodes nodes, double* __restrict__ led_part, Geom G, Phys P,
-          const Scalars* S, int record, const int* __restrict__ ulist,
+          const int* __restrict__ cstart, Nodes nodes,
+          double* __restrict__ led_part, Geom G, Phys P, const Scalars* S,
+          int record, const int* __restrict__ ulist,
           const int* __restrict__ ucount, int strips) {
   if (!S->active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmem& s = *reinterpret_cast<P2GSmem*>(smem_raw);
-  const int nunits = *ucount;
-  for (int ui = blockIdx.x; ui < nunits; ui += gridDim.x)
-    p2g_unit(p, perm, cstart, Z, nodes, led_part, G, P, S, record, s, ulist[ui],
+  const int nunits = ucount[0];
+  __shared__ int next_unit;
+  while (true) {
+    // units are taken in list order from a shared cursor: CTAs that drew
+    // light units take more (the per-SM load stays even)
+    if (threadIdx.x == 0) next_unit = atomicAdd(const_cast<int*>(ucount) + 1, 1);
+    __syncthreads();
+    const int ui = next_unit;
+    __syncthreads();
+    if (ui >= nunits) break;
+    p2g_unit(p, perm, cstart, nodes, led_part, G, P, S, record, s, ulist[ui],
              strips);
+  }
 }
 
 __global__ void k_ledger_final(const double* __restrict__ led_part, int nparts,
@@ -961,15 +902,27 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
       vyL += N * vyn[k];
     }
     if (record) {
-      double ax = 0.0, ay = 0.0;
+      // this step's intermediates as the reference's dprops hold them after
+      // the step (main/optim_par.cpp:387-459,542): apx/apy, grad Z and the
+      // gravity and friction forces of this step's P2G
+      double ax = 0.0, ay = 0.0, dzx = 0.0, dzy = 0.0;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const double N = shp(xi, eta, k);
         ax += N * nodes.avx[nd[k]];
         ay += N * nodes.avy[nd[k]];
+        const double zn = Z[nd[k]];
+        dzx += shg_x(eta, k, ihx, mihx) * zn;
+        dzy += shg_y(xi, k, ihy, mihy) * zn;
       }
       p.apx[i] = ax;
       p.apy[i] = ay;
+      p.dZxp[i] = dzx;
+      p.dZyp[i] = dzy;
+      p.Fpx[i] = p.qgx[i];
+      p.Fpy[i] = p.qgy[i];
+      p.Frx[i] = p.qfx[i];
+      p.Fry[i] = p.qfy[i];
     }
     const double vpx = vxL, vpy = vyL;
     x = x + dt * vpx;
@@ -1014,9 +967,10 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
       p.vpy_dx[i] = vydx;
       p.vpy_dy[i] = vydy;
     }
-    // what the reference stores for the next step (main/optim_par.cpp:
-    // 600-626): momentum, area, basal friction; with the well-balance factor
-    // of the next gravity term (:450)
+    // the record of the next P2G: what the reference stores at the end of
+    // the step (main/optim_par.cpp:600-626: momentum, Ap, basal friction) and
+    // the local coordinates and gravity force in the cell of the next
+    // binning (:387,447-454)
     {
       const double Mp = p.Mp[i], Vp = p.Vp[i];
       p.mpx[i] = vpx * Mp;
@@ -1026,7 +980,12 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
       voellmy(P, vpx, vpy, hp, fbx, fby);
       p.qfx[i] = Ap * fbx;
       p.qfy[i] = Ap * fby;
-      p.qwb[i] = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
+      double qxi, qeta, qgx, qgy;
+      next_record(G, P, Z, x, y, hp, H, Vp, qxi, qeta, qgx, qgy);
+      p.qxi[i] = qxi;
+      p.qeta[i] = qeta;
+      p.qgx[i] = qgx;
+      p.qgy[i] = qgy;
     }
     if (record) {
       // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
