@@ -181,6 +181,31 @@ int dampm_last_timings(dampm_ctx* ctx, int enable_events, double out[5]);
 const char* dampm_last_error(dampm_ctx* ctx);
 const char* dampm_version(void);
 
+/* CFL time step from particle arrays held by the caller on the current
+ * device, computed on the device without allocating any device memory.
+ * No counterpart in the reference: its GPU driver copies vpx, vpy and hp to
+ * the host every step and takes the maxima there
+ * (main/gpu_offload.cpp:284-300).
+ *
+ * vpx, vpy, hp: np device values each (1 <= np <= 2^31-1; np beyond that
+ * returns DAMPM_ERR_CAPACITY, np < 1 DAMPM_ERR_ARG).  out: 5 doubles in
+ * device-writable memory, written asynchronously on cuda_stream (NULL = the
+ * legacy default stream, which must belong to the current device):
+ * {CFL*min(hx,hy)/(1e-2+cel), cel, max|vpx|, max|vpy|, max hp} with
+ * cel = |max(sqrt(g*hmax)+max|vpx|, sqrt(g*hmax)+max|vpy|)|, the step's own
+ * dt formula (main/optim_par.cpp:289-304).
+ *
+ * The reduction scratch is a fixed 28,416-byte array inside this library,
+ * one copy per device; nothing in it has to start at zero.  The first call
+ * on a device looks up that array's address (cudaGetSymbolAddress, with
+ * that device current), so make it before any stream capture.  Calls whose
+ * work can overlap on one device (other streams, other host threads) share
+ * the scratch and race: order them on one stream.  Returns DAMPM_ERR_CUDA
+ * if the lookup or a launch fails. */
+int dampm_cfl_dt_noalloc(const double* vpx, const double* vpy,
+                         const double* hp, long long np, double g, double CFL,
+                         double hx, double hy, double* out, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
