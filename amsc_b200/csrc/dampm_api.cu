@@ -34,8 +34,11 @@ struct dampm_ctx {
   int ntiles = 0;
   double* led_part = nullptr;
   int n_led = 0;
-  int strips = 0, chunks = 0;
-  int *ulist = nullptr, *ucount = nullptr;
+  int strips = 0, useg = 0;  // strips; unit slots per strip (ncols + 1)
+  int *ustart = nullptr, *strip_n = nullptr, *ucount = nullptr;
+  long long* upex = nullptr;
+  int2* uplan = nullptr;
+  int4* ulist = nullptr;
   int *clist = nullptr, *clist_n = nullptr;  // cells with >= 2 particles
   int p2g_grid = 0;
   Scalars* S = nullptr;
@@ -199,10 +202,11 @@ int enqueue_pass(dampm_ctx* ctx) {
   ev_mark(ctx, 0);
   enqueue_sort(ctx);
   ev_mark(ctx, 1);
-  k_units_reset<<<1, 1, 0, ctx->stream>>>(ctx->ucount, ctx->S);
-  k_units<<<grid_for((long long)ctx->strips * ctx->chunks, 256), 256, 0, ctx->stream>>>(
-      ctx->start, ctx->strips, ctx->chunks, ctx->ulist, ctx->ucount, ctx->led_part,
-      ctx->G, ctx->S);
+  k_units_plan<<<ctx->strips, kPlanThreads, 0, ctx->stream>>>(
+      ctx->start, ctx->G, ctx->S, kUnitsPerCta * ctx->p2g_grid, ctx->useg, ctx->ustart,
+      ctx->upex, ctx->uplan, ctx->strip_n);
+  k_units_flat<<<1, kPlanThreads, sizeof(int) * (ctx->strips + 1), ctx->stream>>>(
+      ctx->strip_n, ctx->strips, ctx->useg, ctx->uplan, ctx->ulist, ctx->ucount, ctx->S);
   if (ctx->record) {
     Nodes& n = ctx->nodes;
     double* nf[] = {n.vvxL, n.vvyL, n.Mv,  n.mvx,  n.mvy,   n.avx,   n.avy, n.vvx,
@@ -212,10 +216,10 @@ int enqueue_pass(dampm_ctx* ctx) {
   }
   k_p2g<<<ctx->p2g_grid, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
       ctx->p, ctx->perm, ctx->start, ctx->nodes, ctx->led_part, ctx->G, ctx->P,
-      ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount, ctx->strips);
+      ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount);
   ctx->launches += 2;
   ev_mark(ctx, 3);
-  k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->n_led, ctx->S);
+  k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S);
   ev_mark(ctx, 2);
   k_g2p<<<grid_for(ctx->cap, kG2PThreads), kG2PThreads, 0, ctx->stream>>>(
       ctx->p, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
@@ -354,10 +358,16 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   rc = rc ? rc : dalloc(ctx, &ctx->start, size_t(ctx->nc) + 1);
   rc = rc ? rc : dalloc(ctx, &ctx->tile_sum, size_t(ctx->ntiles) + 1);
   ctx->strips = (grid->Ney + 1 + kTR - 1) / kTR;
-  ctx->chunks = (grid->Nex + 1 + kLC - 1) / kLC;
-  ctx->n_led = ctx->strips * ctx->chunks;
+  ctx->useg = grid->Nex + 1;
+  ctx->n_led = ctx->strips * ctx->useg;  // most units a step can list
+  if (ctx->strips > kMaxStrips)
+    rc = fail(ctx, DAMPM_ERR_ARG, "grid has too many rows for the P2G unit planner");
   rc = rc ? rc : dalloc(ctx, &ctx->led_part, size_t(ctx->n_led) * 6);
+  rc = rc ? rc : dalloc(ctx, &ctx->ustart, size_t(ctx->n_led));
+  rc = rc ? rc : dalloc(ctx, &ctx->upex, size_t(ctx->n_led));
+  rc = rc ? rc : dalloc(ctx, &ctx->uplan, size_t(ctx->n_led));
   rc = rc ? rc : dalloc(ctx, &ctx->ulist, size_t(ctx->n_led));
+  rc = rc ? rc : dalloc(ctx, &ctx->strip_n, size_t(ctx->strips));
   rc = rc ? rc : dalloc(ctx, &ctx->ucount, 2);
   rc = rc ? rc : dalloc(ctx, &ctx->S, 1);
   if (rc == DAMPM_OK) {

@@ -7,10 +7,22 @@
 namespace dampm {
 
 // P2G tiling: kTR node rows per strip (one lane per row in each of the eight
-// warps: four quantity groups x {finishing, starting} chains), kLC node
-// columns per chunk, particle records staged in shared memory kCap at a time.
+// warps: four quantity groups x {finishing, starting} chains); units of
+// variable column width cut to about np / (kUnitsPerCta * CTAs) particles
+// (at least kUnitMinWeight), a column weighing its particles + kColWeight;
+// particle records staged in shared memory kCap at a time.
 constexpr int kTR = 30;
-constexpr int kLC = 16;
+#ifndef DAMPM_UNITS_PER_CTA
+#define DAMPM_UNITS_PER_CTA 4
+#endif
+#ifndef DAMPM_COL_WEIGHT
+#define DAMPM_COL_WEIGHT 192
+#endif
+constexpr int kUnitsPerCta = DAMPM_UNITS_PER_CTA;
+constexpr int kUnitMinWeight = 1024;
+constexpr int kColWeight = DAMPM_COL_WEIGHT;
+constexpr int kPlanThreads = 1024;
+constexpr int kMaxStrips = 8192;  // strip offsets of the unit list in shared memory
 constexpr int kP2GThreads = 256;
 constexpr int kCap = 512;
 constexpr int kP2GMinBlocks = 2;
@@ -73,14 +85,18 @@ __global__ void k_scatter(const int* key, const int* slot, const int* start,
                           int* perm, const Scalars* S);
 __global__ void k_segment_order(const int* start, const int* list,
                                 const int* list_n, int* perm, const Scalars* S);
-__global__ void k_units(const int* cstart, int strips, int chunks, int* ulist,
-                        int* ucount, double* led_part, Geom G, const Scalars* S);
-__global__ void k_units_reset(int* ucount, const Scalars* S);
+__global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
+                             int target_units, int seg, int* ustart,
+                             long long* upex, int2* plan, int* strip_n);
+__global__ void k_units_flat(const int* strip_n, int strips, int seg,
+                             const int2* plan, int4* ulist, int* ucount,
+                             const Scalars* S);
 __global__ void k_p2g(Particles p, const int* perm, const int* cstart,
                       Nodes nodes, double* led_part, Geom G, Phys P,
-                      const Scalars* S, int record, const int* ulist,
-                      const int* ucount, int strips);
-__global__ void k_ledger_final(const double* led_part, int nparts, Scalars* S);
+                      const Scalars* S, int record, const int4* ulist,
+                      const int* ucount);
+__global__ void k_ledger_final(const double* led_part, const int* ucount,
+                               Scalars* S);
 __global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
                       Phys P, Scalars* S, int record, int want_grad);
 

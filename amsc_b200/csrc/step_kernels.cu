@@ -358,8 +358,13 @@ __global__ void k_list_reset(int* list_n, const Scalars* S) {
 
 // Orders each listed cell's segment by ascending particle index (the atomics
 // of k_count hand out slots in arbitrary order).  One warp per cell: a
-// register bitonic sort for up to 32 particles, an insertion sort by lane 0
-// for larger cells.  Particle indices are unique, so the order is total.
+// register bitonic sort for up to 32 particles; a rank sort for up to
+// 32 * kRankPer (each lane holds kRankPer indices and counts, over all the
+// cell's indices broadcast lane by lane, those below each of its own); an
+// insertion sort by lane 0 beyond.  Particle indices are unique, so the
+// ranks are a permutation of [0, m).
+constexpr int kRankPer = 8;
+
 __global__ void k_segment_order(const int* __restrict__ start,
                                 const int* __restrict__ list,
                                 const int* __restrict__ list_n,
@@ -386,6 +391,27 @@ __global__ void k_segment_order(const int* __restrict__ start,
         }
       }
       if (lane < m) perm[b + lane] = v;
+    } else if (m <= 32 * kRankPer) {
+      int v[kRankPer], rank[kRankPer];
+#pragma unroll
+      for (int t = 0; t < kRankPer; ++t) {
+        const int q = lane + 32 * t;
+        v[t] = (q < m) ? perm[b + q] : 0x7fffffff;
+        rank[t] = 0;
+      }
+#pragma unroll
+      for (int t2 = 0; t2 < kRankPer; ++t2) {
+        if (32 * t2 >= m) break;  // warp-uniform
+        for (int src = 0; src < 32; ++src) {
+          const int o = __shfl_sync(0xffffffffu, v[t2], src);
+#pragma unroll
+          for (int t = 0; t < kRankPer; ++t) rank[t] += (o < v[t]) ? 1 : 0;
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < kRankPer; ++t)
+        if (lane + 32 * t < m) perm[b + rank[t]] = v[t];
     } else if (lane == 0) {
       for (int j = b + 1; j < e; ++j) {
         const int v = perm[j];
@@ -625,39 +651,157 @@ __device__ __forceinline__ void chain_range(double (&a)[3], const P2GSmem& s,
 
 }  // namespace
 
-// Lists the P2G units (strip, chunk) whose cell block holds particles; the
-// others have nothing to transfer (their ledger partials are zeroed here).
-// List order is irrelevant: units write disjoint nodes and their ledger
-// partials go to the slot of the unit, reduced in unit order.
-__global__ void k_units(const int* __restrict__ cstart, int strips, int chunks,
-                        int* __restrict__ ulist, int* __restrict__ ucount,
-                        double* __restrict__ led_part, Geom G, const Scalars* S) {
-  if (!S->active) return;
-  const int nrows = G.nrows, ncols = G.ncols;
-  const int nu = strips * chunks;
-  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nu;
-       u += gridDim.x * blockDim.x) {
-    const int strip = u % strips, chunk = u / strips;
-    const int r0 = strip * kTR, cA = chunk * kLC;
-    const int cB = min(cA + kLC, ncols + 1);
-    const int rlo = max(r0 - 1, 0), rhi = min(r0 + kTR - 1, nrows - 1);
-    const int c0 = max(cA - 1, 0), c1 = min(cB - 1, ncols - 1);
-    int n = 0;
-    for (int cc = c0; cc <= c1; ++cc)
-      n += cstart[rhi + cc * nrows + 1] - cstart[rlo + cc * nrows];
-    if (n > 0) {
-      ulist[atomicAdd(ucount, 1)] = u;
-    } else {
+// ---- P2G work units -------------------------------------------------------
+// A unit is node rows [r0, r0+kTR) of one strip x node columns [cA, cB); it
+// walks cell columns cA-1 .. cB-1.  Units are cut per strip so that each
+// carries about the same weight -- its particles plus kColWeight per column
+// -- whatever the local particle density: P2G takes them from a shared
+// cursor, so its time is the average load rather than the heaviest fixed
+// block.  The list is in (strip, column) order and the ledger partial of
+// list entry u sits in slot u, so the ledger reduction order is fixed.
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T block_incl_scan(T v, T* warp_tot, T& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
 #pragma unroll
-      for (int q = 0; q < 6; ++q) led_part[(size_t)u * 6 + q] = 0.0;
-    }
+  for (int o = 1; o < 32; o <<= 1) {
+    const T u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
   }
+  if (lane == 31) warp_tot[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    T t = lane < nw ? warp_tot[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T u = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += u;
+    }
+    if (lane < nw) warp_tot[lane] = t;
+  }
+  __syncthreads();
+  if (w > 0) v += warp_tot[w - 1];
+  total = warp_tot[nw - 1];
+  __syncthreads();  // warp_tot is free again
+  return v;
 }
 
-// ucount[0]: listed units, ucount[1]: P2G's work cursor
-__global__ void k_units_reset(int* ucount, const Scalars* S) {
-  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) {
-    ucount[0] = 0;
+__device__ __forceinline__ int column_count(const int* __restrict__ cstart,
+                                            int rlo, int rhi, int cc, int nrows) {
+  return cstart[rhi + cc * nrows + 1] - cstart[rlo + cc * nrows];
+}
+
+}  // namespace
+
+// One block per strip.  Pass A: node column nc (< ncols) weighs the
+// particles of cell column nc in the strip's cell rows plus kColWeight; nc
+// starts a unit where floor(exclusive prefix / T) changes.  Pass B keeps the
+// units with particles (including those of the leading column cA-1, which
+// feed node column cA).
+__global__ void __launch_bounds__(kPlanThreads)
+    k_units_plan(const int* __restrict__ cstart, Geom G, const Scalars* S,
+                 int target_units, int seg, int* __restrict__ ustart,
+                 long long* __restrict__ upex, int2* __restrict__ plan,
+                 int* __restrict__ strip_n) {
+  if (!S->active) return;
+  __shared__ long long wt_ll[32];
+  __shared__ int wt_i[32];
+  __shared__ long long last_id;
+  const int strip = blockIdx.x;
+  const int nrows = G.nrows, ncols = G.ncols;
+  const int r0 = strip * kTR;
+  const int rlo = max(r0 - 1, 0), rhi = min(r0 + kTR - 1, nrows - 1);
+  long long T = (long long)S->np / max(target_units, 1);
+  if (T < kUnitMinWeight) T = kUnitMinWeight;
+  int* st = ustart + (size_t)strip * seg;
+  long long* px = upex + (size_t)strip * seg;
+  long long carry = 0, prev_id = -1;
+  int K = 0;
+  for (int base = 0; base <= ncols; base += blockDim.x) {
+    const int nc = base + threadIdx.x;
+    long long w = 0;
+    if (nc < ncols) w = column_count(cstart, rlo, rhi, nc, nrows) + kColWeight;
+    long long tot;
+    const long long incl = block_incl_scan<long long>(w, wt_ll, tot);
+    const long long pex = carry + incl - w;
+    const long long id = pex / T;
+    // id of the column before: the neighbour thread's, or the previous tile's
+    long long idp = __shfl_up_sync(0xffffffffu, id, 1);
+    if ((threadIdx.x & 31) == 31) wt_ll[threadIdx.x >> 5] = id;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+      idp = threadIdx.x == 0 ? prev_id : wt_ll[(threadIdx.x >> 5) - 1];
+    if (threadIdx.x == blockDim.x - 1) last_id = id;
+    __syncthreads();
+    const int flag = (nc == 0) || (nc < ncols && id != idp);
+    int ktot;
+    const int kin = block_incl_scan<int>(flag, wt_i, ktot);
+    if (flag) {
+      st[K + kin - 1] = nc;
+      px[K + kin - 1] = pex;
+    }
+    carry += tot;
+    prev_id = last_id;
+    K += ktot;
+    __syncthreads();
+  }
+  const long long ptotal = carry;
+  int J = 0;
+  for (int base = 0; base < K; base += blockDim.x) {
+    const int k = base + threadIdx.x;
+    int flag = 0, cA = 0, cB = 0;
+    if (k < K) {
+      cA = st[k];
+      const bool more = k + 1 < K;
+      cB = more ? st[k + 1] : ncols + 1;
+      const long long sumw = (more ? px[k + 1] : ptotal) - px[k];
+      const long long n = sumw - (long long)kColWeight * (min(cB, ncols) - cA) +
+                          (cA > 0 ? column_count(cstart, rlo, rhi, cA - 1, nrows) : 0);
+      flag = n > 0;
+    }
+    int jtot;
+    const int jin = block_incl_scan<int>(flag, wt_i, jtot);
+    if (flag) plan[(size_t)strip * seg + J + jin - 1] = make_int2(cA, cB);
+    J += jtot;
+  }
+  if (threadIdx.x == 0) strip_n[strip] = J;
+}
+
+// One block: strip offsets by a scan of strip_n, then the flat unit list
+// {strip, cA, cB} in (strip, column) order.  ucount[0] = units,
+// ucount[1] = P2G's work cursor.
+__global__ void __launch_bounds__(kPlanThreads)
+    k_units_flat(const int* __restrict__ strip_n, int strips, int seg,
+                 const int2* __restrict__ plan, int4* __restrict__ ulist,
+                 int* __restrict__ ucount, const Scalars* S) {
+  if (!S->active) return;
+  extern __shared__ int uoff[];  // strips + 1
+  __shared__ int wt_i[32];
+  int carry = 0;
+  for (int base = 0; base < strips; base += blockDim.x) {
+    const int s = base + threadIdx.x;
+    const int n = s < strips ? strip_n[s] : 0;
+    int tot;
+    const int incl = block_incl_scan<int>(n, wt_i, tot);
+    if (s < strips) uoff[s] = carry + incl - n;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) uoff[strips] = carry;
+  __syncthreads();
+  const int total = carry;
+  for (int f = threadIdx.x; f < total; f += blockDim.x) {
+    int lo = 0, hi = strips;  // uoff[lo] <= f < uoff[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (uoff[mid] <= f) lo = mid; else hi = mid;
+    }
+    const int2 u = plan[(size_t)lo * seg + (f - uoff[lo])];
+    ulist[f] = make_int4(lo, u.x, u.y, 0);
+  }
+  if (threadIdx.x == 0) {
+    ucount[0] = total;
     ucount[1] = 0;
   }
 }
@@ -666,11 +810,11 @@ __device__ __forceinline__ void p2g_unit(
     const Particles& p, const int* __restrict__ perm,
     const int* __restrict__ cstart, const Nodes& nodes,
     double* __restrict__ led_part, const Geom& G, const Phys& P,
-    const Scalars* S, int record, P2GSmem& s, int unit, int strips) {
+    const Scalars* S, int record, P2GSmem& s, int slot, int4 unit) {
   const int nrows = G.nrows, ncols = G.ncols;
-  const int r0 = (unit % strips) * kTR;
-  const int cA = (unit / strips) * kLC;
-  const int cB = min(cA + kLC, ncols + 1);
+  const int r0 = unit.x * kTR;
+  const int cA = unit.y;
+  const int cB = unit.z;
   const int rlo = max(r0 - 1, 0);
   const int rhi = min(r0 + kTR - 1, nrows - 1);
   const int ccFirst = max(cA - 1, 0);
@@ -735,7 +879,9 @@ __device__ __forceinline__ void p2g_unit(
     __syncthreads();  // batch `cur` is in buffer `buf`
     if (nxt.valid) issue_gather(s, buf ^ 1, p, pf, nxt);
     const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA;
-    if (!start) {
+    if (!start && cur.cc < cA) {
+      // leading column: only its started chains (node column cA) are needed
+    } else if (!start) {
       switch (grp) {
         case 0: chain_range<0, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
         case 1: chain_range<1, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
@@ -794,7 +940,7 @@ __device__ __forceinline__ void p2g_unit(
     if (tid < 6) {
       double x = 0.0;
       for (int w = 0; w < kP2GThreads / 32; ++w) x += s.led[tid][w];
-      led_part[(size_t)unit * 6 + tid] = x;
+      led_part[(size_t)slot * 6 + tid] = x;
     }
     __syncthreads();
   }
@@ -804,8 +950,8 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     k_p2g(Particles p, const int* __restrict__ perm,
           const int* __restrict__ cstart, Nodes nodes,
           double* __restrict__ led_part, Geom G, Phys P, const Scalars* S,
-          int record, const int* __restrict__ ulist,
-          const int* __restrict__ ucount, int strips) {
+          int record, const int4* __restrict__ ulist,
+          const int* __restrict__ ucount) {
   if (!S->active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmem& s = *reinterpret_cast<P2GSmem*>(smem_raw);
@@ -819,14 +965,14 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     const int ui = next_unit;
     __syncthreads();
     if (ui >= nunits) break;
-    p2g_unit(p, perm, cstart, nodes, led_part, G, P, S, record, s, ulist[ui],
-             strips);
+    p2g_unit(p, perm, cstart, nodes, led_part, G, P, S, record, s, ui, ulist[ui]);
   }
 }
 
-__global__ void k_ledger_final(const double* __restrict__ led_part, int nparts,
-                               Scalars* S) {
+__global__ void k_ledger_final(const double* __restrict__ led_part,
+                               const int* __restrict__ ucount, Scalars* S) {
   if (!S->active) return;
+  const int nparts = ucount[0];
   __shared__ double sm[6][32];
   double v[6] = {0, 0, 0, 0, 0, 0};
   for (int b = threadIdx.x; b < nparts; b += blockDim.x)

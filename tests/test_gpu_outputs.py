@@ -59,9 +59,9 @@ def test_mudflow_small_adaptive(cuda_lib):
 
 @pytest.mark.gpu
 def test_edge_pileup_and_walls(cuda_lib):
-    """A pile-up (one cell with 60 particles: cells above 32 particles take
-    the serial per-cell ordering, columns above the P2G batch size are split
-    into batches), particles on the domain walls and an odd grid."""
+    """Pile-ups (a cell with 60 particles takes the warp rank sort of the
+    per-cell ordering, a cell with 300 the serial one; columns above the P2G
+    batch size are split into batches), particles on the domain walls."""
     d = scenarios.dam_break_flat(nsteps=20)
     x, y = d.arrays["x"].copy(), d.arrays["y"].copy()
     x[:60] = 2.126 + 1e-3 * np.arange(60) / 60
@@ -70,6 +70,8 @@ def test_edge_pileup_and_walls(cuda_lib):
     y[60:700] = np.linspace(0.01, 15.99, 640)
     x[700], y[700] = 0.0, 0.0
     x[701], y[701] = 16.0, 16.0
+    x[702:1002] = 1.1 + 1e-2 * np.arange(300) / 300
+    y[702:1002] = 3.3 + 1e-2 * np.arange(300)[::-1] / 300
     d.arrays["x"], d.arrays["y"] = x, y
     o = Oracle(d, threads=4)
     o.run(20)
