@@ -382,6 +382,8 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
     if (cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smem)) != cudaSuccess)
       rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+    cudaFuncSetAttribute(k_p2g, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         int(cudaSharedmemCarveoutMaxShared));
     int per_sm = 0, nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

@@ -6,8 +6,8 @@
 
 namespace dampm {
 
-// P2G tiling: kTR node rows per strip (one lane per row in each of the eight
-// warps: four quantity groups x {finishing, starting} chains); units of
+// P2G tiling: kTR node rows per strip (one lane per row in each of the four
+// warps, one per quantity group, finishing and starting chains); units of
 // variable column width cut to about np / (kUnitsPerCta * CTAs) particles
 // (at least kUnitMinWeight), a column weighing its particles + kColWeight;
 // particle records staged in shared memory kCap at a time.
@@ -23,9 +23,9 @@ constexpr int kUnitMinWeight = 1024;
 constexpr int kColWeight = DAMPM_COL_WEIGHT;
 constexpr int kPlanThreads = 1024;
 constexpr int kMaxStrips = 8192;  // strip offsets of the unit list in shared memory
-constexpr int kP2GThreads = 256;
+constexpr int kP2GThreads = 128;
 constexpr int kCap = 512;
-constexpr int kP2GMinBlocks = 2;
+constexpr int kP2GMinBlocks = 4;
 constexpr int kG2PThreads = 256;
 constexpr int kScanTile = 4096;
 constexpr int kScanThreads = 1024;

@@ -365,7 +365,9 @@ __global__ void k_list_reset(int* list_n, const Scalars* S) {
 // ranks are a permutation of [0, m).
 constexpr int kRankPer = 8;
 
-__global__ void k_segment_order(const int* __restrict__ start,
+// (eight resident blocks per SM for the common small cells; the rank sort's
+// registers may spill for the rare crowded ones)
+__global__ void __launch_bounds__(256, 8) k_segment_order(const int* __restrict__ start,
                                 const int* __restrict__ list,
                                 const int* __restrict__ list_n,
                                 int* __restrict__ perm, const Scalars* S) {
@@ -429,28 +431,29 @@ __global__ void k_segment_order(const int* __restrict__ start,
 // ---------------------------------------------------------------------------
 // P2G + NODAL
 //
-// Work unit: node rows [r0, r0+kTR) of one strip x node columns [cA, cB) of
-// one chunk; the unit walks the cell columns cA-1 .. cB-1.  For cell column cc
-// the particles of cells (rlo..rhi, cc) are one contiguous range of the sorted
-// order, processed in batches of at most kCap particles.  Each particle's
-// record (local coordinates and the nine transferred quantities, built by the
-// previous step's G2P) is copied with cp.async into one of two shared-memory
-// buffers: the copies of batch k+1 fly while batch k is transferred, and the
-// sorted indices of batch k+2 are loaded meanwhile.
+// Work unit: node rows [r0, r0+kTR) of one strip x node columns [cA, cB); the
+// unit walks the cell columns cA-1 .. cB-1.  For cell column cc the particles
+// of cells (rlo..rhi, cc) are one contiguous range of the sorted order,
+// processed in batches of at most kCap particles.  Each particle's record
+// (local coordinates and the nine transferred quantities, built by the
+// previous step's G2P) is copied with cp.async into shared memory; the sorted
+// indices of the next batch are loaded while the copies fly.  Four CTAs share
+// an SM, so one CTA's copies overlap the others' transfers.
 //
-// Node row r is served by lane r of eight warps: four quantity groups
+// Node row r is served by lane r of four warps, one per quantity group
 // (warp-uniform code) g0 {Mv, mom_x, mom_y}, g1 {FPx, FPy, Fric_x},
-// g2 {Fric_y, Fint_x}, g3 {Fint_y}, each for two chains:
-//   fin   (warps 0-3): node (r, cc)   -- local node 1 of cell (r-1,cc), then 0
-//         of (r,cc); it already holds cells (r-1,cc-1), (r,cc-1);
-//   start (warps 4-7): node (r, cc+1) -- local node 3 of cell (r-1,cc), then 2
-//         of (r,cc).
+// g2 {Fric_y, Fint_x}, g3 {Fint_y}; each lane carries two chains per
+// quantity:
+//   fin   node (r, cc)   -- local node 1 of cell (r-1,cc), then 0 of (r,cc);
+//         it already holds cells (r-1,cc-1), (r,cc-1);
+//   start node (r, cc+1) -- local node 3 of cell (r-1,cc), then 2 of (r,cc).
 // That is each node's contributions in quadgrid's cell-sweep order, so every
 // nodal sum equals the reference's sequential sum bit for bit.  At the end of
-// a column warp 0 applies the nodal update to node column cc and the started
-// chains move to the finishing warps.  Records are stored SoA with an XOR
-// swizzle of the low four index bits so that lanes of consecutive rows
-// (records ~ppc apart) hit distinct banks.
+// a column the finished sums go through shared memory to warp 0, which
+// applies the nodal update to node column cc, and each lane's started chains
+// become its finishing ones.  Records are stored SoA with an XOR swizzle of
+// the low four index bits so that lanes of consecutive rows (records ~ppc
+// apart) hit distinct banks.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -458,10 +461,10 @@ constexpr int kRec = 13;  // xi eta Mp mpx mpy FPx FPy Frx Fry F11 F12 F22 Vp
 constexpr int kPf = (kCap + kP2GThreads - 1) / kP2GThreads;
 
 struct P2GSmem {
-  double rec[2][kRec][kCap];
-  int rowstart[3][kTR + 2];
-  double xch[2][9][kTR];  // finished [0] / started [1] chains per quantity
+  double rec[kRec][kCap];
+  double xch[9][kTR];  // finished sums per quantity
   double led[6][kP2GThreads / 32];
+  int rowstart[3][kTR + 2];
 };
 
 __device__ __forceinline__ int swz(int j) { return j ^ ((j >> 4) & 15); }
@@ -505,8 +508,7 @@ __device__ __forceinline__ void load_perm(int (&pf)[kPf],
   }
 }
 
-__device__ __forceinline__ void issue_gather(P2GSmem& s, int buf,
-                                             const Particles& p,
+__device__ __forceinline__ void issue_gather(P2GSmem& s, const Particles& p,
                                              const int (&pf)[kPf],
                                              const Batch& b) {
 #pragma unroll
@@ -515,19 +517,19 @@ __device__ __forceinline__ void issue_gather(P2GSmem& s, int buf,
     if (j >= b.be) break;
     const int i = pf[u];
     const int l = swz(j - b.bb);
-    cp_async8(&s.rec[buf][0][l], p.qxi + i);
-    cp_async8(&s.rec[buf][1][l], p.qeta + i);
-    cp_async8(&s.rec[buf][2][l], p.Mp + i);
-    cp_async8(&s.rec[buf][3][l], p.mpx + i);
-    cp_async8(&s.rec[buf][4][l], p.mpy + i);
-    cp_async8(&s.rec[buf][5][l], p.qgx + i);
-    cp_async8(&s.rec[buf][6][l], p.qgy + i);
-    cp_async8(&s.rec[buf][7][l], p.qfx + i);
-    cp_async8(&s.rec[buf][8][l], p.qfy + i);
-    cp_async8(&s.rec[buf][9][l], p.F11 + i);
-    cp_async8(&s.rec[buf][10][l], p.F12 + i);
-    cp_async8(&s.rec[buf][11][l], p.F22 + i);
-    cp_async8(&s.rec[buf][12][l], p.Vp + i);
+    cp_async8(&s.rec[0][l], p.qxi + i);
+    cp_async8(&s.rec[1][l], p.qeta + i);
+    cp_async8(&s.rec[2][l], p.Mp + i);
+    cp_async8(&s.rec[3][l], p.mpx + i);
+    cp_async8(&s.rec[4][l], p.mpy + i);
+    cp_async8(&s.rec[5][l], p.qgx + i);
+    cp_async8(&s.rec[6][l], p.qgy + i);
+    cp_async8(&s.rec[7][l], p.qfx + i);
+    cp_async8(&s.rec[8][l], p.qfy + i);
+    cp_async8(&s.rec[9][l], p.F11 + i);
+    cp_async8(&s.rec[10][l], p.F12 + i);
+    cp_async8(&s.rec[11][l], p.F22 + i);
+    cp_async8(&s.rec[12][l], p.Vp + i);
   }
   cp_async_commit();
 }
@@ -588,51 +590,65 @@ struct Shape {
   double ihx, mihx, ihy, mihy;
 };
 
-// One particle's contribution to the chains of quantity group kG; kStart
-// selects the chain (fin: local 1/0, start: local 3/2), `upper` the cell
-// (r-1: local 1/3, r: local 0/2).  With fa = (1-xi) or xi, fb = eta or
-// (1-eta):  N = fa*fb,  Nx = (mihx or ihx)*fb,  Ny = fa*(ihy or mihy) --
-// shp/shg of main/gpu_kernels.cpp:33-59 for that local node.
-template <int kG, bool kStart>
-__device__ __forceinline__ void chain_step(double (&a)[3], const P2GSmem& s,
-                                           int buf, int l, bool upper,
+// One particle's contributions to the chains of quantity group kG: `upper`
+// selects the cell (r-1: local nodes 1 (fin) and 3 (start); r: local nodes 0
+// and 2).  With fb = eta or (1-eta):
+//   fin   N = (1-xi)*fb, Nx = mihx*fb, Ny = (1-xi)*(ihy or mihy)
+//   start N = xi*fb,     Nx = ihx*fb,  Ny = xi*(ihy or mihy)
+// -- shp/shg of main/gpu_kernels.cpp:33-59 for those local nodes.  kFin off
+// runs the started chains alone (a unit's leading column).
+template <int kG, bool kFin>
+__device__ __forceinline__ void chain_step(double (&af)[3], double (&as)[3],
+                                           const P2GSmem& s, int l, bool upper,
                                            const Shape& sh) {
-  const double xi = s.rec[buf][0][l], eta = s.rec[buf][1][l];
-  const double fa = kStart ? xi : (1.0 - xi);
+  const double xi = s.rec[0][l], eta = s.rec[1][l];
+  const double fa = 1.0 - xi;
   const double fb = upper ? eta : (1.0 - eta);
-  const double N = fa * fb;
-  if (kG == 0) {
-    const double q0 = s.rec[buf][2][l], q1 = s.rec[buf][3][l], q2 = s.rec[buf][4][l];
-    a[0] += N * q0;
-    a[1] += N * q1;
-    a[2] += N * q2;
-  } else if (kG == 1) {
-    const double q0 = s.rec[buf][5][l], q1 = s.rec[buf][6][l], q2 = s.rec[buf][7][l];
-    a[0] += N * q0;
-    a[1] += N * q1;
-    a[2] += N * q2;
+  const double Nf = fa * fb;
+  const double Ns = xi * fb;
+  if (kG == 0 || kG == 1) {
+    const int o = kG == 0 ? 2 : 5;
+    const double q0 = s.rec[o][l], q1 = s.rec[o + 1][l], q2 = s.rec[o + 2][l];
+    if (kFin) {
+      af[0] += Nf * q0;
+      af[1] += Nf * q1;
+      af[2] += Nf * q2;
+    }
+    as[0] += Ns * q0;
+    as[1] += Ns * q1;
+    as[2] += Ns * q2;
   } else {
-    const double Nx = (kStart ? sh.ihx : sh.mihx) * fb;
-    const double Ny = fa * (upper ? sh.ihy : sh.mihy);
-    const double f12 = s.rec[buf][10][l], vp = s.rec[buf][12][l];
+    const double hy = upper ? sh.ihy : sh.mihy;
+    const double Nxs = sh.ihx * fb, Nys = xi * hy;
+    const double f12 = s.rec[10][l], vp = s.rec[12][l];
     if (kG == 2) {
-      const double q0 = s.rec[buf][8][l], f11 = s.rec[buf][9][l];
-      a[0] += N * q0;
-      a[1] += (Nx * f11 + Ny * f12) * vp;
+      const double q0 = s.rec[8][l], f11 = s.rec[9][l];
+      if (kFin) {
+        const double Nxf = sh.mihx * fb, Nyf = fa * hy;
+        af[0] += Nf * q0;
+        af[1] += (Nxf * f11 + Nyf * f12) * vp;
+      }
+      as[0] += Ns * q0;
+      as[1] += (Nxs * f11 + Nys * f12) * vp;
     } else {
-      const double f22 = s.rec[buf][11][l];
-      a[0] += (Nx * f12 + Ny * f22) * vp;
+      const double f22 = s.rec[11][l];
+      if (kFin) {
+        const double Nxf = sh.mihx * fb, Nyf = fa * hy;
+        af[0] += (Nxf * f12 + Nyf * f22) * vp;
+      }
+      as[0] += (Nxs * f12 + Nys * f22) * vp;
     }
   }
 }
 
 // The particles of cells (r-1, cc) and (r, cc) are the adjacent ranges
 // [a0, a1) and [a1, b1) of the sorted order: one walk in order.
-template <int kG, bool kStart>
-__device__ __forceinline__ void chain_range(double (&a)[3], const P2GSmem& s,
-                                            int buf, int a0, int a1, int b1,
-                                            int bb, int be, const Shape& sh,
-                                            bool own, double& lp0, double& lp1,
+template <int kG, bool kFin>
+__device__ __forceinline__ void chain_range(double (&af)[3], double (&as)[3],
+                                            const P2GSmem& s, int a0, int a1,
+                                            int b1, int bb, int be,
+                                            const Shape& sh, bool own,
+                                            double& lp0, double& lp1,
                                             double& lp2) {
   const int j1 = min(b1, be);
   int j = max(a0, bb);
@@ -640,13 +656,26 @@ __device__ __forceinline__ void chain_range(double (&a)[3], const P2GSmem& s,
   for (; j < j1; ++j) {
     const int l = swz(j - bb);
     const bool upper = j < a1;
-    chain_step<kG, kStart>(a, s, buf, l, upper, sh);
-    if (kG == 0 && !kStart && own && !upper) {  // particle ledger, once each
-      lp0 += s.rec[buf][2][l];
-      lp1 += s.rec[buf][3][l];
-      lp2 += s.rec[buf][4][l];
+    chain_step<kG, kFin>(af, as, s, l, upper, sh);
+    if (kG == 0 && own && !upper) {  // particle ledger, once each
+      lp0 += s.rec[2][l];
+      lp1 += s.rec[3][l];
+      lp2 += s.rec[4][l];
     }
   }
+}
+
+template <int kG>
+__device__ __forceinline__ void chain_group(double (&af)[3], double (&as)[3],
+                                            const P2GSmem& s, bool lead, int a0,
+                                            int a1, int b1, int bb, int be,
+                                            const Shape& sh, bool own,
+                                            double& lp0, double& lp1,
+                                            double& lp2) {
+  if (lead)
+    chain_range<kG, false>(af, as, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
+  else
+    chain_range<kG, true>(af, as, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
 }
 
 }  // namespace
@@ -822,8 +851,7 @@ __device__ __forceinline__ void p2g_unit(
   const int nrs = rhi - rlo + 2;  // row starts per column
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int grp = warp & 3;          // quantity group (warp-uniform)
-  const bool start = warp >= 4;      // chains of node column cc+1
+  const int grp = warp;  // quantity group (warp-uniform)
   const int row = lane;
   const int r = r0 + row;
   const bool lane_ok = row < kTR;  // lanes kTR..31 idle
@@ -833,12 +861,12 @@ __device__ __forceinline__ void p2g_unit(
   // exchange slots of each group's quantities: g0 0-2, g1 3-5, g2 6-7, g3 8
   const int slot0 = grp == 0 ? 0 : grp == 1 ? 3 : grp == 2 ? 6 : 8;
   const int nq = grp < 2 ? 3 : grp == 2 ? 2 : 1;
+  const bool last_unit_col = (cB == ncols + 1);  // this unit closes node column ncols
 
   double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
-  double acc[3] = {0, 0, 0};
+  double af[3] = {0, 0, 0}, as[3] = {0, 0, 0};
 
-  // prologue: row starts of the first two columns; gather of batch 0; sorted
-  // indices of batch 1
+  // prologue: row starts of the first two columns, sorted indices of batch 0
   for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
     const int k = q / nrs, rr = q - k * nrs;
     const int cc = ccFirst + k;
@@ -852,13 +880,12 @@ __device__ __forceinline__ void p2g_unit(
   cur.be = min(cur.bb + kCap, s.rowstart[ccFirst % 3][nrs - 1]);
   cur.valid = true;
   load_perm(pf, perm, cur);
-  issue_gather(s, 0, p, pf, cur);
-  Batch nxt = next_batch(cur, s, nrs, ccLast);
-  load_perm(pf, perm, nxt);
-  int buf = 0;
   int a0 = 0, a1 = 0, b1 = 0;  // my rows' ranges in the current column
 
   while (true) {
+    issue_gather(s, p, pf, cur);
+    // while the copies fly: this batch's bookkeeping and the next batch's
+    // sorted indices
     const int* R = s.rowstart[cur.cc % 3];
     const bool first_of_col = (cur.bb == R[0]);
     const bool last_of_col = (cur.be == R[nrs - 1]);
@@ -875,58 +902,54 @@ __device__ __forceinline__ void p2g_unit(
         b1 = (r <= rhi) ? R[k + 1] : a1;
       }
     }
+    const Batch nxt = next_batch(cur, s, nrs, ccLast);
+    load_perm(pf, perm, nxt);
     cp_async_wait_all();
-    __syncthreads();  // batch `cur` is in buffer `buf`
-    if (nxt.valid) issue_gather(s, buf ^ 1, p, pf, nxt);
+    __syncthreads();  // batch `cur` is in shared memory
     const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA;
-    if (!start && cur.cc < cA) {
-      // leading column: only its started chains (node column cA) are needed
-    } else if (!start) {
-      switch (grp) {
-        case 0: chain_range<0, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-        case 1: chain_range<1, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-        case 2: chain_range<2, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-        default: chain_range<3, false>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      }
-    } else {
-      switch (grp) {
-        case 0: chain_range<0, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-        case 1: chain_range<1, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-        case 2: chain_range<2, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-        default: chain_range<3, true>(acc, s, buf, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      }
+    const bool lead = cur.cc < cA;  // started chains only
+    switch (grp) {
+      case 0: chain_group<0>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      case 1: chain_group<1>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      case 2: chain_group<2>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      default: chain_group<3>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
     }
     if (last_of_col) {
-      // ---- nodal update of node column cc; started chains move over -------
       if (lane_ok)
-        for (int q = 0; q < nq; ++q) s.xch[start ? 1 : 0][slot0 + q][row] = acc[q];
+        for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = af[q];
       if (has_rs2) s.rowstart[(cur.cc + 2) % 3][tid] = rs2;
-      __syncthreads();
-      if (warp == 0 && row_ok) {
-        const double (*X)[kTR] = s.xch[0];
-        const double (*Y)[kTR] = s.xch[1];
-        if (cur.cc >= cA)
-          nodal_update(acc[0], acc[1], acc[2], X[3][row], X[4][row], X[5][row],
-                       X[6][row], X[7][row], X[8][row], r, cur.cc, G, P, dt, nodes,
-                       record, ln0, ln1, ln2);
-        if (cur.cc == ncols - 1 && cB == ncols + 1)
-          nodal_update(Y[0][row], Y[1][row], Y[2][row], Y[3][row], Y[4][row], Y[5][row],
-                       Y[6][row], Y[7][row], Y[8][row], r, ncols, G, P, dt, nodes,
-                       record, ln0, ln1, ln2);
-      }
-      for (int q = 0; q < 3; ++q)
-        acc[q] = (lane_ok && !start && q < nq) ? s.xch[1][slot0 + q][row] : 0.0;
     }
-    // sorted indices two batches ahead (the row starts they need are stored)
-    const Batch n2 = next_batch(nxt, s, nrs, ccLast);
-    load_perm(pf, perm, n2);
-    __syncthreads();  // buffer `buf` and the exchange slots are free again
+    __syncthreads();  // shared records free; finished sums exchanged
+    if (last_of_col) {
+      // ---- nodal update of node column cc ------------------------------
+      if (warp == 0 && row_ok && cur.cc >= cA) {
+        const double (*X)[kTR] = s.xch;
+        nodal_update(af[0], af[1], af[2], X[3][row], X[4][row], X[5][row],
+                     X[6][row], X[7][row], X[8][row], r, cur.cc, G, P, dt, nodes,
+                     record, ln0, ln1, ln2);
+      }
+      if (cur.cc == ncols - 1 && last_unit_col) {
+        // node column ncols: its chains end with this column
+        __syncthreads();  // warp 0 is done reading the exchange
+        if (lane_ok)
+          for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = as[q];
+        __syncthreads();
+        if (warp == 0 && row_ok) {
+          const double (*X)[kTR] = s.xch;
+          nodal_update(as[0], as[1], as[2], X[3][row], X[4][row], X[5][row],
+                       X[6][row], X[7][row], X[8][row], r, ncols, G, P, dt,
+                       nodes, record, ln0, ln1, ln2);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        af[q] = as[q];
+        as[q] = 0.0;
+      }
+    }
     if (!nxt.valid) break;
     cur = nxt;
-    nxt = n2;
-    buf ^= 1;
   }
-  cp_async_wait_all();
   // ---- ledger partials: fixed-order block reduction ----------------------
   {
     double v[6] = {lp0, lp1, lp2, ln0, ln1, ln2};
