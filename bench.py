@@ -163,6 +163,9 @@ def cpu_baseline_port(d, seconds: float = 15.0):
                       f"{el:.1f} s"}
 
 
+REF_MAX_STEPS = 30
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference's own CPU solver on the host cores.
 
@@ -186,7 +189,8 @@ def run_reference(args, world, rank):
     from oracle import refrun
     d = scenarios.mudflow(N=2048)
     np_ = d.np
-    steps = max(1, args.steps)
+    # a bounded sample: the reference takes seconds per step of this workload
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
     if refrun.available():
         d.scalars.update({"DT_FIXED": 0.0145, "NSTEPS": 5 + steps})
         wd = tempfile.mkdtemp(prefix="dampm_refarm_")
@@ -207,7 +211,7 @@ def run_reference(args, world, rank):
         from oracle.oracle import Oracle
         cores = os.cpu_count() or 1
         o = Oracle(d, threads=cores)
-        for _ in range(max(args.warmup, 1)):
+        for _ in range(max(min(args.warmup, 3), 1)):
             o.run(1)
         t0 = time.perf_counter()
         for _ in range(steps):
@@ -277,9 +281,13 @@ def main():
     ms_per_step = el_ms / args.steps
     st = s.status()
 
-    # roofline of the dominant kernel (P2G), algorithmic bytes per launch:
-    # 96 B per particle (11 f64 fields, sorted index, cell key) + 24 B per
-    # written node (vvxL, vvyL, Z)
+    # roofline of the dominant kernel, algorithmic bytes per launch:
+    # P2G reads each particle's 13-value f64 record (written by the previous
+    # G2P) and its sorted index: 108 B per particle, and writes vvxL, vvyL:
+    # 16 B per node touched.  G2P reads key, x, y, hp, H, Mp, Vp (52 B) and
+    # writes x, y, vpx, vpy, hp, F11, F12, F22, key and the 8-value next
+    # record (132 B): 184 B per particle, and gathers vvxL, vvyL, Z: 24 B per
+    # node touched.
     x = s.download("x")
     y = s.download("y")
     h = float(d.scalars["hx"])
@@ -288,8 +296,8 @@ def main():
           np.clip(np.floor(x / h), 0, int(d.scalars["Nex"]) - 1).astype(np.int64) * nrows)
     n_nodes = _touched_nodes(d, kc)
     np_now = st["np"]
-    p2g_bytes = 96 * np_now + 24 * n_nodes
-    g2p_bytes = 104 * np_now + 16 * n_nodes
+    p2g_bytes = 108 * np_now + 16 * n_nodes
+    g2p_bytes = 184 * np_now + 24 * n_nodes
     p2g_ms = tm[1] / args.steps
     g2p_ms = tm[2] / args.steps
     peak, peak_kind = _peaks()
