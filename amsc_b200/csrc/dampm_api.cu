@@ -224,6 +224,11 @@ int enqueue_pass(dampm_ctx* ctx) {
   k_g2p<<<grid_for(ctx->cap, kG2PThreads), kG2PThreads, 0, ctx->stream>>>(
       ctx->p, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
       (grad_next || ctx->record) ? 1 : 0);
+  if (ctx->record) {
+    k_hv<<<grid_for(ctx->nn, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->perm, ctx->start,
+                                                           ctx->nodes.HV, ctx->G, ctx->S);
+    ctx->launches += 1;
+  }
   ev_mark(ctx, 3);
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->S);
   ctx->launches += 4;

@@ -100,6 +100,9 @@ __global__ void k_ledger_final(const double* led_part, const int* ucount,
 __global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
                       Phys P, Scalars* S, int record, int want_grad);
 
+__global__ void k_hv(const Particles p, const int* perm, const int* cstart,
+                     double* HV, Geom G, const Scalars* S);
+
 size_t p2g_smem_bytes();
 
 }  // namespace dampm

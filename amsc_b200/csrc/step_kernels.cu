@@ -1188,4 +1188,42 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
 
 size_t p2g_smem_bytes() { return sizeof(P2GSmem); }
 
+// HV: p2g of the updated depth hp at the updated positions, each particle
+// still in the cell it was binned to at the start of the step
+// (main/optim_par.cpp:650, after the vars were zeroed at :362-364).  One
+// thread per node walks its four cells in id order -- (r-1,c-1) local 3,
+// (r,c-1) local 2, (r-1,c) local 1, (r,c) local 0 -- and each cell's
+// particles in index order (this step's perm), the quadgrid cell-sweep order.
+// Output-only: launched when outputs are recorded.
+__global__ void k_hv(const Particles p, const int* __restrict__ perm,
+                     const int* __restrict__ cstart, double* __restrict__ HV,
+                     Geom G, const Scalars* S) {
+  if (!S->active) return;
+  const int nrows = G.nrows, ncols = G.ncols;
+  const int nn = (nrows + 1) * (ncols + 1);
+  const double ihx = 1.0 / G.hx, ihy = 1.0 / G.hy;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
+       n += gridDim.x * blockDim.x) {
+    const int r = n % (nrows + 1), c = n / (nrows + 1);
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      // q: 0 -> cell (r-1,c-1) local 3, 1 -> (r,c-1) local 2,
+      //    2 -> (r-1,c) local 1,   3 -> (r,c) local 0
+      const int cr = (q & 1) ? r : r - 1;
+      const int cc = (q & 2) ? c : c - 1;
+      const int inode = 3 - q;
+      if (cr < 0 || cr >= nrows || cc < 0 || cc >= ncols) continue;
+      const int cell = cr + cc * nrows;
+      for (int j = cstart[cell]; j < cstart[cell + 1]; ++j) {
+        const int i = perm[j];
+        double xi, eta;
+        local_xy_g(p.x[i], p.y[i], cc, cr, G, ihx, ihy, xi, eta);
+        acc += shp(xi, eta, inode) * p.hp[i];
+      }
+    }
+    HV[n] = acc;
+  }
+}
+
 }  // namespace dampm

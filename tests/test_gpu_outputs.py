@@ -9,7 +9,7 @@ from oracle.oracle import Oracle
 OUT_FIELDS = ("apx", "apy", "Zp", "hpZ", "dZxp", "dZyp", "Fpx", "Fpy", "Fric_px",
               "Fric_py", "vpx_dx", "vpx_dy", "vpy_dx", "vpy_dy", "vpxL", "vpyL")
 NODAL = ("Mv", "mom_vx", "mom_vy", "avx", "avy", "vvx", "vvy", "vvxL", "vvyL", "FPxv",
-         "FPyv", "Fric_x", "Fric_y", "F_int_vx", "F_int_vy")
+         "FPyv", "Fric_x", "Fric_y", "F_int_vx", "F_int_vy", "HV")
 
 
 @pytest.mark.gpu
