@@ -1,0 +1,112 @@
+"""Batches of independent scenarios on one GPU (``dampm_batch_*``).
+
+Each scenario keeps its own grid, terrain, particles, physics and loop
+(fixed dt for NSTEPS passes or CFL until T); one launch per kernel advances
+all of them.  A scenario's numbers are the same alone (``Solver``) and in a
+batch.  The reference runs one DATA per process (main/optim_par.cpp:128-682);
+this is that loop body applied to many scenarios at once.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+
+from .data import DATA
+from .dampm import DampmError, _f64, _ptr, load_library, make_structs
+
+BATCH_FIELDS = ("x", "y", "vpx", "vpy", "hp", "F_11", "F_12", "F_22", "Mp", "Vp", "H",
+                "mom_px", "mom_py")
+
+
+class Batch:
+    """A set of scenarios resident in HBM, stepped together."""
+
+    def __init__(self, particle_cap: int, node_cap: int, scenario_cap: int,
+                 stream: Optional[int] = None):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.dampm_batch_create(int(particle_cap), int(node_cap), int(scenario_cap), 0,
+                                         C.c_void_p(stream or 0), C.byref(h))
+        if rc != 0:
+            raise DampmError(f"dampm_batch_create failed ({rc})")
+        self.h = h
+        self.np: Dict[int, int] = {}
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self.lib.dampm_batch_last_error(self.h).decode() if self.h else ""
+            raise DampmError(f"dampm batch call failed ({rc}): {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dampm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def footprint(d: DATA) -> Dict[str, int]:
+        """Capacity a scenario takes: particles and nodes."""
+        return {"particles": d.np, "nodes": d.nnodes}
+
+    def add(self, d: DATA) -> int:
+        d.validate()
+        g, p, _ = make_structs(d)
+        A = d.arrays
+        arrs = [_f64(A[k]) for k in ("x", "y", "Mp", "Ap", "vpx", "vpy", "hp", "mom_px",
+                                     "mom_py", "Vp")]
+        Z = _f64(A["Z"])
+        handle = C.c_int()
+        self._check(self.lib.dampm_batch_add(self.h, C.byref(g), C.byref(p), _ptr(Z), d.np,
+                                             *[_ptr(a) for a in arrs], C.byref(handle)))
+        self.np[handle.value] = d.np
+        return handle.value
+
+    def remove(self, handle: int):
+        self._check(self.lib.dampm_batch_remove(self.h, int(handle)))
+        self.np.pop(handle, None)
+
+    def compact(self):
+        self._check(self.lib.dampm_batch_compact(self.h))
+
+    def step(self, n: int = 1):
+        self._check(self.lib.dampm_batch_step(self.h, int(n)))
+
+    def sync(self):
+        self._check(self.lib.dampm_batch_sync(self.h))
+
+    def query(self, handle: int) -> Dict[str, float]:
+        it, t, dt, run, np_ = C.c_int(), C.c_double(), C.c_double(), C.c_int(), C.c_longlong()
+        self._check(self.lib.dampm_batch_query(self.h, int(handle), C.byref(it), C.byref(t),
+                                               C.byref(dt), C.byref(run), C.byref(np_)))
+        return {"it": it.value, "t": t.value, "dt": dt.value, "running": bool(run.value),
+                "np": np_.value}
+
+    def download(self, handle: int, name: str) -> np.ndarray:
+        out = np.empty(self.np[handle], dtype=np.float64)
+        self._check(self.lib.dampm_batch_download(self.h, int(handle), name.encode(), _ptr(out)))
+        return out
+
+    def ledgers(self, handle: int) -> np.ndarray:
+        out = np.empty(9, dtype=np.float64)
+        self._check(self.lib.dampm_batch_ledgers(self.h, int(handle), _ptr(out)))
+        return out
+
+    def usage(self) -> Dict[str, int]:
+        out = (C.c_longlong * 8)()
+        self._check(self.lib.dampm_batch_usage(self.h, out))
+        keys = ("live", "removed", "particles", "particle_cap", "nodes", "node_cap",
+                "scenario_cap", "launches")
+        return dict(zip(keys, [int(v) for v in out]))

@@ -1,0 +1,559 @@
+// batch_api.cu -- the extern "C" boundary of batches of independent scenarios
+// (include/dampm_cuda.h, dampm_batch_*).
+//
+// A batch packs many scenarios (each its own grid, terrain, particles,
+// rheology and loop: fixed dt for NSTEPS or CFL until T) back to back in one
+// set of device arrays and advances all of them with one launch per kernel
+// and pass.  Scenarios join at the end of the packed arrays (dampm_batch_add)
+// and leave by being marked dead (dampm_batch_remove); dampm_batch_compact
+// moves the live ones into the other half of a double buffer so that the
+// freed room can be reused.  Merge/split and recorded outputs are not part of
+// a batch.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dampm_cuda.h"
+#include "dampm_kernels.h"
+#include "host_util.h"
+
+using namespace dampm;
+
+namespace {
+
+struct HostScn {
+  int handle = -1;
+  Scn d{};  // the device table entry
+  dampm_grid grid{};
+  dampm_params params{};
+  long long nn = 0, nc = 0;
+};
+
+}  // namespace
+
+struct dampm_batch {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  long long P_cap = 0, N_cap = 0;
+  int S_cap = 0, STRIP_cap = 0, B_cap = 0;
+  long long USEG_cap = 0;
+  // packed totals (live and dead scenarios)
+  long long P_tot = 0, N_tot = 0, C_tot = 0, useg_tot = 0;
+  int strips_tot = 0, nblk = 0;
+  std::vector<HostScn> scns;  // packed order = device table order
+  int next_handle = 0;
+  // device
+  Particles p[2]{};
+  double* Z[2] = {nullptr, nullptr};
+  int cur = 0;
+  double *vvxL = nullptr, *vvyL = nullptr;
+  int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr;
+  int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr;
+  int* ustart = nullptr;
+  long long* upex = nullptr;
+  int2* uplan = nullptr;
+  int4* ulist = nullptr;
+  int *strip_n = nullptr, *ucount = nullptr, *strip_scn = nullptr;
+  double* led_part = nullptr;
+  int2 *scn_units = nullptr, *gblk = nullptr;
+  int4 *mblk = nullptr, *nmove = nullptr;
+  Scn* scn = nullptr;
+  Scalars *S = nullptr, *Sg = nullptr;
+  Scalars* Sh = nullptr;  // pinned mirror of S
+  int p2g_grid = 1;
+  long long launches = 0;
+  std::vector<void*> allocs;
+  std::string err;
+};
+
+namespace {
+
+#define BCK(call)                                                         \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      b->err = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+      return DAMPM_ERR_CUDA;                                              \
+    }                                                                     \
+  } while (0)
+
+int bfail(dampm_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  return code;
+}
+
+template <class T>
+int balloc(dampm_batch* b, T** ptr, size_t n) {
+  void* q = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+  if (e != cudaSuccess) {
+    b->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return DAMPM_ERR_CUDA;
+  }
+  b->allocs.push_back(q);
+  *ptr = static_cast<T*>(q);
+  return DAMPM_OK;
+}
+
+// the persistent per-particle arrays of one half of the double buffer
+int alloc_particles(dampm_batch* b, Particles& p) {
+  double** f[] = {&p.x,   &p.y,   &p.vpx, &p.vpy, &p.hp,  &p.F11, &p.F12, &p.F22,
+                  &p.Mp,  &p.Vp,  &p.H,   &p.mpx, &p.mpy, &p.qfx, &p.qfy, &p.qxi,
+                  &p.qeta, &p.qgx, &p.qgy, &p.Ap,  &p.Fbx, &p.Fby};
+  for (double** q : f) {
+    int rc = balloc(b, q, size_t(b->P_cap));
+    if (rc) return rc;
+  }
+  int** fi[] = {&p.label, &p.level, &p.key};
+  for (int** q : fi) {
+    int rc = balloc(b, q, size_t(b->P_cap));
+    if (rc) return rc;
+  }
+  return DAMPM_OK;
+}
+
+Particles shifted(const Particles& p, long long off) {
+  Particles q = p;
+  double** f[] = {&q.x,   &q.y,   &q.vpx, &q.vpy, &q.hp,  &q.F11, &q.F12, &q.F22,
+                  &q.Mp,  &q.Vp,  &q.H,   &q.mpx, &q.mpy, &q.qfx, &q.qfy, &q.qxi,
+                  &q.qeta, &q.qgx, &q.qgy, &q.Ap,  &q.Fbx, &q.Fby};
+  for (double** d : f)
+    if (*d) *d += off;
+  int** fi[] = {&q.label, &q.level, &q.key};
+  for (int** d : fi)
+    if (*d) *d += off;
+  return q;
+}
+
+int strips_of(const dampm_grid& g) { return (g.Ney + 1 + kTR - 1) / kTR; }
+
+// Rebuilds the strip and G2P block tables from the host scenario list and
+// uploads them with the scenario table and the batch totals.
+int upload_tables(dampm_batch* b) {
+  std::vector<int> strip_scn(std::max(b->strips_tot, 1));
+  std::vector<int2> gblk;
+  gblk.reserve(b->nblk);
+  std::vector<Scn> tab(b->scns.size());
+  for (size_t s = 0; s < b->scns.size(); ++s) {
+    const Scn& d = b->scns[s].d;
+    tab[s] = d;
+    for (int k = 0; k < d.nstrips; ++k) strip_scn[d.strip_off + k] = int(s);
+    for (int f = 0; f < d.np; f += kG2PThreads) gblk.push_back(make_int2(int(s), f));
+  }
+  b->nblk = int(gblk.size());
+  if (!tab.empty())
+    BCK(cudaMemcpyAsync(b->scn, tab.data(), sizeof(Scn) * tab.size(),
+                        cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(b->strip_scn, strip_scn.data(), sizeof(int) * strip_scn.size(),
+                      cudaMemcpyHostToDevice, b->stream));
+  if (!gblk.empty())
+    BCK(cudaMemcpyAsync(b->gblk, gblk.data(), sizeof(int2) * gblk.size(),
+                        cudaMemcpyHostToDevice, b->stream));
+  Scalars g{};
+  g.np = int(b->P_tot);
+  g.active = 1;
+  BCK(cudaMemcpyAsync(b->Sg, &g, sizeof(Scalars), cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));  // host vectors die here
+  return DAMPM_OK;
+}
+
+int find(dampm_batch* b, int handle) {
+  for (size_t s = 0; s < b->scns.size(); ++s)
+    if (b->scns[s].handle == handle) return int(s);
+  return -1;
+}
+
+int read_scalars(dampm_batch* b) {
+  if (b->scns.empty()) return DAMPM_OK;
+  BCK(cudaMemcpyAsync(b->Sh, b->S, sizeof(Scalars) * b->scns.size(),
+                      cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return DAMPM_OK;
+}
+
+// One pass of every live scenario.
+int enqueue_pass(dampm_batch* b) {
+  cudaStream_t st = b->stream;
+  const int nscn = int(b->scns.size());
+  const int ntiles = int((b->C_tot + kScanTile - 1) / kScanTile);
+  k_b_step_begin<<<1, 1024, 0, st>>>(b->scn, b->S, nscn, b->Sg);
+  const int gp = grid_blocks(b->P_tot, 256);
+  k_count<<<gp, 256, 0, st>>>(b->p[b->cur].key, b->count, b->slot, b->Sg);
+  k_scan_tiles<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(b->count, int(b->C_tot),
+                                                               b->tile_sum, b->Sg);
+  k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(b->tile_sum, ntiles, b->Sg);
+  k_list_reset<<<1, 1, 0, st>>>(b->clist_n, b->Sg);
+  k_scan_apply<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(
+      b->count, int(b->C_tot), b->tile_sum, b->start, b->clist, b->clist_n, b->Sg);
+  k_scatter<<<gp, 256, 0, st>>>(b->p[b->cur].key, b->slot, b->start, b->perm, b->Sg);
+  k_segment_order<<<148 * 8, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
+                                            b->Sg);
+  k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
+      b->start, b->scn, b->S, b->strip_scn, b->Sg, kUnitsPerCta * b->p2g_grid, b->ustart,
+      b->upex, b->uplan, b->strip_n);
+  k_b_units_flat<<<1, kPlanThreads, sizeof(int) * (b->strips_tot + 1), st>>>(
+      b->strip_n, b->strips_tot, b->strip_scn, b->scn, nscn, b->uplan, b->ulist,
+      b->ucount, b->scn_units, b->Sg);
+  k_b_p2g<<<b->p2g_grid, kP2GThreads, p2g_smem_bytes(), st>>>(
+      b->p[b->cur], b->perm, b->start, b->vvxL, b->vvyL, b->led_part, b->scn, b->S,
+      b->ulist, b->ucount, b->Sg);
+  k_b_ledger<<<nscn, 256, 0, st>>>(b->led_part, b->scn_units, b->scn, b->S, nscn,
+                                   b->Sg);
+  k_b_g2p<<<b->nblk, kG2PThreads, 0, st>>>(b->p[b->cur], b->vvxL, b->vvyL, b->Z[b->cur],
+                                           b->scn, b->S, b->gblk, b->Sg);
+  k_b_step_end<<<1, 1024, 0, st>>>(b->scn, b->S, nscn);
+  b->launches += 14;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  return DAMPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_cap,
+                       int precision, void* cuda_stream, dampm_batch** out) {
+  if (!out || particle_cap < 1 || node_cap < 4 || scenario_cap < 1 ||
+      particle_cap > 0x7fffffffLL || node_cap > 0x7fffffffLL)
+    return DAMPM_ERR_ARG;
+  if (precision != DAMPM_FP64) return DAMPM_ERR_ARG;
+  dampm_batch* b = new dampm_batch();
+  b->P_cap = particle_cap;
+  b->N_cap = node_cap;
+  b->S_cap = scenario_cap;
+  b->STRIP_cap = kMaxStrips;
+  b->USEG_cap = node_cap / 8 + 64LL * scenario_cap + 1024;
+  b->B_cap = int(particle_cap / kG2PThreads) + scenario_cap + 1;
+  if (cuda_stream) {
+    b->stream = static_cast<cudaStream_t>(cuda_stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete b;
+      return DAMPM_ERR_CUDA;
+    }
+    b->own_stream = true;
+  }
+  int rc = alloc_particles(b, b->p[0]);
+  rc = rc ? rc : alloc_particles(b, b->p[1]);
+  const size_t nn = size_t(node_cap), pc = size_t(particle_cap);
+  rc = rc ? rc : balloc(b, &b->Z[0], nn);
+  rc = rc ? rc : balloc(b, &b->Z[1], nn);
+  rc = rc ? rc : balloc(b, &b->vvxL, nn);
+  rc = rc ? rc : balloc(b, &b->vvyL, nn);
+  // cells of all scenarios: fewer than their nodes
+  rc = rc ? rc : balloc(b, &b->count, nn + 4);
+  rc = rc ? rc : balloc(b, &b->start, nn + 1);
+  rc = rc ? rc : balloc(b, &b->clist, nn + 4);
+  rc = rc ? rc : balloc(b, &b->clist_n, 4);
+  rc = rc ? rc : balloc(b, &b->tile_sum, nn / kScanTile + 2);
+  rc = rc ? rc : balloc(b, &b->slot, pc);
+  rc = rc ? rc : balloc(b, &b->perm, pc);
+  const size_t us = size_t(b->USEG_cap);
+  rc = rc ? rc : balloc(b, &b->ustart, us);
+  rc = rc ? rc : balloc(b, &b->upex, us);
+  rc = rc ? rc : balloc(b, &b->uplan, us);
+  rc = rc ? rc : balloc(b, &b->ulist, us);
+  rc = rc ? rc : balloc(b, &b->led_part, us * 6);
+  rc = rc ? rc : balloc(b, &b->strip_n, size_t(b->STRIP_cap));
+  rc = rc ? rc : balloc(b, &b->strip_scn, size_t(b->STRIP_cap));
+  rc = rc ? rc : balloc(b, &b->ucount, 2);
+  rc = rc ? rc : balloc(b, &b->scn_units, size_t(scenario_cap));
+  rc = rc ? rc : balloc(b, &b->gblk, size_t(b->B_cap));
+  rc = rc ? rc : balloc(b, &b->mblk, size_t(b->B_cap));
+  rc = rc ? rc : balloc(b, &b->nmove, nn / kG2PThreads + size_t(scenario_cap) + 1);
+  rc = rc ? rc : balloc(b, &b->scn, size_t(scenario_cap));
+  rc = rc ? rc : balloc(b, &b->S, size_t(scenario_cap));
+  rc = rc ? rc : balloc(b, &b->Sg, 1);
+  if (rc == DAMPM_OK &&
+      cudaMallocHost(&b->Sh, sizeof(Scalars) * size_t(scenario_cap)) != cudaSuccess)
+    rc = bfail(b, DAMPM_ERR_CUDA, "cudaMallocHost failed");
+  if (rc == DAMPM_OK) {
+    cudaMemsetAsync(b->count, 0, sizeof(int) * (nn + 4), b->stream);
+    cudaMemsetAsync(b->vvxL, 0, sizeof(double) * nn, b->stream);
+    cudaMemsetAsync(b->vvyL, 0, sizeof(double) * nn, b->stream);
+    cudaMemsetAsync(b->S, 0, sizeof(Scalars) * size_t(scenario_cap), b->stream);
+    cudaMemsetAsync(b->Sg, 0, sizeof(Scalars), b->stream);
+    const size_t smem = p2g_smem_bytes();
+    if (cudaFuncSetAttribute(k_b_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smem)) != cudaSuccess)
+      rc = bfail(b, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+    cudaFuncSetAttribute(k_b_p2g, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         int(cudaSharedmemCarveoutMaxShared));
+    int per_sm = 0, nsm = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_p2g, kP2GThreads, smem);
+    b->p2g_grid = std::max(1, nsm * std::max(per_sm, 1));
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) rc = DAMPM_ERR_CUDA;
+  }
+  if (rc != DAMPM_OK) {
+    dampm_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return DAMPM_OK;
+}
+
+int dampm_batch_destroy(dampm_batch* b) {
+  if (!b) return DAMPM_ERR_ARG;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (void* q : b->allocs) cudaFree(q);
+  if (b->Sh) cudaFreeHost(b->Sh);
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return DAMPM_OK;
+}
+
+const char* dampm_batch_last_error(dampm_batch* b) {
+  return b ? b->err.c_str() : "null batch";
+}
+
+int dampm_batch_add(dampm_batch* b, const dampm_grid* grid, const dampm_params* params,
+                    const double* Z, long long np, const double* x, const double* y,
+                    const double* Mp, const double* Ap, const double* vpx,
+                    const double* vpy, const double* hp, const double* mom_px,
+                    const double* mom_py, const double* Vp, int* handle) {
+  if (!b || !grid || !params || !Z || !handle || np < 1) return DAMPM_ERR_ARG;
+  if (!x || !y || !Mp || !Ap || !vpx || !vpy || !hp || !mom_px || !mom_py || !Vp)
+    return DAMPM_ERR_ARG;
+  if (grid->Nex < 1 || grid->Ney < 1 || !(grid->hx > 0) || !(grid->hy > 0))
+    return bfail(b, DAMPM_ERR_ARG, "bad grid");
+  HostScn h;
+  h.grid = *grid;
+  h.params = *params;
+  h.nn = (long long)(grid->Nex + 1) * (grid->Ney + 1);
+  h.nc = (long long)grid->Nex * grid->Ney;
+  const int nstrips = strips_of(*grid);
+  const long long useg = (long long)nstrips * (grid->Nex + 1);
+  const int blocks = int((np + kG2PThreads - 1) / kG2PThreads);
+  if (int(b->scns.size()) >= b->S_cap || b->P_tot + np > b->P_cap ||
+      b->N_tot + h.nn > b->N_cap || b->strips_tot + nstrips > b->STRIP_cap ||
+      b->useg_tot + useg > b->USEG_cap || b->nblk + blocks > b->B_cap)
+    return bfail(b, DAMPM_ERR_CAPACITY,
+                 "batch full: remove finished scenarios and compact, or create a larger batch");
+  Scn& d = h.d;
+  d.G = make_geom(*grid);
+  d.P = make_phys(*params);
+  d.p_off = int(b->P_tot);
+  d.np = int(np);
+  d.n_off = int(b->N_tot);
+  d.c_off = int(b->C_tot);
+  d.strip_off = b->strips_tot;
+  d.nstrips = nstrips;
+  d.useg_off = int(b->useg_tot);
+  d.live = 1;
+  h.handle = b->next_handle++;
+  const int pos = int(b->scns.size());
+  // particles and terrain into the current half
+  Particles p = shifted(b->p[b->cur], d.p_off);
+  const size_t by = sizeof(double) * size_t(np);
+  cudaStream_t st = b->stream;
+  BCK(cudaMemcpyAsync(p.x, x, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.y, y, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.Mp, Mp, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.Ap, Ap, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.vpx, vpx, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.vpy, vpy, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.hp, hp, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.mpx, mom_px, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.mpy, mom_py, by, cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(p.Vp, Vp, by, cudaMemcpyHostToDevice, st));
+  double* Zs = b->Z[b->cur] + d.n_off;
+  BCK(cudaMemcpyAsync(Zs, Z, sizeof(double) * size_t(h.nn), cudaMemcpyHostToDevice, st));
+  Scalars s0{};
+  s0.fresh = 1;
+  s0.np = int(np);
+  b->Sh[pos] = s0;
+  BCK(cudaMemcpyAsync(b->S + pos, b->Sh + pos, sizeof(Scalars), cudaMemcpyHostToDevice,
+                      st));
+  // the initial state of main/optim_par.cpp:239-264 (the terrain gradients
+  // only feed recorded outputs, which a batch does not keep, so Z stands in)
+  k_init_particles<<<grid_blocks(np, 256), 256, 0, st>>>(p, Zs, Zs, Zs, d.G, d.P,
+                                                         b->S + pos, int(np), d.c_off);
+  k_prep<<<grid_blocks(np, 256), 256, 0, st>>>(p, Zs, d.G, d.P, b->S + pos, 0);
+  b->launches += 2;
+  BCK(cudaGetLastError());
+  b->scns.push_back(h);
+  b->P_tot += np;
+  b->N_tot += h.nn;
+  b->C_tot += h.nc;
+  b->strips_tot += nstrips;
+  b->useg_tot += useg;
+  int rc = upload_tables(b);
+  if (rc) return rc;
+  *handle = h.handle;
+  return DAMPM_OK;
+}
+
+int dampm_batch_remove(dampm_batch* b, int handle) {
+  if (!b) return DAMPM_ERR_ARG;
+  const int s = find(b, handle);
+  if (s < 0) return bfail(b, DAMPM_ERR_ARG, "unknown scenario handle");
+  b->scns[s].d.live = 0;
+  b->scns[s].handle = -1;
+  const int live = 0;
+  BCK(cudaMemcpyAsync(reinterpret_cast<char*>(b->scn + s) + offsetof(Scn, live), &live,
+                      sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return DAMPM_OK;
+}
+
+int dampm_batch_compact(dampm_batch* b) {
+  if (!b) return DAMPM_ERR_ARG;
+  bool any_dead = false;
+  for (const HostScn& h : b->scns) any_dead |= !h.d.live;
+  if (!any_dead) return DAMPM_OK;
+  int rc = read_scalars(b);
+  if (rc) return rc;
+  std::vector<HostScn> keep;
+  std::vector<Scalars> S;
+  std::vector<int4> mv, nm;
+  long long P = 0, N = 0, C = 0, U = 0;
+  int strips = 0;
+  for (size_t s = 0; s < b->scns.size(); ++s) {
+    HostScn h = b->scns[s];
+    if (!h.d.live) continue;
+    const Scn old = h.d;
+    h.d.p_off = int(P);
+    h.d.n_off = int(N);
+    h.d.c_off = int(C);
+    h.d.strip_off = strips;
+    h.d.useg_off = int(U);
+    for (int f = 0; f < old.np; f += kG2PThreads)
+      mv.push_back(make_int4(h.d.p_off + f, old.p_off + f,
+                             std::min(kG2PThreads, old.np - f), h.d.c_off - old.c_off));
+    for (long long f = 0; f < h.nn; f += kG2PThreads)
+      nm.push_back(make_int4(int(h.d.n_off + f), int(old.n_off + f),
+                             int(std::min<long long>(kG2PThreads, h.nn - f)), 0));
+    P += old.np;
+    N += h.nn;
+    C += h.nc;
+    strips += old.nstrips;
+    U += (long long)old.nstrips * (h.grid.Nex + 1);
+    S.push_back(b->Sh[s]);
+    keep.push_back(h);
+  }
+  const int nxt = 1 - b->cur;
+  if (!mv.empty()) {
+    BCK(cudaMemcpyAsync(b->mblk, mv.data(), sizeof(int4) * mv.size(),
+                        cudaMemcpyHostToDevice, b->stream));
+    k_b_move<<<int(mv.size()), kG2PThreads, 0, b->stream>>>(b->p[nxt], b->p[b->cur],
+                                                            b->mblk);
+  }
+  if (!nm.empty()) {
+    BCK(cudaMemcpyAsync(b->nmove, nm.data(), sizeof(int4) * nm.size(),
+                        cudaMemcpyHostToDevice, b->stream));
+    k_b_move_nodes<<<int(nm.size()), kG2PThreads, 0, b->stream>>>(b->Z[nxt], b->Z[b->cur],
+                                                                  b->nmove);
+  }
+  for (size_t s = 0; s < S.size(); ++s) b->Sh[s] = S[s];
+  if (!S.empty())
+    BCK(cudaMemcpyAsync(b->S, b->Sh, sizeof(Scalars) * S.size(), cudaMemcpyHostToDevice,
+                        b->stream));
+  BCK(cudaGetLastError());
+  b->cur = nxt;
+  b->scns = keep;
+  b->P_tot = P;
+  b->N_tot = N;
+  b->C_tot = C;
+  b->strips_tot = strips;
+  b->useg_tot = U;
+  return upload_tables(b);
+}
+
+int dampm_batch_step(dampm_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return DAMPM_ERR_ARG;
+  if (b->scns.empty()) return DAMPM_OK;
+  for (int k = 0; k < nsteps; ++k) {
+    int rc = enqueue_pass(b);
+    if (rc) return rc;
+  }
+  return DAMPM_OK;
+}
+
+int dampm_batch_sync(dampm_batch* b) {
+  if (!b) return DAMPM_ERR_ARG;
+  int rc = read_scalars(b);
+  if (rc) return rc;
+  for (size_t s = 0; s < b->scns.size(); ++s)
+    if (b->scns[s].d.live && b->Sh[s].status)
+      return bfail(b, DAMPM_ERR_DEVICE, "device status word set");
+  return DAMPM_OK;
+}
+
+int dampm_batch_query(dampm_batch* b, int handle, int* it, double* t, double* dt_last,
+                      int* running, long long* np) {
+  if (!b) return DAMPM_ERR_ARG;
+  const int s = find(b, handle);
+  if (s < 0) return bfail(b, DAMPM_ERR_ARG, "unknown scenario handle");
+  int rc = read_scalars(b);
+  if (rc) return rc;
+  const Scalars& S = b->Sh[s];
+  const Phys& P = b->scns[s].d.P;
+  if (it) *it = S.it;
+  if (t) *t = S.t;
+  if (dt_last) *dt_last = S.dt;
+  // the loop condition of the next pass (main/optim_par.cpp:281)
+  if (running) *running = (S.status == 0) && (P.fixed ? (S.it < P.NSTEPS) : (S.t < P.T));
+  if (np) *np = b->scns[s].d.np;
+  return S.status ? bfail(b, DAMPM_ERR_DEVICE, "device status word set") : DAMPM_OK;
+}
+
+int dampm_batch_download(dampm_batch* b, int handle, const char* field, double* out) {
+  if (!b || !field || !out) return DAMPM_ERR_ARG;
+  const int s = find(b, handle);
+  if (s < 0) return bfail(b, DAMPM_ERR_ARG, "unknown scenario handle");
+  const Particles p = shifted(b->p[b->cur], b->scns[s].d.p_off);
+  const std::string f(field);
+  const double* src = nullptr;
+  if (f == "x") src = p.x;
+  else if (f == "y") src = p.y;
+  else if (f == "vpx") src = p.vpx;
+  else if (f == "vpy") src = p.vpy;
+  else if (f == "hp") src = p.hp;
+  else if (f == "F_11") src = p.F11;
+  else if (f == "F_12" || f == "F_21") src = p.F12;
+  else if (f == "F_22") src = p.F22;
+  else if (f == "Mp") src = p.Mp;
+  else if (f == "Vp") src = p.Vp;
+  else if (f == "H") src = p.H;
+  else if (f == "mom_px") src = p.mpx;
+  else if (f == "mom_py") src = p.mpy;
+  if (!src) return bfail(b, DAMPM_ERR_UNKNOWN_FIELD, "unknown batch field " + f);
+  BCK(cudaMemcpyAsync(out, src, sizeof(double) * size_t(b->scns[s].d.np),
+                      cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return DAMPM_OK;
+}
+
+int dampm_batch_ledgers(dampm_batch* b, int handle, double out[9]) {
+  if (!b || !out) return DAMPM_ERR_ARG;
+  const int s = find(b, handle);
+  if (s < 0) return bfail(b, DAMPM_ERR_ARG, "unknown scenario handle");
+  int rc = read_scalars(b);
+  if (rc) return rc;
+  for (int k = 0; k < 9; ++k) out[k] = b->Sh[s].ledger[k];
+  return DAMPM_OK;
+}
+
+int dampm_batch_usage(dampm_batch* b, long long out[8]) {
+  if (!b || !out) return DAMPM_ERR_ARG;
+  long long live = 0, dead = 0;
+  for (const HostScn& h : b->scns) (h.d.live ? live : dead) += 1;
+  out[0] = live;
+  out[1] = dead;
+  out[2] = b->P_tot;
+  out[3] = b->P_cap;
+  out[4] = b->N_tot;
+  out[5] = b->N_cap;
+  out[6] = b->S_cap;
+  out[7] = b->launches;
+  return DAMPM_OK;
+}
+
+}  // extern "C"

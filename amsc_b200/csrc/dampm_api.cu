@@ -12,6 +12,7 @@
 #include "../../include/dampm_cuda.h"
 #include "dampm_kernels.h"
 #include "ms_kernels.h"
+#include "host_util.h"
 
 using namespace dampm;
 
@@ -249,26 +250,6 @@ int sync_status(dampm_ctx* ctx) {
   return DAMPM_OK;
 }
 
-Phys make_phys(const dampm_params& d) {
-  Phys P{};
-  P.g = d.g;
-  P.rho = d.rho;
-  P.mu = d.mu;
-  P.tauy = d.tauy;
-  P.xi = d.xi;
-  const double fric_ang = d.phi * M_PI / 180.;  // main/optim_par.cpp:193
-  P.tan_fa = std::tan(fric_ang);
-  P.BING = d.BINGHAM_ON;
-  P.FON = d.FRICTION_ON;
-  P.CFL = d.CFL;
-  P.eq_level = d.eq_level;
-  P.DT_FIXED = d.DT_FIXED;
-  P.T = d.T;
-  P.BC = d.BC_FLAG;
-  P.NSTEPS = d.NSTEPS;
-  P.fixed = d.DT_FIXED > 0.0 ? 1 : 0;
-  return P;
-}
 
 __global__ void k_int_to_double(const int* a, double* b, const Scalars* S) {
   const int np = S->np;
@@ -326,17 +307,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
     ctx->ms = dampm_ms_params{0.9, 0.30, 0.0, 1e30, 0.05, 0.01, -2, 2, 2, 10, 1e9};
   }
   ctx->precision = precision;
-  ctx->G.nrows = grid->Ney;
-  ctx->G.ncols = grid->Nex;
-  ctx->G.hx = grid->hx;
-  ctx->G.hy = grid->hy;
-  ctx->G.Lx = grid->Nex * grid->hx;
-  ctx->G.Ly = grid->Ney * grid->hy;
-  {
-    int e;
-    ctx->G.hx_pow2 = std::frexp(grid->hx, &e) == 0.5 ? 1 : 0;
-    ctx->G.hy_pow2 = std::frexp(grid->hy, &e) == 0.5 ? 1 : 0;
-  }
+  ctx->G = make_geom(*grid);
   ctx->P = make_phys(*params);
   ctx->nn = int(nn);
   ctx->nc = grid->Nex * grid->Ney;
@@ -470,7 +441,7 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
   CK(cudaStreamSynchronize(ctx->stream));  // Sh is reused below
   if (np > 0) {
     k_init_particles<<<grid_for(np, 256), 256, 0, ctx->stream>>>(
-        p, ctx->Z, ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np));
+        p, ctx->Z, ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np), 0);
     k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->Z, ctx->G, ctx->P,
                                                        ctx->S, 0);
     CK(cudaGetLastError());

@@ -66,7 +66,7 @@ __global__ void k_step_begin(Scalars* S, Geom G, Phys P);
 __global__ void k_step_end(Scalars* S);
 __global__ void k_init_particles(Particles p, const double* Z,
                                  const double* dZdx, const double* dZdy,
-                                 Geom G, Phys P, Scalars* S, int np);
+                                 Geom G, Phys P, Scalars* S, int np, int key_off);
 __global__ void k_keys(const double* x, const double* y, int* key, Geom G,
                        const Scalars* S);
 __global__ void k_reduce_state(Particles p, Scalars* S);
@@ -99,6 +99,43 @@ __global__ void k_ledger_final(const double* led_part, const int* ucount,
                                Scalars* S);
 __global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
                       Phys P, Scalars* S, int record, int want_grad);
+
+// ---- batches of independent scenarios --------------------------------------
+// One scenario of a batch: its geometry, physics and place in the packed
+// arrays (particles, nodes and cells of all scenarios, back to back).
+struct Scn {
+  Geom G;
+  Phys P;
+  int p_off, np;           // particles [p_off, p_off + np)
+  int n_off;               // first node
+  int c_off;               // first cell (cell keys are c_off + r + c*nrows)
+  int strip_off, nstrips;  // its strips in the batch's strip order
+  int useg_off;            // first unit-plan slot of its first strip
+  int live;                // 0 once removed
+};
+
+__global__ void k_b_step_begin(const Scn* scn, Scalars* S, int nscn, Scalars* Sg);
+__global__ void k_b_step_end(const Scn* scn, Scalars* S, int nscn);
+__global__ void k_b_units_plan(const int* cstart, const Scn* scn, const Scalars* S,
+                               const int* strip_scn, const Scalars* Sg,
+                               int target_units, int* ustart, long long* upex,
+                               int2* plan, int* strip_n);
+__global__ void k_b_units_flat(const int* strip_n, int strips, const int* strip_scn,
+                               const Scn* scn, int nscn, const int2* plan,
+                               int4* ulist, int* ucount, int2* scn_units,
+                               const Scalars* Sg);
+__global__ void k_b_p2g(Particles p, const int* perm, const int* cstart,
+                        double* vvxL, double* vvyL, double* led_part,
+                        const Scn* scn, Scalars* S, const int4* ulist,
+                        const int* ucount, const Scalars* Sg);
+__global__ void k_b_ledger(const double* led_part, const int2* scn_units,
+                           const Scn* scn, Scalars* S, int nscn,
+                           const Scalars* Sg);
+__global__ void k_b_g2p(Particles p, const double* vvxL, const double* vvyL,
+                        const double* Z, const Scn* scn, Scalars* S,
+                        const int2* gblk, const Scalars* Sg);
+__global__ void k_b_move(Particles dst, Particles src, const int4* mblk);
+__global__ void k_b_move_nodes(double* dst, const double* src, const int4* nblk);
 
 __global__ void k_hv(const Particles p, const int* perm, const int* cstart,
                      double* HV, Geom G, const Scalars* S);

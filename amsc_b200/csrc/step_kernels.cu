@@ -19,8 +19,9 @@ namespace dampm {
 // ---------------------------------------------------------------------------
 // loop control
 // ---------------------------------------------------------------------------
-__global__ void k_step_begin(Scalars* S, Geom G, Phys P) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One scenario's pass start: the loop condition, dt, it++ (device side).
+__device__ __forceinline__ void step_begin_one(Scalars* S, const Geom& G,
+                                               const Phys& P) {
   const bool cond = P.fixed ? (S->it < P.NSTEPS) : (S->t < P.T);
   if (!cond || S->status != 0) {
     S->active = 0;
@@ -50,8 +51,7 @@ __global__ void k_step_begin(Scalars* S, Geom G, Phys P) {
   S->red_next[0] = S->red_next[1] = S->red_next[2] = 0ull;
 }
 
-__global__ void k_step_end(Scalars* S) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void step_end_one(Scalars* S) {
   if (!S->active) return;
   S->t += S->dt;
   S->fresh = 0;
@@ -60,13 +60,23 @@ __global__ void k_step_end(Scalars* S) {
   S->red_cur[2] = S->red_next[2];
 }
 
+__global__ void k_step_begin(Scalars* S, Geom G, Phys P) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  step_begin_one(S, G, P);
+}
+
+__global__ void k_step_end(Scalars* S) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  step_end_one(S);
+}
+
 // ---------------------------------------------------------------------------
 // initialisation after upload: main/optim_par.cpp:239-264
 // ---------------------------------------------------------------------------
 __global__ void k_init_particles(Particles p, const double* __restrict__ Z,
                                  const double* __restrict__ dZdx,
                                  const double* __restrict__ dZdy, Geom G,
-                                 Phys P, Scalars* S, int np) {
+                                 Phys P, Scalars* S, int np, int key_off) {
   __shared__ unsigned long long red[3];
   if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
   __syncthreads();
@@ -75,7 +85,7 @@ __global__ void k_init_particles(Particles p, const double* __restrict__ Z,
        i += gridDim.x * blockDim.x) {
     const double x = p.x[i], y = p.y[i];
     const int r = cell_row(y, G.hy, G.nrows), c = cell_col(x, G.hx, G.ncols);
-    p.key[i] = r + c * G.nrows;
+    p.key[i] = r + c * G.nrows + key_off;
     p.label[i] = i;
     p.level[i] = 0;
     double xi, eta;
@@ -729,23 +739,20 @@ __device__ __forceinline__ int column_count(const int* __restrict__ cstart,
 // starts a unit where floor(exclusive prefix / T) changes.  Pass B keeps the
 // units with particles (including those of the leading column cA-1, which
 // feed node column cA).
-__global__ void __launch_bounds__(kPlanThreads)
-    k_units_plan(const int* __restrict__ cstart, Geom G, const Scalars* S,
-                 int target_units, int seg, int* __restrict__ ustart,
-                 long long* __restrict__ upex, int2* __restrict__ plan,
-                 int* __restrict__ strip_n) {
-  if (!S->active) return;
+// Cuts strip `strip` of one grid (cstart of that grid's cells) into units
+// of weight about T; st/px are the strip's scratch, plan its output.  All
+// threads of the block call it; it returns the number of units kept.
+__device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
+                                          const Geom& G, long long T, int strip,
+                                          int* __restrict__ st,
+                                          long long* __restrict__ px,
+                                          int2* __restrict__ plan) {
   __shared__ long long wt_ll[32];
   __shared__ int wt_i[32];
   __shared__ long long last_id;
-  const int strip = blockIdx.x;
   const int nrows = G.nrows, ncols = G.ncols;
   const int r0 = strip * kTR;
   const int rlo = max(r0 - 1, 0), rhi = min(r0 + kTR - 1, nrows - 1);
-  long long T = (long long)S->np / max(target_units, 1);
-  if (T < kUnitMinWeight) T = kUnitMinWeight;
-  int* st = ustart + (size_t)strip * seg;
-  long long* px = upex + (size_t)strip * seg;
   long long carry = 0, prev_id = -1;
   int K = 0;
   for (int base = 0; base <= ncols; base += blockDim.x) {
@@ -792,9 +799,28 @@ __global__ void __launch_bounds__(kPlanThreads)
     }
     int jtot;
     const int jin = block_incl_scan<int>(flag, wt_i, jtot);
-    if (flag) plan[(size_t)strip * seg + J + jin - 1] = make_int2(cA, cB);
+    if (flag) plan[J + jin - 1] = make_int2(cA, cB);
     J += jtot;
   }
+  return J;
+}
+
+__device__ __forceinline__ long long unit_weight(const Scalars* S,
+                                                 int target_units) {
+  long long T = (long long)S->np / max(target_units, 1);
+  return T < kUnitMinWeight ? kUnitMinWeight : T;
+}
+
+__global__ void __launch_bounds__(kPlanThreads)
+    k_units_plan(const int* __restrict__ cstart, Geom G, const Scalars* S,
+                 int target_units, int seg, int* __restrict__ ustart,
+                 long long* __restrict__ upex, int2* __restrict__ plan,
+                 int* __restrict__ strip_n) {
+  if (!S->active) return;
+  const int strip = blockIdx.x;
+  const size_t b = (size_t)strip * seg;
+  const int J = plan_strip(cstart, G, unit_weight(S, target_units), strip,
+                           ustart + b, upex + b, plan + b);
   if (threadIdx.x == 0) strip_n[strip] = J;
 }
 
@@ -992,13 +1018,13 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
   }
 }
 
-__global__ void k_ledger_final(const double* __restrict__ led_part,
-                               const int* __restrict__ ucount, Scalars* S) {
-  if (!S->active) return;
-  const int nparts = ucount[0];
+// Block reduction, in a fixed order, of the ledger partials of units
+// [u0, u1) into S->ledger, and the conservation errors.
+__device__ __forceinline__ void ledger_reduce(const double* __restrict__ led_part,
+                                              int u0, int u1, Scalars* S) {
   __shared__ double sm[6][32];
   double v[6] = {0, 0, 0, 0, 0, 0};
-  for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+  for (int b = u0 + threadIdx.x; b < u1; b += blockDim.x)
 #pragma unroll
     for (int q = 0; q < 6; ++q) v[q] += led_part[(size_t)b * 6 + q];
 #pragma unroll
@@ -1028,146 +1054,154 @@ __global__ void k_ledger_final(const double* __restrict__ led_part,
   }
 }
 
+__global__ void k_ledger_final(const double* __restrict__ led_part,
+                               const int* __restrict__ ucount, Scalars* S) {
+  if (!S->active) return;
+  ledger_reduce(led_part, 0, ucount[0], S);
+}
+
 // ---------------------------------------------------------------------------
 // G2P: velocity, advection, velocity gradients at the new position with the
 // cell of the step start, height update, Bingham stress, next cell key and
 // the CFL max-reductions (main/optim_par.cpp:532-651).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kG2PThreads, 3)
-    k_g2p(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
-          Phys P, Scalars* S, int record, int want_grad) {
-  if (!S->active) return;
-  __shared__ unsigned long long red[3];
-  if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
-  __syncthreads();
-  const int np = S->np;
-  const double dt = S->dt;
+// One particle of G2P (the body of k_g2p and of the batched G2P).  key_off
+// is added to the cell key (the scenario's first cell in a batch).
+__device__ __forceinline__ void g2p_particle(
+    const Particles& p, int i, const Nodes& nodes, const double* __restrict__ Z,
+    const Geom& G, const Phys& P, const Shape& sh, double dt, int record,
+    int want_grad, int key_off, unsigned long long& m0, unsigned long long& m1,
+    unsigned long long& m2) {
   const int nrows = G.nrows, ncols = G.ncols;
   const double hx = G.hx, hy = G.hy;
-  const double ihx = 1.0 / hx, mihx = -1.0 / hx;
-  const double ihy = 1.0 / hy, mihy = -1.0 / hy;
+  const double ihx = sh.ihx, mihx = sh.mihx;
+  const double ihy = sh.ihy, mihy = sh.mihy;
   const double eps = 1e-10;
-  unsigned long long m0 = 0, m1 = 0, m2 = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
-       i += gridDim.x * blockDim.x) {
-    const int key = p.key[i];
-    const int r = key % nrows, c = key / nrows;
-    int nd[4];
-    double vxn[4], vyn[4];
+  const int key = p.key[i] - key_off;
+  const int r = key % nrows, c = key / nrows;
+  int nd[4];
+  double vxn[4], vyn[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      nd[k] = node_of(k, c, r, nrows);
-      vxn[k] = nodes.vvxL[nd[k]];
-      vyn[k] = nodes.vvyL[nd[k]];
-    }
-    double x = p.x[i], y = p.y[i];
-    double xi, eta;
-    local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
-    double vxL = 0.0, vyL = 0.0;
+  for (int k = 0; k < 4; ++k) {
+    nd[k] = node_of(k, c, r, nrows);
+    vxn[k] = nodes.vvxL[nd[k]];
+    vyn[k] = nodes.vvyL[nd[k]];
+  }
+  double x = p.x[i], y = p.y[i];
+  double xi, eta;
+  local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
+  double vxL = 0.0, vyL = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double N = shp(xi, eta, k);
+    vxL += N * vxn[k];
+    vyL += N * vyn[k];
+  }
+  if (record) {
+    // this step's intermediates as the reference's dprops hold them after
+    // the step (main/optim_par.cpp:387-459,542): apx/apy, grad Z and the
+    // gravity and friction forces of this step's P2G
+    double ax = 0.0, ay = 0.0, dzx = 0.0, dzy = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const double N = shp(xi, eta, k);
-      vxL += N * vxn[k];
-      vyL += N * vyn[k];
+      ax += N * nodes.avx[nd[k]];
+      ay += N * nodes.avy[nd[k]];
+      const double zn = Z[nd[k]];
+      dzx += shg_x(eta, k, ihx, mihx) * zn;
+      dzy += shg_y(xi, k, ihy, mihy) * zn;
     }
-    if (record) {
-      // this step's intermediates as the reference's dprops hold them after
-      // the step (main/optim_par.cpp:387-459,542): apx/apy, grad Z and the
-      // gravity and friction forces of this step's P2G
-      double ax = 0.0, ay = 0.0, dzx = 0.0, dzy = 0.0;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const double N = shp(xi, eta, k);
-        ax += N * nodes.avx[nd[k]];
-        ay += N * nodes.avy[nd[k]];
-        const double zn = Z[nd[k]];
-        dzx += shg_x(eta, k, ihx, mihx) * zn;
-        dzy += shg_y(xi, k, ihy, mihy) * zn;
-      }
-      p.apx[i] = ax;
-      p.apy[i] = ay;
-      p.dZxp[i] = dzx;
-      p.dZyp[i] = dzy;
-      p.Fpx[i] = p.qgx[i];
-      p.Fpy[i] = p.qgy[i];
-      p.Frx[i] = p.qfx[i];
-      p.Fry[i] = p.qfy[i];
-    }
-    const double vpx = vxL, vpy = vyL;
-    x = x + dt * vpx;
-    y = y + dt * vpy;
-    if (x < eps) x = eps;
-    if (x > G.Lx - eps) x = G.Lx - eps;
-    if (y < eps) y = eps;
-    if (y > G.Ly - eps) y = G.Ly - eps;
-    // g2pd {vvxL, vvyL} at the new position, old cell (main/optim_par.cpp:578)
-    local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
-    double vxdx = 0.0, vydx = 0.0, vxdy = 0.0, vydy = 0.0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const double Nx = shg_x(eta, k, ihx, mihx);
-      const double Ny = shg_y(xi, k, ihy, mihy);
-      vxdx += Nx * vxn[k];
-      vxdy += Ny * vxn[k];
-      vydx += Nx * vyn[k];
-      vydy += Ny * vyn[k];
-    }
-    // height from the strain rate (main/optim_par.cpp:595-599)
-    const double div = vxdx + vydy;
-    double hp = p.hp[i];
-    hp = hp / (1 + dt * div);
-    hp = hp < 1e-2 ? 1e-2 : hp;
-    double F11, F12, F22;
-    const double H = p.H[i];
-    bingham_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
-    p.x[i] = x;
-    p.y[i] = y;
-    p.vpx[i] = vpx;
-    p.vpy[i] = vpy;
-    p.hp[i] = hp;
-    p.F11[i] = F11;
-    p.F12[i] = F12;
-    p.F22[i] = F22;
-    const int nr = cell_row(y, hy, nrows), ncl = cell_col(x, hx, ncols);
-    p.key[i] = nr + ncl * nrows;
-    if (want_grad) {
-      p.vpx_dx[i] = vxdx;
-      p.vpx_dy[i] = vxdy;
-      p.vpy_dx[i] = vydx;
-      p.vpy_dy[i] = vydy;
-    }
-    // the record of the next P2G: what the reference stores at the end of
-    // the step (main/optim_par.cpp:600-626: momentum, Ap, basal friction) and
-    // the local coordinates and gravity force in the cell of the next
-    // binning (:387,447-454)
-    {
-      const double Mp = p.Mp[i], Vp = p.Vp[i];
-      p.mpx[i] = vpx * Mp;
-      p.mpy[i] = vpy * Mp;
-      const double Ap = hp > 1.e-2 ? Vp / hp : 0.0;
-      double fbx, fby;
-      voellmy(P, vpx, vpy, hp, fbx, fby);
-      p.qfx[i] = Ap * fbx;
-      p.qfy[i] = Ap * fby;
-      double qxi, qeta, qgx, qgy;
-      next_record(G, P, Z, x, y, hp, H, Vp, qxi, qeta, qgx, qgy);
-      p.qxi[i] = qxi;
-      p.qeta[i] = qeta;
-      p.qgx[i] = qgx;
-      p.qgy[i] = qgy;
-    }
-    if (record) {
-      // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
-      double zp = 0.0;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) zp += shp(xi, eta, k) * Z[nd[k]];
-      p.Zp[i] = zp;
-      p.hpZ[i] = hp + zp;
-    }
-    m0 = max(m0, ordered_key(fabs(vpx)));
-    m1 = max(m1, ordered_key(fabs(vpy)));
-    m2 = max(m2, ordered_key(hp));
+    p.apx[i] = ax;
+    p.apy[i] = ay;
+    p.dZxp[i] = dzx;
+    p.dZyp[i] = dzy;
+    p.Fpx[i] = p.qgx[i];
+    p.Fpy[i] = p.qgy[i];
+    p.Frx[i] = p.qfx[i];
+    p.Fry[i] = p.qfy[i];
   }
+  const double vpx = vxL, vpy = vyL;
+  x = x + dt * vpx;
+  y = y + dt * vpy;
+  if (x < eps) x = eps;
+  if (x > G.Lx - eps) x = G.Lx - eps;
+  if (y < eps) y = eps;
+  if (y > G.Ly - eps) y = G.Ly - eps;
+  // g2pd {vvxL, vvyL} at the new position, old cell (main/optim_par.cpp:578)
+  local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
+  double vxdx = 0.0, vydx = 0.0, vxdy = 0.0, vydy = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double Nx = shg_x(eta, k, ihx, mihx);
+    const double Ny = shg_y(xi, k, ihy, mihy);
+    vxdx += Nx * vxn[k];
+    vxdy += Ny * vxn[k];
+    vydx += Nx * vyn[k];
+    vydy += Ny * vyn[k];
+  }
+  // height from the strain rate (main/optim_par.cpp:595-599)
+  const double div = vxdx + vydy;
+  double hp = p.hp[i];
+  hp = hp / (1 + dt * div);
+  hp = hp < 1e-2 ? 1e-2 : hp;
+  double F11, F12, F22;
+  const double H = p.H[i];
+  bingham_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
+  p.x[i] = x;
+  p.y[i] = y;
+  p.vpx[i] = vpx;
+  p.vpy[i] = vpy;
+  p.hp[i] = hp;
+  p.F11[i] = F11;
+  p.F12[i] = F12;
+  p.F22[i] = F22;
+  const int nr = cell_row(y, hy, nrows), ncl = cell_col(x, hx, ncols);
+  p.key[i] = nr + ncl * nrows + key_off;
+  if (want_grad) {
+    p.vpx_dx[i] = vxdx;
+    p.vpx_dy[i] = vxdy;
+    p.vpy_dx[i] = vydx;
+    p.vpy_dy[i] = vydy;
+  }
+  // the record of the next P2G: what the reference stores at the end of
+  // the step (main/optim_par.cpp:600-626: momentum, Ap, basal friction) and
+  // the local coordinates and gravity force in the cell of the next
+  // binning (:387,447-454)
+  {
+    const double Mp = p.Mp[i], Vp = p.Vp[i];
+    p.mpx[i] = vpx * Mp;
+    p.mpy[i] = vpy * Mp;
+    const double Ap = hp > 1.e-2 ? Vp / hp : 0.0;
+    double fbx, fby;
+    voellmy(P, vpx, vpy, hp, fbx, fby);
+    p.qfx[i] = Ap * fbx;
+    p.qfy[i] = Ap * fby;
+    double qxi, qeta, qgx, qgy;
+    next_record(G, P, Z, x, y, hp, H, Vp, qxi, qeta, qgx, qgy);
+    p.qxi[i] = qxi;
+    p.qeta[i] = qeta;
+    p.qgx[i] = qgx;
+    p.qgy[i] = qgy;
+  }
+  if (record) {
+    // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
+    double zp = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) zp += shp(xi, eta, k) * Z[nd[k]];
+    p.Zp[i] = zp;
+    p.hpZ[i] = hp + zp;
+  }
+  m0 = max(m0, ordered_key(fabs(vpx)));
+  m1 = max(m1, ordered_key(fabs(vpy)));
+  m2 = max(m2, ordered_key(hp));
+}
+
+// Block reduction of the CFL maxima into one scenario's next-step slots.
+__device__ __forceinline__ void cfl_block_max(unsigned long long m0,
+                                              unsigned long long m1,
+                                              unsigned long long m2,
+                                              unsigned long long* red,
+                                              Scalars* S) {
   for (int o = 16; o > 0; o >>= 1) {
     m0 = max(m0, __shfl_xor_sync(0xffffffffu, m0, o));
     m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, o));
@@ -1186,7 +1220,219 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
   }
 }
 
+__global__ void __launch_bounds__(kG2PThreads, 3)
+    k_g2p(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
+          Phys P, Scalars* S, int record, int want_grad) {
+  if (!S->active) return;
+  __shared__ unsigned long long red[3];
+  if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
+  __syncthreads();
+  const int np = S->np;
+  const double dt = S->dt;
+  const Shape sh{1.0 / G.hx, -1.0 / G.hx, 1.0 / G.hy, -1.0 / G.hy};
+  unsigned long long m0 = 0, m1 = 0, m2 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x)
+    g2p_particle(p, i, nodes, Z, G, P, sh, dt, record, want_grad, 0, m0, m1, m2);
+  cfl_block_max(m0, m1, m2, red, S);
+}
+
 size_t p2g_smem_bytes() { return sizeof(P2GSmem); }
+
+// ---------------------------------------------------------------------------
+// BATCH: the same step over many independent scenarios packed back to back.
+// Each scenario keeps its own loop state (Scalars), geometry and physics; the
+// sort runs over the cells of all of them at once (keys are offset by each
+// scenario's first cell), P2G takes units of every scenario from one list,
+// and G2P runs one block per 256 particles of one scenario.  A scenario's
+// numbers are the same alone and in a batch: its sums run in the same
+// per-node order whatever the unit cuts.
+// ---------------------------------------------------------------------------
+__global__ void k_b_step_begin(const Scn* __restrict__ scn, Scalars* S, int nscn,
+                               Scalars* Sg) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < nscn; s += blockDim.x) {
+    if (scn[s].live) {
+      step_begin_one(&S[s], scn[s].G, scn[s].P);
+      if (S[s].active) atomicOr(&any, 1);
+    } else {
+      S[s].active = 0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) Sg->active = any;
+}
+
+__global__ void k_b_step_end(const Scn* __restrict__ scn, Scalars* S, int nscn) {
+  for (int s = threadIdx.x; s < nscn; s += blockDim.x)
+    if (scn[s].live) step_end_one(&S[s]);
+}
+
+// one block per strip of the batch
+__global__ void __launch_bounds__(kPlanThreads)
+    k_b_units_plan(const int* __restrict__ cstart, const Scn* __restrict__ scn,
+                   const Scalars* S, const int* __restrict__ strip_scn,
+                   const Scalars* Sg, int target_units, int* __restrict__ ustart,
+                   long long* __restrict__ upex, int2* __restrict__ plan,
+                   int* __restrict__ strip_n) {
+  const int b = blockIdx.x;
+  const int s = strip_scn[b];
+  if (!Sg->active || !S[s].active) {
+    if (threadIdx.x == 0) strip_n[b] = 0;
+    return;
+  }
+  const Geom G = scn[s].G;
+  const int local = b - scn[s].strip_off;
+  const size_t base = (size_t)scn[s].useg_off + (size_t)local * (G.ncols + 1);
+  const int J = plan_strip(cstart + scn[s].c_off, G, unit_weight(Sg, target_units),
+                           local, ustart + base, upex + base, plan + base);
+  if (threadIdx.x == 0) strip_n[b] = J;
+}
+
+// one block: the flat list {scenario, strip, cA, cB} in strip order, and each
+// scenario's range of list positions (its ledger slots)
+__global__ void __launch_bounds__(kPlanThreads)
+    k_b_units_flat(const int* __restrict__ strip_n, int strips,
+                   const int* __restrict__ strip_scn, const Scn* __restrict__ scn,
+                   int nscn, const int2* __restrict__ plan, int4* __restrict__ ulist,
+                   int* __restrict__ ucount, int2* __restrict__ scn_units,
+                   const Scalars* Sg) {
+  if (!Sg->active) return;
+  extern __shared__ int uoff[];  // strips + 1
+  __shared__ int wt_i[32];
+  int carry = 0;
+  for (int base = 0; base < strips; base += blockDim.x) {
+    const int b = base + threadIdx.x;
+    const int n = b < strips ? strip_n[b] : 0;
+    int tot;
+    const int incl = block_incl_scan<int>(n, wt_i, tot);
+    if (b < strips) uoff[b] = carry + incl - n;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) uoff[strips] = carry;
+  __syncthreads();
+  const int total = carry;
+  for (int f = threadIdx.x; f < total; f += blockDim.x) {
+    int lo = 0, hi = strips;  // uoff[lo] <= f < uoff[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (uoff[mid] <= f) lo = mid; else hi = mid;
+    }
+    const int s = strip_scn[lo];
+    const int local = lo - scn[s].strip_off;
+    const size_t base =
+        (size_t)scn[s].useg_off + (size_t)local * (scn[s].G.ncols + 1);
+    const int2 u = plan[base + (f - uoff[lo])];
+    ulist[f] = make_int4(s, local, u.x, u.y);
+  }
+  for (int s = threadIdx.x; s < nscn; s += blockDim.x) {
+    const int b0 = scn[s].strip_off, b1 = b0 + scn[s].nstrips;
+    scn_units[s] = make_int2(uoff[b0], uoff[b1]);
+  }
+  if (threadIdx.x == 0) {
+    ucount[0] = total;
+    ucount[1] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
+    k_b_p2g(Particles p, const int* __restrict__ perm, const int* __restrict__ cstart,
+            double* __restrict__ vvxL, double* __restrict__ vvyL,
+            double* __restrict__ led_part, const Scn* __restrict__ scn, Scalars* S,
+            const int4* __restrict__ ulist, const int* __restrict__ ucount,
+            const Scalars* Sg) {
+  if (!Sg->active) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
+  const int nunits = ucount[0];
+  __shared__ int next_unit;
+  while (true) {
+    if (threadIdx.x == 0) next_unit = atomicAdd(const_cast<int*>(ucount) + 1, 1);
+    __syncthreads();
+    const int ui = next_unit;
+    __syncthreads();
+    if (ui >= nunits) break;
+    const int4 u = ulist[ui];
+    const Geom G = scn[u.x].G;
+    const Phys P = scn[u.x].P;
+    const int n_off = scn[u.x].n_off, c_off = scn[u.x].c_off;
+    Nodes nd{};
+    nd.vvxL = vvxL + n_off;
+    nd.vvyL = vvyL + n_off;
+    p2g_unit(p, perm, cstart + c_off, nd, led_part, G, P, &S[u.x], 0, sm, ui,
+             make_int4(u.y, u.z, u.w, 0));
+  }
+}
+
+// one block per scenario
+__global__ void k_b_ledger(const double* __restrict__ led_part,
+                           const int2* __restrict__ scn_units,
+                           const Scn* __restrict__ scn, Scalars* S, int nscn,
+                           const Scalars* Sg) {
+  const int s = blockIdx.x;
+  if (!Sg->active || s >= nscn || !scn[s].live || !S[s].active) return;
+  ledger_reduce(led_part, scn_units[s].x, scn_units[s].y, &S[s]);
+}
+
+// gblk[b] = {scenario, its first particle handled by block b}
+__global__ void __launch_bounds__(kG2PThreads, 3)
+    k_b_g2p(Particles p, const double* __restrict__ vvxL,
+            const double* __restrict__ vvyL, const double* __restrict__ Z,
+            const Scn* __restrict__ scn, Scalars* S, const int2* __restrict__ gblk,
+            const Scalars* Sg) {
+  if (!Sg->active) return;
+  const int2 e = gblk[blockIdx.x];
+  const int s = e.x;
+  if (!S[s].active) return;  // block-uniform
+  __shared__ unsigned long long red[3];
+  if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
+  __syncthreads();
+  const Geom G = scn[s].G;
+  const Phys P = scn[s].P;
+  const int p_off = scn[s].p_off, np = scn[s].np;
+  const int n_off = scn[s].n_off, c_off = scn[s].c_off;
+  Nodes nd{};
+  nd.vvxL = const_cast<double*>(vvxL) + n_off;
+  nd.vvyL = const_cast<double*>(vvyL) + n_off;
+  const Shape sh{1.0 / G.hx, -1.0 / G.hx, 1.0 / G.hy, -1.0 / G.hy};
+  unsigned long long m0 = 0, m1 = 0, m2 = 0;
+  const int li = e.y + threadIdx.x;
+  if (li < np)
+    g2p_particle(p, p_off + li, nd, Z + n_off, G, P, sh, S[s].dt, 0, 0, c_off, m0,
+                 m1, m2);
+  cfl_block_max(m0, m1, m2, red, &S[s]);
+}
+
+// Compaction of a batch into the other half of its double buffer:
+// mblk[b] = {destination first particle, source first particle, count <= 256,
+// cell-key shift}.
+__global__ void k_b_move(Particles dst, Particles src, const int4* __restrict__ mblk) {
+  const int4 m = mblk[blockIdx.x];
+  if ((int)threadIdx.x >= m.z) return;
+  const int i = m.y + threadIdx.x, o = m.x + threadIdx.x;
+  double* const* df[] = {&dst.x, &dst.y, &dst.vpx, &dst.vpy, &dst.hp, &dst.F11,
+                         &dst.F12, &dst.F22, &dst.Mp, &dst.Vp, &dst.H, &dst.mpx,
+                         &dst.mpy, &dst.qfx, &dst.qfy, &dst.qxi, &dst.qeta, &dst.qgx,
+                         &dst.qgy, &dst.Ap, &dst.Fbx, &dst.Fby};
+  double* const* sf[] = {&src.x, &src.y, &src.vpx, &src.vpy, &src.hp, &src.F11,
+                         &src.F12, &src.F22, &src.Mp, &src.Vp, &src.H, &src.mpx,
+                         &src.mpy, &src.qfx, &src.qfy, &src.qxi, &src.qeta, &src.qgx,
+                         &src.qgy, &src.Ap, &src.Fbx, &src.Fby};
+#pragma unroll
+  for (int f = 0; f < 22; ++f) (*df[f])[o] = (*sf[f])[i];
+  dst.label[o] = src.label[i];
+  dst.level[o] = src.level[i];
+  dst.key[o] = src.key[i] + m.w;
+}
+
+// nblk[b] = {destination first node, source first node, count <= 256, 0}
+__global__ void k_b_move_nodes(double* __restrict__ dst, const double* __restrict__ src,
+                               const int4* __restrict__ nblk) {
+  const int4 m = nblk[blockIdx.x];
+  if ((int)threadIdx.x < m.z) dst[m.x + threadIdx.x] = src[m.y + threadIdx.x];
+}
 
 // HV: p2g of the updated depth hp at the updated positions, each particle
 // still in the cell it was binned to at the start of the step

@@ -85,6 +85,21 @@ def _declare(lib):
         "dampm_last_timings": (C.c_int, [P, C.c_int, _DP]),
         "dampm_last_error": (C.c_char_p, [P]),
         "dampm_version": (C.c_char_p, []),
+        "dampm_batch_create": (C.c_int, [C.c_longlong, C.c_longlong, C.c_int, C.c_int, P,
+                                         C.POINTER(P)]),
+        "dampm_batch_destroy": (C.c_int, [P]),
+        "dampm_batch_add": (C.c_int, [P, C.POINTER(dampm_grid), C.POINTER(dampm_params), _DP,
+                                      C.c_longlong] + [_DP] * 10 + [C.POINTER(C.c_int)]),
+        "dampm_batch_remove": (C.c_int, [P, C.c_int]),
+        "dampm_batch_compact": (C.c_int, [P]),
+        "dampm_batch_step": (C.c_int, [P, C.c_int]),
+        "dampm_batch_sync": (C.c_int, [P]),
+        "dampm_batch_query": (C.c_int, [P, C.c_int, C.POINTER(C.c_int), _DP, _DP,
+                                        C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+        "dampm_batch_download": (C.c_int, [P, C.c_int, C.c_char_p, _DP]),
+        "dampm_batch_ledgers": (C.c_int, [P, C.c_int, _DP]),
+        "dampm_batch_usage": (C.c_int, [P, C.POINTER(C.c_longlong)]),
+        "dampm_batch_last_error": (C.c_char_p, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

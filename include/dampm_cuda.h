@@ -206,6 +206,63 @@ int dampm_cfl_dt_noalloc(const double* vpx, const double* vpy,
                          const double* hp, long long np, double g, double CFL,
                          double hx, double hy, double* out, void* cuda_stream);
 
+/* ---- Batches of independent scenarios -------------------------------------
+ * One set of device arrays holds many scenarios back to back, each with its
+ * own grid, terrain, particles, physics and loop (fixed dt for NSTEPS passes,
+ * or CFL until T); one launch per kernel advances all of them.  A scenario's
+ * numbers are the same alone (dampm_ctx) and in a batch.  There is no
+ * counterpart in the reference, which runs one DATA per process
+ * (main/optim_par.cpp:128-682); the batch applies that loop body to each
+ * scenario.  Merge/split and recorded outputs are not part of a batch. */
+typedef struct dampm_batch dampm_batch;
+
+/* Capacities: total particles and total nodes over the scenarios the batch
+ * holds at once (live and removed-but-not-compacted), and scenario slots.
+ * Device memory is allocated here once: ~390 B per particle and ~56 B per
+ * node of capacity. */
+int dampm_batch_create(long long particle_cap, long long node_cap,
+                       int scenario_cap, int precision, void* cuda_stream,
+                       dampm_batch** out);
+int dampm_batch_destroy(dampm_batch* b);
+
+/* Appends one scenario (DATA arrays in DATA order, terrain Z in quadgrid node
+ * order; the gradients dZdx/dZdy only feed recorded outputs and are not
+ * taken).  Returns DAMPM_ERR_CAPACITY when the batch is full.  *handle
+ * identifies the scenario in later calls. */
+int dampm_batch_add(dampm_batch* b, const dampm_grid* grid,
+                    const dampm_params* params, const double* Z, long long np,
+                    const double* x, const double* y, const double* Mp,
+                    const double* Ap, const double* vpx, const double* vpy,
+                    const double* hp, const double* mom_px, const double* mom_py,
+                    const double* Vp, int* handle);
+
+/* Stops a scenario; its room is reclaimed by dampm_batch_compact, which moves
+ * the live scenarios together (a synchronising call). */
+int dampm_batch_remove(dampm_batch* b, int handle);
+int dampm_batch_compact(dampm_batch* b);
+
+/* Enqueues nsteps passes of every live scenario (asynchronous); a scenario
+ * whose loop condition fails does nothing in a pass. */
+int dampm_batch_step(dampm_batch* b, int nsteps);
+int dampm_batch_sync(dampm_batch* b);
+
+/* Loop state of one scenario (synchronises): iteration, time, last dt,
+ * whether its loop condition still holds, particle count. */
+int dampm_batch_query(dampm_batch* b, int handle, int* it, double* t,
+                      double* dt_last, int* running, long long* np);
+
+/* One particle field of one scenario, reference index order: x, y, vpx, vpy,
+ * hp, F_11, F_12 (= F_21), F_22, Mp, Vp, H, mom_px, mom_py. */
+int dampm_batch_download(dampm_batch* b, int handle, const char* field,
+                         double* out);
+int dampm_batch_ledgers(dampm_batch* b, int handle, double out[9]);
+
+/* {live scenarios, removed scenarios awaiting compaction, particles held,
+ *  particle capacity, nodes held, node capacity, scenario slots, kernel
+ *  launches so far}: what an admission policy needs. */
+int dampm_batch_usage(dampm_batch* b, long long out[8]);
+const char* dampm_batch_last_error(dampm_batch* b);
+
 #ifdef __cplusplus
 }
 #endif
