@@ -51,7 +51,7 @@ struct dampm_batch {
   int cur = 0;
   double *vvxL = nullptr, *vvyL = nullptr;
   int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr;
-  int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr;
+  int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr, *cbig = nullptr;
   int* ustart = nullptr;
   long long* upex = nullptr;
   int2* uplan = nullptr;
@@ -191,7 +191,9 @@ int enqueue_pass(dampm_batch* b) {
       b->count, int(b->C_tot), b->tile_sum, b->start, b->clist, b->clist_n, b->Sg);
   k_scatter<<<gp, 256, 0, st>>>(b->p[b->cur].key, b->slot, b->start, b->perm, b->Sg);
   k_segment_order<<<148 * 8, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
-                                            b->Sg);
+                                            b->cbig, b->Sg);
+  k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
+                                            b->slot, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
       b->start, b->scn, b->S, b->strip_scn, b->Sg, kUnitsPerCta * b->p2g_grid, b->ustart,
       b->upex, b->uplan, b->strip_n);
@@ -206,7 +208,7 @@ int enqueue_pass(dampm_batch* b) {
   k_b_g2p<<<b->nblk, kG2PThreads, 0, st>>>(b->p[b->cur], b->vvxL, b->vvyL, b->Z[b->cur],
                                            b->scn, b->S, b->gblk, b->Sg);
   k_b_step_end<<<1, 1024, 0, st>>>(b->scn, b->S, nscn);
-  b->launches += 14;
+  b->launches += 15;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
   return DAMPM_OK;
@@ -253,6 +255,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   rc = rc ? rc : balloc(b, &b->tile_sum, nn / kScanTile + 2);
   rc = rc ? rc : balloc(b, &b->slot, pc);
   rc = rc ? rc : balloc(b, &b->perm, pc);
+  rc = rc ? rc : balloc(b, &b->cbig, pc / 256 + 4);
   const size_t us = size_t(b->USEG_cap);
   rc = rc ? rc : balloc(b, &b->ustart, us);
   rc = rc ? rc : balloc(b, &b->upex, us);

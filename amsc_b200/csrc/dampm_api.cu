@@ -41,6 +41,7 @@ struct dampm_ctx {
   int2* uplan = nullptr;
   int4* ulist = nullptr;
   int *clist = nullptr, *clist_n = nullptr;  // cells with >= 2 particles
+  int* cbig = nullptr;  // cells with more than 256 particles (capacity / 256)
   int p2g_grid = 0;
   Scalars* S = nullptr;
   Scalars* Sh = nullptr;  // pinned host mirror
@@ -153,6 +154,10 @@ int alloc_particles(dampm_ctx* ctx, long long cap) {
     int rc = dalloc(ctx, q, cap);
     if (rc) return rc;
   }
+  {
+    int rc = dalloc(ctx, &ctx->cbig, size_t(cap / 256 + 4));
+    if (rc) return rc;
+  }
   int rc = ms_alloc(ctx->msb, cap, ctx->nc, [&](void** q, size_t bytes) {
     return dalloc(ctx, reinterpret_cast<unsigned char**>(q), bytes);
   });
@@ -175,8 +180,11 @@ void enqueue_sort(dampm_ctx* ctx) {
   k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->slot, ctx->start,
                                          ctx->perm, ctx->S);
   k_segment_order<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,
-                                                   ctx->clist_n, ctx->perm, ctx->S);
-  ctx->launches += 7;
+                                                   ctx->clist_n, ctx->perm, ctx->cbig,
+                                                   ctx->S);
+  k_segment_order_big<<<148, 1024, 0, ctx->stream>>>(ctx->start, ctx->cbig, ctx->clist_n,
+                                                     ctx->perm, ctx->slot, ctx->S);
+  ctx->launches += 8;
 }
 
 int enqueue_pass(dampm_ctx* ctx) {

@@ -83,8 +83,11 @@ __global__ void k_scan_apply(int* count, int n, const int* tile_sum,
 __global__ void k_list_reset(int* list_n, const Scalars* S);
 __global__ void k_scatter(const int* key, const int* slot, const int* start,
                           int* perm, const Scalars* S);
-__global__ void k_segment_order(const int* start, const int* list,
-                                const int* list_n, int* perm, const Scalars* S);
+__global__ void k_segment_order(const int* start, const int* list, int* list_n,
+                                int* perm, int* big, const Scalars* S);
+__global__ void k_segment_order_big(const int* start, const int* big,
+                                    const int* list_n, int* perm, int* tmp,
+                                    const Scalars* S);
 __global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
                              int target_units, int seg, int* ustart,
                              long long* upex, int2* plan, int* strip_n);

@@ -362,25 +362,32 @@ __global__ void k_scatter(const int* __restrict__ key,
     perm[start[key[i]] + slot[i]] = i;
 }
 
+// list_n[0]: cells with two or more particles; list_n[1]: crowded cells
+// handed on to k_segment_order_big
 __global__ void k_list_reset(int* list_n, const Scalars* S) {
-  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) *list_n = 0;
+  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) {
+    list_n[0] = 0;
+    list_n[1] = 0;
+  }
 }
 
 // Orders each listed cell's segment by ascending particle index (the atomics
 // of k_count hand out slots in arbitrary order).  One warp per cell: a
 // register bitonic sort for up to 32 particles; a rank sort for up to
 // 32 * kRankPer (each lane holds kRankPer indices and counts, over all the
-// cell's indices broadcast lane by lane, those below each of its own); an
-// insertion sort by lane 0 beyond.  Particle indices are unique, so the
-// ranks are a permutation of [0, m).
+// cell's indices broadcast lane by lane, those below each of its own).
+// Particle indices are unique, so the ranks are a permutation of [0, m).
+// Larger cells are listed in `big` for k_segment_order_big.
 constexpr int kRankPer = 8;
+constexpr int kBigRun = 8192;
 
 // (eight resident blocks per SM for the common small cells; the rank sort's
 // registers may spill for the rare crowded ones)
 __global__ void __launch_bounds__(256, 8) k_segment_order(const int* __restrict__ start,
                                 const int* __restrict__ list,
-                                const int* __restrict__ list_n,
-                                int* __restrict__ perm, const Scalars* S) {
+                                int* __restrict__ list_n,
+                                int* __restrict__ perm, int* __restrict__ big,
+                                const Scalars* S) {
   if (!S->active) return;
   const int lane = threadIdx.x & 31;
   const int nl = *list_n;
@@ -425,16 +432,78 @@ __global__ void __launch_bounds__(256, 8) k_segment_order(const int* __restrict_
       for (int t = 0; t < kRankPer; ++t)
         if (lane + 32 * t < m) perm[b + rank[t]] = v[t];
     } else if (lane == 0) {
-      for (int j = b + 1; j < e; ++j) {
-        const int v = perm[j];
-        int k = j - 1;
-        while (k >= b && perm[k] > v) {
-          perm[k + 1] = perm[k];
-          --k;
-        }
-        perm[k + 1] = v;
-      }
+      big[atomicAdd(&list_n[1], 1)] = c;
     }
+  }
+}
+
+// Crowded cells (more than 32 * kRankPer particles), one block of 1024
+// threads each: runs of up to kBigRun indices are sorted by a bitonic network
+// in shared memory; longer cells then merge the sorted runs pairwise (each
+// output position finds its split by a binary search along the merge path),
+// ping-ponging between perm and tmp (the sort's slot array, free once the
+// scatter has run).
+__global__ void __launch_bounds__(1024)
+    k_segment_order_big(const int* __restrict__ start, const int* __restrict__ big,
+                        const int* __restrict__ list_n, int* __restrict__ perm,
+                        int* __restrict__ tmp, const Scalars* S) {
+  if (!S->active) return;
+  __shared__ int sv[kBigRun];
+  const int nb = list_n[1];
+  for (int q = blockIdx.x; q < nb; q += gridDim.x) {
+    const int c = big[q];
+    const int b = start[c], m = start[c + 1] - b;
+    for (int r0 = 0; r0 < m; r0 += kBigRun) {
+      const int len = min(kBigRun, m - r0);
+      int P = 1;
+      while (P < len) P <<= 1;
+      for (int i = threadIdx.x; i < P; i += blockDim.x)
+        sv[i] = (i < len) ? perm[b + r0 + i] : 0x7fffffff;
+      __syncthreads();
+      for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const int ixj = i ^ j;
+            if (ixj > i) {
+              const int a = sv[i], d = sv[ixj];
+              if ((a > d) == ((i & k) == 0)) {
+                sv[i] = d;
+                sv[ixj] = a;
+              }
+            }
+          }
+          __syncthreads();
+        }
+      }
+      for (int i = threadIdx.x; i < len; i += blockDim.x) perm[b + r0 + i] = sv[i];
+      __syncthreads();
+    }
+    int* src = perm + b;
+    int* dst = tmp + b;
+    for (int w = kBigRun; w < m; w <<= 1) {
+      for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const int lo = (k / (2 * w)) * (2 * w);
+        const int la = min(w, m - lo), lb = max(0, min(w, m - lo - la));
+        const int* A = src + lo;
+        const int* B = A + la;
+        const int kk = k - lo;
+        int i0 = max(0, kk - lb), i1 = min(kk, la);
+        while (i0 < i1) {
+          const int mid = (i0 + i1) >> 1;
+          if (A[mid] < B[kk - mid - 1]) i0 = mid + 1; else i1 = mid;
+        }
+        const int j = kk - i0;
+        dst[k] = (j >= lb || (i0 < la && A[i0] < B[j])) ? A[i0] : B[j];
+      }
+      __syncthreads();
+      int* t = src;
+      src = dst;
+      dst = t;
+    }
+    if (src != perm + b) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) perm[b + i] = src[i];
+    }
+    __syncthreads();
   }
 }
 

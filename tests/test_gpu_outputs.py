@@ -82,6 +82,26 @@ def test_edge_pileup_and_walls(cuda_lib):
 
 
 @pytest.mark.gpu
+def test_cell_with_twenty_thousand_particles(cuda_lib):
+    """One cell holding 20,000 particles: its index order comes from sorted
+    runs of 8192 merged pairwise (k_segment_order_big)."""
+    d = scenarios.bench_slab(30000, nsteps=3)
+    x, y = d.arrays["x"].copy(), d.arrays["y"].copy()
+    rng = np.random.default_rng(7)
+    pick = rng.permutation(x.size)[:20000]
+    hx = float(d.scalars["hx"])
+    x[pick] = 40.3 * hx + 0.2 * hx * rng.random(20000)
+    y[pick] = 5.3 * hx + 0.2 * hx * rng.random(20000)
+    d.arrays["x"], d.arrays["y"] = x, y
+    o = Oracle(d, threads=8)
+    o.run(3)
+    with Solver(d) as s:
+        s.step(3)
+        for k in ("x", "y", "vpx", "vpy", "hp", "F_11", "F_22"):
+            np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+
+
+@pytest.mark.gpu
 def test_odd_grid_and_non_pow2_spacing(cuda_lib):
     """Lake at rest (hx = 0.2, not a power of two; BC off) on a 50x50 grid and
     a 37x23 rectangular grid."""
