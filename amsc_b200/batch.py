@@ -104,6 +104,16 @@ class Batch:
         self._check(self.lib.dampm_batch_ledgers(self.h, int(handle), _ptr(out)))
         return out
 
+    def states(self) -> Dict[int, Dict[str, float]]:
+        """Loop state of every live scenario, one synchronisation."""
+        cap = max(len(self.np), 1)
+        hs, run, its = (C.c_int * cap)(), (C.c_int * cap)(), (C.c_int * cap)()
+        ts = (C.c_double * cap)()
+        n = C.c_int()
+        self._check(self.lib.dampm_batch_states(self.h, cap, hs, run, its, ts, C.byref(n)))
+        return {hs[k]: {"running": bool(run[k]), "it": its[k], "t": ts[k]}
+                for k in range(n.value)}
+
     def usage(self) -> Dict[str, int]:
         out = (C.c_longlong * 8)()
         self._check(self.lib.dampm_batch_usage(self.h, out))

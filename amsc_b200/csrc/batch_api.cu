@@ -544,6 +544,30 @@ int dampm_batch_ledgers(dampm_batch* b, int handle, double out[9]) {
   return DAMPM_OK;
 }
 
+int dampm_batch_states(dampm_batch* b, int cap, int* handles, int* running, int* its,
+                       double* ts, int* count) {
+  if (!b || !count || cap < 0 || (cap > 0 && (!handles || !running || !its || !ts)))
+    return DAMPM_ERR_ARG;
+  int rc = read_scalars(b);
+  if (rc) return rc;
+  int n = 0;
+  for (size_t s = 0; s < b->scns.size(); ++s) {
+    const HostScn& h = b->scns[s];
+    if (!h.d.live) continue;
+    if (n >= cap) return bfail(b, DAMPM_ERR_ARG, "state arrays shorter than the live count");
+    const Scalars& S = b->Sh[s];
+    const Phys& P = h.d.P;
+    handles[n] = h.handle;
+    running[n] = (S.status == 0) && (P.fixed ? (S.it < P.NSTEPS) : (S.t < P.T));
+    its[n] = S.it;
+    ts[n] = S.t;
+    if (S.status) return bfail(b, DAMPM_ERR_DEVICE, "device status word set");
+    ++n;
+  }
+  *count = n;
+  return DAMPM_OK;
+}
+
 int dampm_batch_usage(dampm_batch* b, long long out[8]) {
   if (!b || !out) return DAMPM_ERR_ARG;
   long long live = 0, dead = 0;

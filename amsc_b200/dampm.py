@@ -99,6 +99,8 @@ def _declare(lib):
         "dampm_batch_download": (C.c_int, [P, C.c_int, C.c_char_p, _DP]),
         "dampm_batch_ledgers": (C.c_int, [P, C.c_int, _DP]),
         "dampm_batch_usage": (C.c_int, [P, C.POINTER(C.c_longlong)]),
+        "dampm_batch_states": (C.c_int, [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]),
         "dampm_batch_last_error": (C.c_char_p, [P]),
     }
     for name, (res, args) in sig.items():

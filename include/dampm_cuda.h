@@ -251,6 +251,12 @@ int dampm_batch_sync(dampm_batch* b);
 int dampm_batch_query(dampm_batch* b, int handle, int* it, double* t,
                       double* dt_last, int* running, long long* np);
 
+/* The loop state of every live scenario in one synchronising call: handle,
+ * whether its loop condition still holds, iteration, time.  cap is the
+ * length of the arrays; *count receives the live count. */
+int dampm_batch_states(dampm_batch* b, int cap, int* handles, int* running,
+                       int* its, double* ts, int* count);
+
 /* One particle field of one scenario, reference index order: x, y, vpx, vpy,
  * hp, F_11, F_12 (= F_21), F_22, Mp, Vp, H, mom_px, mom_py. */
 int dampm_batch_download(dampm_batch* b, int handle, const char* field,
