@@ -229,7 +229,9 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   b->N_cap = node_cap;
   b->S_cap = scenario_cap;
   b->STRIP_cap = kMaxStrips;
-  b->USEG_cap = node_cap / 8 + 64LL * scenario_cap + 1024;
+  // unit-plan slots: a scenario takes ceil((Ney+1)/30) * (Nex+1) of them,
+  // at most nn/30 + (Nex+1)
+  b->USEG_cap = node_cap / 24 + 2048LL * scenario_cap + 1024;
   b->B_cap = int(particle_cap / kG2PThreads) + scenario_cap + 1;
   if (cuda_stream) {
     b->stream = static_cast<cudaStream_t>(cuda_stream);

@@ -9,6 +9,7 @@ between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload ensemble [--scenarios 512] [--steps 1000]
+    python bench.py --workload serving [--requests 300] [--rate 100] [--budget-gb 150]
 
 One JSON line on rank 0.  Multi-GPU runs are independent replicas (one
 scenario, or one ensemble, per GPU, weak scaling): the step has no exchange.
@@ -342,13 +343,105 @@ def run_ensemble(args, world, rank, local):
     return 0
 
 
+def run_serving(args, world, rank, local):
+    """--workload serving: requests arriving as a Poisson stream, served by
+    continuous batching; scenarios/s and time-to-result percentiles."""
+    import torch
+    torch.cuda.set_device(local)
+    from amsc_b200 import scenarios
+    from amsc_b200.dampm import Solver
+    from amsc_b200.serving import Request, Server, latency_summary, poisson_arrivals
+
+    n = args.requests
+    arr = poisson_arrivals(n, args.rate, seed=777 + rank)
+    reqs = [Request(k, scenarios.serving_request(200000 * rank + k, t_end=args.t_end),
+                    float(arr[k])) for k in range(n)]
+    free, _ = torch.cuda.mem_get_info()
+    budget = min(args.budget_gb * 1e9, 0.8 * free)
+    stream = torch.cuda.Stream()
+    srv = Server(budget, max_scenarios=args.max_scenarios, tick=args.tick,
+                 stream=stream.cuda_stream)
+    # warm-up: one short request through the same server
+    warm = scenarios.serving_request(999999, t_end=0.2)
+    srv.run([Request(-1, warm, 0.0)])
+    l0 = srv.b.usage()["launches"]
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    _barrier(world)
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    launches = srv.b.usage()["launches"] - l0
+    occupancy = srv.occupancy[:]
+    srv.close()
+    makespan = _allreduce(max(r.finished for r in reqs), world)
+    total = _allreduce(float(n), world, "sum")
+    value = total / makespan
+    lat = latency_summary(reqs)
+    passes = sum(r.passes for r in reqs)
+    particle_steps = sum(r.passes * r.data.np for r in reqs)
+    # the plain path: a sample of the same requests one at a time, host in to
+    # host out, through dampm_ctx
+    m = min(args.plain_sample, n)
+    tp = time.perf_counter()
+    for r in reqs[:m]:
+        with Solver(r.data, stream=stream.cuda_stream) as s:
+            s.run()
+            for f in ("x", "y", "hp"):
+                s.download(f)
+    plain = m / (time.perf_counter() - tp) if m else None
+    h2d = sum(8 * (10 * r.data.np + r.data.nnodes) for r in reqs)
+    d2h = sum(8 * 3 * r.data.np for r in reqs)
+    if rank == 0:
+        line = {
+            "metric": "serving scenarios/s", "value": value, "unit": "scenarios/s",
+            "n_gpus": world, "steps": int(passes), "warmup": 1,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"serving: {n} requests, Poisson {args.rate}/s, side "
+                                   "logU[64,1024] cells, h=1 m, CFL 0.4 to t=60 s",
+                       "requests": n, "rate_per_s": args.rate, "t_end_s": args.t_end,
+                       "budget_gb": round(budget / 1e9, 1), "tick_passes": args.tick,
+                       "parallelism": f"continuous batching; replicas{world}",
+                       "l2": "state > 126 MB L2 at full occupancy, no flush"},
+            "latency": lat,
+            "makespan_s": makespan, "wall_s": wall,
+            "particle_steps_per_s": particle_steps / makespan,
+            "mean_live_scenarios": float(np.mean(occupancy)) if occupancy else 0.0,
+            "max_live_scenarios": int(max(occupancy)) if occupancy else 0,
+            "compactions": srv.compactions,
+            "plain_path": {"value": plain, "unit": "scenarios/s",
+                           "sample": f"first {m} requests alone through dampm_ctx, upload "
+                                     "to results on the host"},
+            "serving_vs_plain": (value / world) / plain if plain else None,
+            "e2e": {"value": value, "unit": "scenarios/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": "time-to-result runs from arrival to results on the host"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    _barrier(world)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="mudflow", choices=["mudflow", "ensemble"])
+    ap.add_argument("--workload", default="mudflow",
+                    choices=["mudflow", "ensemble", "serving"])
+    ap.add_argument("--requests", type=int, default=300)
+    ap.add_argument("--rate", type=float, default=100.0)
+    ap.add_argument("--t-end", type=float, default=60.0)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--max-scenarios", type=int, default=1024)
+    ap.add_argument("--tick", type=int, default=16)
     ap.add_argument("--scenarios", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -358,6 +451,15 @@ def main():
     if args.steps is None:
         args.steps = 1000 if args.workload == "ensemble" else 400
     world, rank, local = _dist_init()
+    if args.workload == "serving":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no request loop; its per-scenario CPU "
+                                  "time is the mudflow reference arm"}))
+            _barrier(world)
+            return 0
+        return run_serving(args, world, rank, local)
     if args.workload == "ensemble":
         if args.impl == "reference":
             if rank == 0:
