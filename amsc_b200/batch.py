@@ -24,10 +24,17 @@ class Batch:
     """A set of scenarios resident in HBM, stepped together."""
 
     def __init__(self, particle_cap: int, node_cap: int, scenario_cap: int,
-                 stream: Optional[int] = None):
+                 stream: Optional[int] = None, precision: str = "fp64"):
+        """precision "fp64" is the plain path; "fp32" keeps particle and
+        nodal fields in FP32 with compensated nodal sums (terrain, the
+        well-balanced depth terms, ledgers and time stay FP64)."""
         self.lib = load_library()
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision is fp64 or fp32")
+        self.precision = precision
         h = C.c_void_p()
-        rc = self.lib.dampm_batch_create(int(particle_cap), int(node_cap), int(scenario_cap), 0,
+        rc = self.lib.dampm_batch_create(int(particle_cap), int(node_cap), int(scenario_cap),
+                                         1 if precision == "fp32" else 0,
                                          C.c_void_p(stream or 0), C.byref(h))
         if rc != 0:
             raise DampmError(f"dampm_batch_create failed ({rc})")

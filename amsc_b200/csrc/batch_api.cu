@@ -46,10 +46,12 @@ struct dampm_batch {
   std::vector<HostScn> scns;  // packed order = device table order
   int next_handle = 0;
   // device
-  Particles p[2]{};
+  int precision = DAMPM_FP64;
+  ParticlesT<double> p64[2]{};  // FP64: the two halves of the double buffer
+  ParticlesT<float> p32[2]{};   // FP32 form
   double* Z[2] = {nullptr, nullptr};
   int cur = 0;
-  double *vvxL = nullptr, *vvyL = nullptr;
+  void *vvxL = nullptr, *vvyL = nullptr;  // real type of the precision
   int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr;
   int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr, *cbig = nullptr;
   int* ustart = nullptr;
@@ -99,12 +101,24 @@ int balloc(dampm_batch* b, T** ptr, size_t n) {
   return DAMPM_OK;
 }
 
+template <class R>
+ParticlesT<R>* halves(dampm_batch* b);
+template <>
+ParticlesT<double>* halves<double>(dampm_batch* b) { return b->p64; }
+template <>
+ParticlesT<float>* halves<float>(dampm_batch* b) { return b->p32; }
+
+const int* keys_of(dampm_batch* b) {
+  return b->precision == DAMPM_FP32 ? b->p32[b->cur].key : b->p64[b->cur].key;
+}
+
 // the persistent per-particle arrays of one half of the double buffer
-int alloc_particles(dampm_batch* b, Particles& p) {
-  double** f[] = {&p.x,   &p.y,   &p.vpx, &p.vpy, &p.hp,  &p.F11, &p.F12, &p.F22,
-                  &p.Mp,  &p.Vp,  &p.H,   &p.mpx, &p.mpy, &p.qfx, &p.qfy, &p.qxi,
-                  &p.qeta, &p.qgx, &p.qgy, &p.Ap,  &p.Fbx, &p.Fby};
-  for (double** q : f) {
+template <class R>
+int alloc_particles(dampm_batch* b, ParticlesT<R>& p) {
+  R** f[] = {&p.x,   &p.y,   &p.vpx, &p.vpy, &p.hp,  &p.F11, &p.F12, &p.F22,
+             &p.Mp,  &p.Vp,  &p.H,   &p.mpx, &p.mpy, &p.qfx, &p.qfy, &p.qxi,
+             &p.qeta, &p.qgx, &p.qgy, &p.Ap,  &p.Fbx, &p.Fby};
+  for (R** q : f) {
     int rc = balloc(b, q, size_t(b->P_cap));
     if (rc) return rc;
   }
@@ -116,12 +130,13 @@ int alloc_particles(dampm_batch* b, Particles& p) {
   return DAMPM_OK;
 }
 
-Particles shifted(const Particles& p, long long off) {
-  Particles q = p;
-  double** f[] = {&q.x,   &q.y,   &q.vpx, &q.vpy, &q.hp,  &q.F11, &q.F12, &q.F22,
-                  &q.Mp,  &q.Vp,  &q.H,   &q.mpx, &q.mpy, &q.qfx, &q.qfy, &q.qxi,
-                  &q.qeta, &q.qgx, &q.qgy, &q.Ap,  &q.Fbx, &q.Fby};
-  for (double** d : f)
+template <class R>
+ParticlesT<R> shifted(const ParticlesT<R>& p, long long off) {
+  ParticlesT<R> q = p;
+  R** f[] = {&q.x,   &q.y,   &q.vpx, &q.vpy, &q.hp,  &q.F11, &q.F12, &q.F22,
+             &q.Mp,  &q.Vp,  &q.H,   &q.mpx, &q.mpy, &q.qfx, &q.qfy, &q.qxi,
+             &q.qeta, &q.qgx, &q.qgy, &q.Ap,  &q.Fbx, &q.Fby};
+  for (R** d : f)
     if (*d) *d += off;
   int** fi[] = {&q.label, &q.level, &q.key};
   for (int** d : fi)
@@ -182,14 +197,14 @@ int enqueue_pass(dampm_batch* b) {
   const int ntiles = int((b->C_tot + kScanTile - 1) / kScanTile);
   k_b_step_begin<<<1, 1024, 0, st>>>(b->scn, b->S, nscn, b->Sg);
   const int gp = grid_blocks(b->P_tot, 256);
-  k_count<<<gp, 256, 0, st>>>(b->p[b->cur].key, b->count, b->slot, b->Sg);
+  k_count<<<gp, 256, 0, st>>>(keys_of(b), b->count, b->slot, b->Sg);
   k_scan_tiles<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(b->count, int(b->C_tot),
                                                                b->tile_sum, b->Sg);
   k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(b->tile_sum, ntiles, b->Sg);
   k_list_reset<<<1, 1, 0, st>>>(b->clist_n, b->Sg);
   k_scan_apply<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(
       b->count, int(b->C_tot), b->tile_sum, b->start, b->clist, b->clist_n, b->Sg);
-  k_scatter<<<gp, 256, 0, st>>>(b->p[b->cur].key, b->slot, b->start, b->perm, b->Sg);
+  k_scatter<<<gp, 256, 0, st>>>(keys_of(b), b->slot, b->start, b->perm, b->Sg);
   k_segment_order<<<148 * 8, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
                                             b->cbig, b->Sg);
   k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
@@ -200,17 +215,90 @@ int enqueue_pass(dampm_batch* b) {
   k_b_units_flat<<<1, kPlanThreads, sizeof(int) * (b->strips_tot + 1), st>>>(
       b->strip_n, b->strips_tot, b->strip_scn, b->scn, nscn, b->uplan, b->ulist,
       b->ucount, b->scn_units, b->Sg);
-  k_b_p2g<<<b->p2g_grid, kP2GThreads, p2g_smem_bytes(), st>>>(
-      b->p[b->cur], b->perm, b->start, b->vvxL, b->vvyL, b->led_part, b->scn, b->S,
-      b->ulist, b->ucount, b->Sg);
+  if (b->precision == DAMPM_FP32)
+    launch_b_p2g<float>(b->p2g_grid, st, b->p32[b->cur], b->perm, b->start,
+                        static_cast<float*>(b->vvxL), static_cast<float*>(b->vvyL),
+                        b->led_part, b->scn, b->S, b->ulist, b->ucount, b->Sg);
+  else
+    launch_b_p2g<double>(b->p2g_grid, st, b->p64[b->cur], b->perm, b->start,
+                         static_cast<double*>(b->vvxL), static_cast<double*>(b->vvyL),
+                         b->led_part, b->scn, b->S, b->ulist, b->ucount, b->Sg);
   k_b_ledger<<<nscn, 256, 0, st>>>(b->led_part, b->scn_units, b->scn, b->S, nscn,
                                    b->Sg);
-  k_b_g2p<<<b->nblk, kG2PThreads, 0, st>>>(b->p[b->cur], b->vvxL, b->vvyL, b->Z[b->cur],
-                                           b->scn, b->S, b->gblk, b->Sg);
+  if (b->precision == DAMPM_FP32)
+    launch_b_g2p<float>(b->nblk, st, b->p32[b->cur], static_cast<const float*>(b->vvxL),
+                        static_cast<const float*>(b->vvyL), b->Z[b->cur], b->scn, b->S,
+                        b->gblk, b->Sg);
+  else
+    launch_b_g2p<double>(b->nblk, st, b->p64[b->cur], static_cast<const double*>(b->vvxL),
+                         static_cast<const double*>(b->vvyL), b->Z[b->cur], b->scn, b->S,
+                         b->gblk, b->Sg);
   k_b_step_end<<<1, 1024, 0, st>>>(b->scn, b->S, nscn);
   b->launches += 15;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  return DAMPM_OK;
+}
+
+// Particles of one scenario into the current half (converted to R on the
+// host), then the initial state of main/optim_par.cpp:239-264 on the device.
+template <class R>
+int upload_scenario(dampm_batch* b, const Scn& d, int pos, long long np,
+                    const double* const* in, double* Zs) {
+  ParticlesT<R> p = shifted(halves<R>(b)[b->cur], d.p_off);
+  R* dst[10] = {p.x, p.y, p.Mp, p.Ap, p.vpx, p.vpy, p.hp, p.mpx, p.mpy, p.Vp};
+  cudaStream_t st = b->stream;
+  std::vector<R> tmp;
+  for (int k = 0; k < 10; ++k) {
+    const R* src;
+    if (sizeof(R) == sizeof(double)) {
+      src = reinterpret_cast<const R*>(in[k]);
+    } else {
+      tmp.assign(in[k], in[k] + np);
+      src = tmp.data();
+    }
+    BCK(cudaMemcpyAsync(dst[k], src, sizeof(R) * size_t(np), cudaMemcpyHostToDevice, st));
+    if (sizeof(R) != sizeof(double)) BCK(cudaStreamSynchronize(st));  // tmp is reused
+  }
+  // (the terrain gradients only feed recorded outputs, which a batch does
+  // not keep, so Z stands in for them)
+  launch_init_particles<R>(grid_blocks(np, 256), 256, st, p, Zs, Zs, Zs, d.G, d.P,
+                           b->S + pos, int(np), d.c_off);
+  launch_prep<R>(grid_blocks(np, 256), 256, st, p, Zs, d.G, d.P, b->S + pos, 0);
+  b->launches += 2;
+  BCK(cudaGetLastError());
+  return DAMPM_OK;
+}
+
+template <class R>
+int download_field(dampm_batch* b, const Scn& d, const std::string& f, double* out) {
+  const ParticlesT<R> p = shifted(halves<R>(b)[b->cur], d.p_off);
+  const R* src = nullptr;
+  if (f == "x") src = p.x;
+  else if (f == "y") src = p.y;
+  else if (f == "vpx") src = p.vpx;
+  else if (f == "vpy") src = p.vpy;
+  else if (f == "hp") src = p.hp;
+  else if (f == "F_11") src = p.F11;
+  else if (f == "F_12" || f == "F_21") src = p.F12;
+  else if (f == "F_22") src = p.F22;
+  else if (f == "Mp") src = p.Mp;
+  else if (f == "Vp") src = p.Vp;
+  else if (f == "H") src = p.H;
+  else if (f == "mom_px") src = p.mpx;
+  else if (f == "mom_py") src = p.mpy;
+  if (!src) return bfail(b, DAMPM_ERR_UNKNOWN_FIELD, "unknown batch field " + f);
+  if (sizeof(R) == sizeof(double)) {
+    BCK(cudaMemcpyAsync(out, src, sizeof(double) * size_t(d.np), cudaMemcpyDeviceToHost,
+                        b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+  } else {
+    std::vector<R> tmp(size_t(d.np));
+    BCK(cudaMemcpyAsync(tmp.data(), src, sizeof(R) * size_t(d.np), cudaMemcpyDeviceToHost,
+                        b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < d.np; ++i) out[i] = double(tmp[i]);
+  }
   return DAMPM_OK;
 }
 
@@ -223,8 +311,11 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   if (!out || particle_cap < 1 || node_cap < 4 || scenario_cap < 1 ||
       particle_cap > 0x7fffffffLL || node_cap > 0x7fffffffLL)
     return DAMPM_ERR_ARG;
-  if (precision != DAMPM_FP64) return DAMPM_ERR_ARG;
+  if (precision != DAMPM_FP64 && precision != DAMPM_FP32) return DAMPM_ERR_ARG;
   dampm_batch* b = new dampm_batch();
+  b->precision = precision;
+  const bool f32 = precision == DAMPM_FP32;
+  const size_t rsz = f32 ? sizeof(float) : sizeof(double);
   b->P_cap = particle_cap;
   b->N_cap = node_cap;
   b->S_cap = scenario_cap;
@@ -242,13 +333,13 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
     }
     b->own_stream = true;
   }
-  int rc = alloc_particles(b, b->p[0]);
-  rc = rc ? rc : alloc_particles(b, b->p[1]);
+  int rc = f32 ? alloc_particles(b, b->p32[0]) : alloc_particles(b, b->p64[0]);
+  if (!rc) rc = f32 ? alloc_particles(b, b->p32[1]) : alloc_particles(b, b->p64[1]);
   const size_t nn = size_t(node_cap), pc = size_t(particle_cap);
   rc = rc ? rc : balloc(b, &b->Z[0], nn);
   rc = rc ? rc : balloc(b, &b->Z[1], nn);
-  rc = rc ? rc : balloc(b, &b->vvxL, nn);
-  rc = rc ? rc : balloc(b, &b->vvyL, nn);
+  rc = rc ? rc : balloc(b, reinterpret_cast<unsigned char**>(&b->vvxL), nn * rsz);
+  rc = rc ? rc : balloc(b, reinterpret_cast<unsigned char**>(&b->vvyL), nn * rsz);
   // cells of all scenarios: fewer than their nodes
   rc = rc ? rc : balloc(b, &b->count, nn + 4);
   rc = rc ? rc : balloc(b, &b->start, nn + 1);
@@ -279,20 +370,15 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
     rc = bfail(b, DAMPM_ERR_CUDA, "cudaMallocHost failed");
   if (rc == DAMPM_OK) {
     cudaMemsetAsync(b->count, 0, sizeof(int) * (nn + 4), b->stream);
-    cudaMemsetAsync(b->vvxL, 0, sizeof(double) * nn, b->stream);
-    cudaMemsetAsync(b->vvyL, 0, sizeof(double) * nn, b->stream);
+    cudaMemsetAsync(b->vvxL, 0, rsz * nn, b->stream);
+    cudaMemsetAsync(b->vvyL, 0, rsz * nn, b->stream);
     cudaMemsetAsync(b->S, 0, sizeof(Scalars) * size_t(scenario_cap), b->stream);
     cudaMemsetAsync(b->Sg, 0, sizeof(Scalars), b->stream);
-    const size_t smem = p2g_smem_bytes();
-    if (cudaFuncSetAttribute(k_b_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem)) != cudaSuccess)
-      rc = bfail(b, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
-    cudaFuncSetAttribute(k_b_p2g, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         int(cudaSharedmemCarveoutMaxShared));
-    int per_sm = 0, nsm = 0, dev = 0;
+    const int per_sm = f32 ? setup_b_p2g<float>() : setup_b_p2g<double>();
+    if (per_sm == 0) rc = bfail(b, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+    int nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_p2g, kP2GThreads, smem);
     b->p2g_grid = std::max(1, nsm * std::max(per_sm, 1));
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) rc = DAMPM_ERR_CUDA;
   }
@@ -355,19 +441,7 @@ int dampm_batch_add(dampm_batch* b, const dampm_grid* grid, const dampm_params* 
   h.handle = b->next_handle++;
   const int pos = int(b->scns.size());
   // particles and terrain into the current half
-  Particles p = shifted(b->p[b->cur], d.p_off);
-  const size_t by = sizeof(double) * size_t(np);
   cudaStream_t st = b->stream;
-  BCK(cudaMemcpyAsync(p.x, x, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.y, y, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.Mp, Mp, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.Ap, Ap, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.vpx, vpx, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.vpy, vpy, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.hp, hp, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.mpx, mom_px, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.mpy, mom_py, by, cudaMemcpyHostToDevice, st));
-  BCK(cudaMemcpyAsync(p.Vp, Vp, by, cudaMemcpyHostToDevice, st));
   double* Zs = b->Z[b->cur] + d.n_off;
   BCK(cudaMemcpyAsync(Zs, Z, sizeof(double) * size_t(h.nn), cudaMemcpyHostToDevice, st));
   Scalars s0{};
@@ -376,12 +450,10 @@ int dampm_batch_add(dampm_batch* b, const dampm_grid* grid, const dampm_params* 
   b->Sh[pos] = s0;
   BCK(cudaMemcpyAsync(b->S + pos, b->Sh + pos, sizeof(Scalars), cudaMemcpyHostToDevice,
                       st));
-  // the initial state of main/optim_par.cpp:239-264 (the terrain gradients
-  // only feed recorded outputs, which a batch does not keep, so Z stands in)
-  k_init_particles<<<grid_blocks(np, 256), 256, 0, st>>>(p, Zs, Zs, Zs, d.G, d.P,
-                                                         b->S + pos, int(np), d.c_off);
-  k_prep<<<grid_blocks(np, 256), 256, 0, st>>>(p, Zs, d.G, d.P, b->S + pos, 0);
-  b->launches += 2;
+  const double* in[10] = {x, y, Mp, Ap, vpx, vpy, hp, mom_px, mom_py, Vp};
+  int urc = b->precision == DAMPM_FP32 ? upload_scenario<float>(b, d, pos, np, in, Zs)
+                                       : upload_scenario<double>(b, d, pos, np, in, Zs);
+  if (urc) return urc;
   BCK(cudaGetLastError());
   b->scns.push_back(h);
   b->P_tot += np;
@@ -447,8 +519,11 @@ int dampm_batch_compact(dampm_batch* b) {
   if (!mv.empty()) {
     BCK(cudaMemcpyAsync(b->mblk, mv.data(), sizeof(int4) * mv.size(),
                         cudaMemcpyHostToDevice, b->stream));
-    k_b_move<<<int(mv.size()), kG2PThreads, 0, b->stream>>>(b->p[nxt], b->p[b->cur],
-                                                            b->mblk);
+    if (b->precision == DAMPM_FP32)
+      launch_b_move<float>(int(mv.size()), b->stream, b->p32[nxt], b->p32[b->cur], b->mblk);
+    else
+      launch_b_move<double>(int(mv.size()), b->stream, b->p64[nxt], b->p64[b->cur],
+                            b->mblk);
   }
   if (!nm.empty()) {
     BCK(cudaMemcpyAsync(b->nmove, nm.data(), sizeof(int4) * nm.size(),
@@ -513,27 +588,9 @@ int dampm_batch_download(dampm_batch* b, int handle, const char* field, double* 
   if (!b || !field || !out) return DAMPM_ERR_ARG;
   const int s = find(b, handle);
   if (s < 0) return bfail(b, DAMPM_ERR_ARG, "unknown scenario handle");
-  const Particles p = shifted(b->p[b->cur], b->scns[s].d.p_off);
   const std::string f(field);
-  const double* src = nullptr;
-  if (f == "x") src = p.x;
-  else if (f == "y") src = p.y;
-  else if (f == "vpx") src = p.vpx;
-  else if (f == "vpy") src = p.vpy;
-  else if (f == "hp") src = p.hp;
-  else if (f == "F_11") src = p.F11;
-  else if (f == "F_12" || f == "F_21") src = p.F12;
-  else if (f == "F_22") src = p.F22;
-  else if (f == "Mp") src = p.Mp;
-  else if (f == "Vp") src = p.Vp;
-  else if (f == "H") src = p.H;
-  else if (f == "mom_px") src = p.mpx;
-  else if (f == "mom_py") src = p.mpy;
-  if (!src) return bfail(b, DAMPM_ERR_UNKNOWN_FIELD, "unknown batch field " + f);
-  BCK(cudaMemcpyAsync(out, src, sizeof(double) * size_t(b->scns[s].d.np),
-                      cudaMemcpyDeviceToHost, b->stream));
-  BCK(cudaStreamSynchronize(b->stream));
-  return DAMPM_OK;
+  return b->precision == DAMPM_FP32 ? download_field<float>(b, b->scns[s].d, f, out)
+                                    : download_field<double>(b, b->scns[s].d, f, out);
 }
 
 int dampm_batch_ledgers(dampm_batch* b, int handle, double out[9]) {

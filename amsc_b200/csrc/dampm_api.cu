@@ -448,10 +448,10 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));  // Sh is reused below
   if (np > 0) {
-    k_init_particles<<<grid_for(np, 256), 256, 0, ctx->stream>>>(
-        p, ctx->Z, ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np), 0);
-    k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->Z, ctx->G, ctx->P,
-                                                       ctx->S, 0);
+    launch_init_particles<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z,
+                                  ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np), 0);
+    launch_prep<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z, ctx->G, ctx->P,
+                        ctx->S, 0);
     CK(cudaGetLastError());
   }
   ctx->it_host = 0;
@@ -695,8 +695,8 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
                      ctx->stream));
   k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.x, p.y, p.key, ctx->G, ctx->S);
   k_reduce_state<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->S);
-  k_prep<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->Z, ctx->G, ctx->P,
-                                                     ctx->S, fresh ? 0 : 1);
+  launch_prep<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z, ctx->G, ctx->P,
+                      ctx->S, fresh ? 0 : 1);
   CK(cudaGetLastError());
   return DAMPM_OK;
 }

@@ -82,6 +82,11 @@ __device__ __forceinline__ int cell_col(double x, double hx, int ncols) {
   return int(f);
 }
 
+// The functions below are templates on the real type R of the particle
+// arithmetic: R = double is the FP64 path (the expressions are the
+// reference's, operand for operand); R = float is the FP32 form, whose
+// well-balanced depth terms are still evaluated in FP64.
+
 // Local coordinates in cell (r, c): (x - c*hx)/hx, (y - r*hy)/hy
 // (pnode, main/gpu_kernels.cpp:21-31).
 __device__ __forceinline__ void local_xy(double x, double y, int c, int r,
@@ -93,98 +98,101 @@ __device__ __forceinline__ void local_xy(double x, double y, int c, int r,
 
 // Same values as local_xy; when h is a power of two the quotient by h equals
 // the product with 1/h exactly, and the division is skipped.
-__device__ __forceinline__ void local_xy_g(double x, double y, int c, int r,
-                                           const Geom& G, double ihx,
-                                           double ihy, double& xi,
-                                           double& eta) {
-  const double dx = x - c * G.hx, dy = y - r * G.hy;
-  xi = G.hx_pow2 ? dx * ihx : dx / G.hx;
-  eta = G.hy_pow2 ? dy * ihy : dy / G.hy;
+template <class R>
+__device__ __forceinline__ void local_xy_g(R x, R y, int c, int r, const Geom& G,
+                                           R ihx, R ihy, R& xi, R& eta) {
+  const R dx = x - c * R(G.hx), dy = y - r * R(G.hy);
+  xi = G.hx_pow2 ? dx * ihx : dx / R(G.hx);
+  eta = G.hy_pow2 ? dy * ihy : dy / R(G.hy);
 }
 
 // shp (main/gpu_kernels.cpp:33-41)
-__device__ __forceinline__ double shp(double xi, double eta, int inode) {
+template <class R>
+__device__ __forceinline__ R shp(R xi, R eta, int inode) {
   switch (inode) {
     case 3: return xi * eta;
-    case 2: return xi * (1.0 - eta);
-    case 1: return (1.0 - xi) * eta;
-    default: return (1.0 - xi) * (1.0 - eta);
+    case 2: return xi * (R(1) - eta);
+    case 1: return (R(1) - xi) * eta;
+    default: return (R(1) - xi) * (R(1) - eta);
   }
 }
 
 // shg (main/gpu_kernels.cpp:43-59); ihx = 1.0/hx, mihx = -1.0/hx, etc.
-__device__ __forceinline__ double shg_x(double eta, int inode, double ihx,
-                                        double mihx) {
+template <class R>
+__device__ __forceinline__ R shg_x(R eta, int inode, R ihx, R mihx) {
   switch (inode) {
     case 3: return ihx * eta;
-    case 2: return ihx * (1.0 - eta);
+    case 2: return ihx * (R(1) - eta);
     case 1: return mihx * eta;
-    default: return mihx * (1.0 - eta);
+    default: return mihx * (R(1) - eta);
   }
 }
-__device__ __forceinline__ double shg_y(double xi, int inode, double ihy,
-                                        double mihy) {
+template <class R>
+__device__ __forceinline__ R shg_y(R xi, int inode, R ihy, R mihy) {
   switch (inode) {
     case 3: return xi * ihy;
     case 2: return xi * mihy;
-    case 1: return (1.0 - xi) * ihy;
-    default: return (1.0 - xi) * mihy;
+    case 1: return (R(1) - xi) * ihy;
+    default: return (R(1) - xi) * mihy;
   }
 }
 
 // Voellmy basal friction (main/optim_par.cpp:613-626).
-__device__ __forceinline__ void voellmy(const Phys& P, double vx, double vy,
-                                        double h, double& fbx, double& fby) {
-  const double nv = sqrt(vx * vx + vy * vy);
-  if (P.FON > 0 && nv > 1e-10 && P.xi > 0) {
-    const double v2 = vx * vx + vy * vy;
-    const double s = P.rho * P.g * h * P.tan_fa + P.rho * P.g * v2 / P.xi;
-    fbx = -P.FON * s * vx / nv;
-    fby = -P.FON * s * vy / nv;
+template <class R>
+__device__ __forceinline__ void voellmy(const Phys& P, R vx, R vy, R h, R& fbx,
+                                        R& fby) {
+  const R nv = sqrt(vx * vx + vy * vy);
+  if (P.FON > 0 && nv > R(1e-10) && P.xi > 0) {
+    const R rho = R(P.rho), g = R(P.g);
+    const R v2 = vx * vx + vy * vy;
+    const R s = rho * g * h * R(P.tan_fa) + rho * g * v2 / R(P.xi);
+    fbx = -R(P.FON) * s * vx / nv;
+    fby = -R(P.FON) * s * vy / nv;
   } else {
-    fbx = 0.0;
-    fby = 0.0;
+    fbx = R(0);
+    fby = R(0);
   }
 }
 
 // Bingham stress + well-balanced pressure: the stress_tensor_t functor of
-// main/optim_par.cpp:68-120.  F_21 == F_12.
-__device__ __forceinline__ void bingham_stress(const Phys& P, double vpx,
-                                               double vpy, double hp, double H,
-                                               double vpx_dx, double vpy_dy,
-                                               double vpx_dy, double vpy_dx,
-                                               double& F11, double& F12,
-                                               double& F22) {
-  const double A = 3. / 2., C = 65. / 32.;
-  const double nrm = sqrt(vpx * vpx + vpy * vpy);
-  const double mu = P.mu, tau_Y = P.tauy;
-  const double ALF = hp > 1.e-3 ? (6. * mu * nrm) / ((hp + 0.001) * tau_Y) : 0.0;
-  const double B = -114. / 32. - ALF;
-  const double Z1 = (-B + sqrt(B * B - 4. * A * C)) / (2. * A);
-  const double Z2 = (-B - sqrt(B * B - 4. * A * C)) / (2. * A);
-  const double ZZ = fabs(Z1 - .5) <= .5 ? Z1 : Z2;
-  const double D_xx = vpx_dx;
-  const double D_xy = 0.5 * (vpx_dy + vpy_dx);
-  const double D_yy = vpy_dy;
-  const double D_zx =
-      hp > 1.e-3 ? 0.5 * (3. / (2. + ZZ)) * (vpx / (hp + 0.001)) : 0.0;
-  const double D_zy =
-      hp > 1.e-3 ? 0.5 * (3. / (2. + ZZ)) * (vpy / (hp + 0.001)) : 0.0;
-  const double D_zz = -(vpx_dx + vpy_dy);
-  const double invII = 0.5 * (D_xx * D_xx + D_yy * D_yy + D_zz * D_zz) +
-                       D_zx * D_zx + D_zy * D_zy + D_xy * D_xy;
-  double sig_xx = 0.0, sig_xy = 0.0, sig_yy = 0.0;
-  if (invII != 0) {
-    const double k = tau_Y / sqrt(invII) + 2. * mu;
+// main/optim_par.cpp:68-120.  F_21 == F_12.  The pressure term
+// 0.5*rho*g*(hp - H^2/hp), which nearly cancels over a lake at rest, is
+// evaluated in FP64 whatever R is.
+template <class R>
+__device__ __forceinline__ void bingham_stress(const Phys& P, R vpx, R vpy, R hp,
+                                               R H, R vpx_dx, R vpy_dy, R vpx_dy,
+                                               R vpy_dx, R& F11, R& F12, R& F22) {
+  const R A = R(3.) / R(2.), C = R(65.) / R(32.);
+  const R nrm = sqrt(vpx * vpx + vpy * vpy);
+  const R mu = R(P.mu), tau_Y = R(P.tauy);
+  const R ALF = hp > R(1.e-3) ? (R(6.) * mu * nrm) / ((hp + R(0.001)) * tau_Y) : R(0);
+  const R B = -R(114.) / R(32.) - ALF;
+  const R Z1 = (-B + sqrt(B * B - R(4.) * A * C)) / (R(2.) * A);
+  const R Z2 = (-B - sqrt(B * B - R(4.) * A * C)) / (R(2.) * A);
+  const R ZZ = fabs(Z1 - R(.5)) <= R(.5) ? Z1 : Z2;
+  const R D_xx = vpx_dx;
+  const R D_xy = R(0.5) * (vpx_dy + vpy_dx);
+  const R D_yy = vpy_dy;
+  const R D_zx =
+      hp > R(1.e-3) ? R(0.5) * (R(3.) / (R(2.) + ZZ)) * (vpx / (hp + R(0.001))) : R(0);
+  const R D_zy =
+      hp > R(1.e-3) ? R(0.5) * (R(3.) / (R(2.) + ZZ)) * (vpy / (hp + R(0.001))) : R(0);
+  const R D_zz = -(vpx_dx + vpy_dy);
+  const R invII = R(0.5) * (D_xx * D_xx + D_yy * D_yy + D_zz * D_zz) +
+                  D_zx * D_zx + D_zy * D_zy + D_xy * D_xy;
+  R sig_xx = R(0), sig_xy = R(0), sig_yy = R(0);
+  if (invII != R(0)) {
+    const R k = tau_Y / sqrt(invII) + R(2.) * mu;
     sig_xx = k * D_xx;
     sig_xy = k * D_xy;
     sig_yy = k * D_yy;
   }
-  const double h_corr = hp > 1e-10 ? hp - (H * H) / hp : 0.0;
+  const double hpd = hp, Hd = H;
+  const double h_corr = hpd > 1e-10 ? hpd - (Hd * Hd) / hpd : 0.0;
   const double pres = .5 * P.rho * P.g * h_corr;
-  F11 = P.BING * sig_xx - pres;
-  F12 = P.BING * sig_xy;
-  F22 = P.BING * sig_yy - pres;
+  F11 = R(P.BING * double(sig_xx) - pres);
+  F12 = R(P.BING * double(sig_xy));
+  F22 = R(P.BING * double(sig_yy) - pres);
 }
 
 }  // namespace dampm

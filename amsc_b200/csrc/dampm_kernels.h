@@ -30,10 +30,12 @@ constexpr int kG2PThreads = 256;
 constexpr int kScanTile = 4096;
 constexpr int kScanThreads = 1024;
 
-// Particle SoA in reference index order (FP64 path).
-struct Particles {
+// Particle SoA in reference index order; R = double is the FP64 path,
+// R = float the FP32 form (batches).
+template <class R>
+struct ParticlesT {
   // persistent state
-  double *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
+  R *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
   int *label, *level, *key;
   // the record the next P2G transfers, written by G2P (or by k_prep after an
   // upload, a state upload or a merge/split):
@@ -43,35 +45,42 @@ struct Particles {
   //   qxi, qeta local coordinates in the cell of the next binning;
   //   qgx, qgy  gravity force -g*Vp*rho*grad(Z)*(1 - H/hp) there
   //             (main/optim_par.cpp:387,447-454).
-  double *mpx, *mpy, *qfx, *qfy, *qxi, *qeta, *qgx, *qgy;
+  R *mpx, *mpy, *qfx, *qfy, *qxi, *qeta, *qgx, *qgy;
   // Ap and Fb as stored at upload / merge/split (valid while Scalars::fresh
   // is set; otherwise they are derived from the state)
-  double *Ap, *Fbx, *Fby;
+  R *Ap, *Fbx, *Fby;
   // velocity gradients (merge/split input, outputs)
-  double *vpx_dx, *vpx_dy, *vpy_dx, *vpy_dy;
+  R *vpx_dx, *vpx_dy, *vpy_dx, *vpy_dy;
   // output-only fields (allocated when outputs are recorded)
-  double *apx, *apy, *Zp, *hpZ, *dZxp, *dZyp, *Fpx, *Fpy, *Frx, *Fry;
-  double *xp, *yp;
+  R *apx, *apy, *Zp, *hpZ, *dZxp, *dZyp, *Fpx, *Fpy, *Frx, *Fry;
+  R *xp, *yp;
 };
+using Particles = ParticlesT<double>;
 
 // Nodal fields, quadgrid node order.
-struct Nodes {
-  double *vvxL, *vvyL;
+template <class R>
+struct NodesT {
+  R *vvxL, *vvyL;
   // recorded only on output steps
-  double *Mv, *mvx, *mvy, *avx, *avy, *vvx, *vvy, *FPxv, *FPyv, *Fricx,
+  R *Mv, *mvx, *mvy, *avx, *avy, *vvx, *vvy, *FPxv, *FPyv, *Fricx,
       *Fricy, *Fintx, *Finty, *HV;
 };
+using Nodes = NodesT<double>;
 
 __global__ void k_step_begin(Scalars* S, Geom G, Phys P);
 __global__ void k_step_end(Scalars* S);
-__global__ void k_init_particles(Particles p, const double* Z,
-                                 const double* dZdx, const double* dZdy,
-                                 Geom G, Phys P, Scalars* S, int np, int key_off);
+// Host launchers of the kernels that exist in both precisions (the kernel
+// templates are instantiated in step_kernels.cu, next to their definitions).
+template <class R>
+void launch_init_particles(int grid, int block, cudaStream_t st, ParticlesT<R> p,
+                           const double* Z, const double* dZdx, const double* dZdy,
+                           Geom G, Phys P, Scalars* S, int np, int key_off);
 __global__ void k_keys(const double* x, const double* y, int* key, Geom G,
                        const Scalars* S);
 __global__ void k_reduce_state(Particles p, Scalars* S);
-__global__ void k_prep(Particles p, const double* Z, Geom G, Phys P,
-                       const Scalars* S, int derive);
+template <class R>
+void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const double* Z,
+                 Geom G, Phys P, const Scalars* S, int derive);
 __global__ void k_count(const int* key, int* count, int* slot,
                         const Scalars* S);
 __global__ void k_scan_tiles(const int* count, int n, int* tile_sum,
@@ -127,22 +136,33 @@ __global__ void k_b_units_flat(const int* strip_n, int strips, const int* strip_
                                const Scn* scn, int nscn, const int2* plan,
                                int4* ulist, int* ucount, int2* scn_units,
                                const Scalars* Sg);
-__global__ void k_b_p2g(Particles p, const int* perm, const int* cstart,
-                        double* vvxL, double* vvyL, double* led_part,
-                        const Scn* scn, Scalars* S, const int4* ulist,
-                        const int* ucount, const Scalars* Sg);
+template <class R>
+void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
+                  const int* cstart, R* vvxL, R* vvyL, double* led_part, const Scn* scn,
+                  Scalars* S, const int4* ulist, const int* ucount, const Scalars* Sg);
+// sets the batched P2G kernel's shared-memory attributes; returns the
+// resident CTAs per SM (0 on failure)
+template <class R>
+int setup_b_p2g();
 __global__ void k_b_ledger(const double* led_part, const int2* scn_units,
                            const Scn* scn, Scalars* S, int nscn,
                            const Scalars* Sg);
-__global__ void k_b_g2p(Particles p, const double* vvxL, const double* vvyL,
-                        const double* Z, const Scn* scn, Scalars* S,
-                        const int2* gblk, const Scalars* Sg);
-__global__ void k_b_move(Particles dst, Particles src, const int4* mblk);
+template <class R>
+void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const R* vvxL,
+                  const R* vvyL, const double* Z, const Scn* scn, Scalars* S,
+                  const int2* gblk, const Scalars* Sg);
+template <class R>
+void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> src,
+                   const int4* mblk);
+// float <-> double copies of one particle field (FP32 batch upload/download)
+__global__ void k_to_f32(const double* a, float* b, long long n);
+__global__ void k_to_f64(const float* a, double* b, long long n);
 __global__ void k_b_move_nodes(double* dst, const double* src, const int4* nblk);
 
 __global__ void k_hv(const Particles p, const int* perm, const int* cstart,
                      double* HV, Geom G, const Scalars* S);
 
-size_t p2g_smem_bytes();
+size_t p2g_smem_bytes();       // FP64 P2G staging
+size_t p2g_smem_bytes_f32();   // FP32 P2G staging
 
 }  // namespace dampm

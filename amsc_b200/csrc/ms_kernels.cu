@@ -453,7 +453,7 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
   k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
-  k_prep<<<gp, 256, 0, st>>>(p, Z, G, P, S, 0);
+  launch_prep<double>(gp, 256, st, p, Z, G, P, S, 0);
   n += 4;
   return n;
 }

@@ -73,7 +73,8 @@ __global__ void k_step_end(Scalars* S) {
 // ---------------------------------------------------------------------------
 // initialisation after upload: main/optim_par.cpp:239-264
 // ---------------------------------------------------------------------------
-__global__ void k_init_particles(Particles p, const double* __restrict__ Z,
+template <class R>
+__global__ void k_init_particles(ParticlesT<R> p, const double* __restrict__ Z,
                                  const double* __restrict__ dZdx,
                                  const double* __restrict__ dZdy, Geom G,
                                  Phys P, Scalars* S, int np, int key_off) {
@@ -173,39 +174,47 @@ __global__ void k_reduce_state(Particles p, Scalars* S) {
 // Ap/Fb/mom (derive == 0: after an upload or a merge/split) or from the state
 // alone (derive != 0), exactly as the reference computes these values
 // (main/optim_par.cpp:387,447-459,600-626).
+// The terrain gradient and the well-balanced factor 1 - H/hp are evaluated
+// in FP64 whatever R is (the bed slope and the near-cancelling free-surface
+// difference).
+template <class R>
 __device__ __forceinline__ void next_record(const Geom& G, const Phys& P,
-                                            const double* __restrict__ Z,
-                                            double x, double y, double hp,
-                                            double H, double Vp, double& xi,
-                                            double& eta, double& gx, double& gy) {
-  const int r = cell_row(y, G.hy, G.nrows), c = cell_col(x, G.hx, G.ncols);
-  const double ihx = 1.0 / G.hx, mihx = -1.0 / G.hx;
-  const double ihy = 1.0 / G.hy, mihy = -1.0 / G.hy;
+                                            const double* __restrict__ Z, R x,
+                                            R y, R hp, R H, R Vp, R& xi, R& eta,
+                                            R& gx, R& gy) {
+  const int r = cell_row(double(y), G.hy, G.nrows);
+  const int c = cell_col(double(x), G.hx, G.ncols);
+  const R ihx = R(1) / R(G.hx), ihy = R(1) / R(G.hy);
   local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
   // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
+  const double dihx = 1.0 / G.hx, dmihx = -1.0 / G.hx;
+  const double dihy = 1.0 / G.hy, dmihy = -1.0 / G.hy;
+  const double dxi = xi, deta = eta;
   double dzx = 0.0, dzy = 0.0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const double zn = Z[node_of(k, c, r, G.nrows)];
-    dzx += shg_x(eta, k, ihx, mihx) * zn;
-    dzy += shg_y(xi, k, ihy, mihy) * zn;
+    dzx += shg_x(deta, k, dihx, dmihx) * zn;
+    dzy += shg_y(dxi, k, dihy, dmihy) * zn;
   }
   // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
-  const double wb = hp > 1e-10 ? 1.0 - (H / hp) : 1.0;
-  gx = -P.g * Vp * P.rho * dzx * wb;
-  gy = -P.g * Vp * P.rho * dzy * wb;
+  const double hpd = hp, Hd = H, Vpd = Vp;
+  const double wb = hpd > 1e-10 ? 1.0 - (Hd / hpd) : 1.0;
+  gx = R(-P.g * Vpd * P.rho * dzx * wb);
+  gy = R(-P.g * Vpd * P.rho * dzy * wb);
 }
 
-__global__ void k_prep(Particles p, const double* __restrict__ Z, Geom G,
+template <class R>
+__global__ void k_prep(ParticlesT<R> p, const double* __restrict__ Z, Geom G,
                        Phys P, const Scalars* S, int derive) {
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
-    const double hp = p.hp[i];
-    double Ap, fbx, fby;
+    const R hp = p.hp[i];
+    R Ap, fbx, fby;
     if (derive) {
-      Ap = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
-      voellmy(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
+      Ap = hp > R(1.e-2) ? p.Vp[i] / hp : R(0);
+      voellmy<R>(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
       p.mpx[i] = p.vpx[i] * p.Mp[i];
       p.mpy[i] = p.vpy[i] * p.Mp[i];
     } else {
@@ -215,8 +224,8 @@ __global__ void k_prep(Particles p, const double* __restrict__ Z, Geom G,
     }
     p.qfx[i] = Ap * fbx;
     p.qfy[i] = Ap * fby;
-    double xi, eta, gx, gy;
-    next_record(G, P, Z, p.x[i], p.y[i], hp, p.H[i], p.Vp[i], xi, eta, gx, gy);
+    R xi, eta, gx, gy;
+    next_record<R>(G, P, Z, p.x[i], p.y[i], hp, p.H[i], p.Vp[i], xi, eta, gx, gy);
     p.qxi[i] = xi;
     p.qeta[i] = eta;
     p.qgx[i] = gx;
@@ -539,18 +548,29 @@ namespace {
 constexpr int kRec = 13;  // xi eta Mp mpx mpy FPx FPy Frx Fry F11 F12 F22 Vp
 constexpr int kPf = (kCap + kP2GThreads - 1) / kP2GThreads;
 
-struct P2GSmem {
-  double rec[kRec][kCap];
-  double xch[9][kTR];  // finished sums per quantity
+template <class R>
+struct P2GSmemT {
+  R rec[kRec][kCap];
+  R xch[9][kTR];  // finished sums per quantity
   double led[6][kP2GThreads / 32];
   int rowstart[3][kTR + 2];
 };
+using P2GSmem = P2GSmemT<double>;
 
-__device__ __forceinline__ int swz(int j) { return j ^ ((j >> 4) & 15); }
+// Record slot of batch position j: an XOR of the bank-selecting low bits by
+// the next ones (16 eight-byte or 32 four-byte slots span the 32 banks).
+template <class R>
+__device__ __forceinline__ int swz(int j) {
+  return sizeof(R) == 8 ? (j ^ ((j >> 4) & 15)) : (j ^ ((j >> 5) & 31));
+}
 
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+template <int kBytes>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  if (kBytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -565,7 +585,8 @@ struct Batch {
 };
 
 // the batch after b: the rest of its column, else the start of the next one
-__device__ __forceinline__ Batch next_batch(const Batch& b, const P2GSmem& s,
+template <class R>
+__device__ __forceinline__ Batch next_batch(const Batch& b, const P2GSmemT<R>& s,
                                             int nrs, int ccLast) {
   Batch n{0, 0, 0, false};
   if (!b.valid) return n;
@@ -587,63 +608,66 @@ __device__ __forceinline__ void load_perm(int (&pf)[kPf],
   }
 }
 
-__device__ __forceinline__ void issue_gather(P2GSmem& s, const Particles& p,
+template <class R>
+__device__ __forceinline__ void issue_gather(P2GSmemT<R>& s, const ParticlesT<R>& p,
                                              const int (&pf)[kPf],
                                              const Batch& b) {
+  constexpr int kB = sizeof(R);
 #pragma unroll
   for (int u = 0; u < kPf; ++u) {
     const int j = b.bb + threadIdx.x + u * kP2GThreads;
     if (j >= b.be) break;
     const int i = pf[u];
-    const int l = swz(j - b.bb);
-    cp_async8(&s.rec[0][l], p.qxi + i);
-    cp_async8(&s.rec[1][l], p.qeta + i);
-    cp_async8(&s.rec[2][l], p.Mp + i);
-    cp_async8(&s.rec[3][l], p.mpx + i);
-    cp_async8(&s.rec[4][l], p.mpy + i);
-    cp_async8(&s.rec[5][l], p.qgx + i);
-    cp_async8(&s.rec[6][l], p.qgy + i);
-    cp_async8(&s.rec[7][l], p.qfx + i);
-    cp_async8(&s.rec[8][l], p.qfy + i);
-    cp_async8(&s.rec[9][l], p.F11 + i);
-    cp_async8(&s.rec[10][l], p.F12 + i);
-    cp_async8(&s.rec[11][l], p.F22 + i);
-    cp_async8(&s.rec[12][l], p.Vp + i);
+    const int l = swz<R>(j - b.bb);
+    cp_async<kB>(&s.rec[0][l], p.qxi + i);
+    cp_async<kB>(&s.rec[1][l], p.qeta + i);
+    cp_async<kB>(&s.rec[2][l], p.Mp + i);
+    cp_async<kB>(&s.rec[3][l], p.mpx + i);
+    cp_async<kB>(&s.rec[4][l], p.mpy + i);
+    cp_async<kB>(&s.rec[5][l], p.qgx + i);
+    cp_async<kB>(&s.rec[6][l], p.qgy + i);
+    cp_async<kB>(&s.rec[7][l], p.qfx + i);
+    cp_async<kB>(&s.rec[8][l], p.qfy + i);
+    cp_async<kB>(&s.rec[9][l], p.F11 + i);
+    cp_async<kB>(&s.rec[10][l], p.F12 + i);
+    cp_async<kB>(&s.rec[11][l], p.F22 + i);
+    cp_async<kB>(&s.rec[12][l], p.Vp + i);
   }
   cp_async_commit();
 }
 
 // Nodal momentum, velocity and wall conditions of node (r, nc) from its nine
 // P2G sums (main/optim_par.cpp:467-529); also accumulates the node ledger.
+template <class R>
 __device__ __forceinline__ void nodal_update(
-    double Mv, double momx, double momy, double FPx, double FPy, double Frx,
-    double Fry, double Fix, double Fiy, int r, int nc, const Geom& G,
-    const Phys& P, double dt, const Nodes& nodes, int record, double& ln0,
-    double& ln1, double& ln2) {
+    R Mv, R momx, R momy, R FPx, R FPy, R Frx, R Fry, R Fix, R Fiy, int r, int nc,
+    const Geom& G, const Phys& P, double dtd, const NodesT<R>& nodes, int record,
+    double& ln0, double& ln1, double& ln2) {
   const int nrows = G.nrows, ncols = G.ncols;
   const int n = r + nc * (nrows + 1);
-  const double Fextx = FPx + Frx;
-  const double Fexty = FPy + Fry;
-  const double Ftx = Fextx - Fix;
-  const double Fty = Fexty - Fiy;
+  const R dt = R(dtd);
+  const R Fextx = FPx + Frx;
+  const R Fexty = FPy + Fry;
+  const R Ftx = Fextx - Fix;
+  const R Fty = Fexty - Fiy;
   ln0 += Mv;
   ln1 += momx;
   ln2 += momy;
   momx = dt * Ftx + momx;
   momy = dt * Fty + momy;
-  const bool act = Mv > 1.e-2;
-  double avx = act ? Ftx / Mv : 0.0;
-  double avy = act ? Fty / Mv : 0.0;
-  double vvx = act ? momx / Mv : 0.0;
-  double vvy = act ? momy / Mv : 0.0;
-  double vvxL = dt * avx + vvx;
-  double vvyL = dt * avy + vvy;
+  const bool act = Mv > R(1.e-2);
+  R avx = act ? Ftx / Mv : R(0);
+  R avy = act ? Fty / Mv : R(0);
+  R vvx = act ? momx / Mv : R(0);
+  R vvy = act ? momy / Mv : R(0);
+  R vvxL = dt * avx + vvx;
+  R vvyL = dt * avy + vvy;
   if (P.BC) {  // cells on the walls zero their 4 nodes (main/optim_par.cpp:503-529)
     if (nc == 0 || nc == 1 || nc == ncols - 1 || nc == ncols) {
-      avx = 0.0; vvx = 0.0; vvxL = 0.0; momx = 0.0;
+      avx = R(0); vvx = R(0); vvxL = R(0); momx = R(0);
     }
     if (r == 0 || r == 1 || r == nrows - 1 || r == nrows) {
-      avy = 0.0; vvy = 0.0; vvyL = 0.0; momy = 0.0;
+      avy = R(0); vvy = R(0); vvyL = R(0); momy = R(0);
     }
   }
   nodes.vvxL[n] = vvxL;
@@ -665,8 +689,40 @@ __device__ __forceinline__ void nodal_update(
   }
 }
 
-struct Shape {
-  double ihx, mihx, ihy, mihy;
+template <class R>
+struct ShapeT {
+  R ihx, mihx, ihy, mihy;
+};
+using Shape = ShapeT<double>;
+
+// s += v.  The FP32 chains are compensated (Kahan): c carries the part of
+// the running sum that the last rounding lost, so a chain of thousands of
+// contributions keeps FP32 precision.  The FP64 chains are the reference's
+// plain sums.
+template <class R>
+__device__ __forceinline__ void acc_add(R& s, R& c, R v) {
+  if constexpr (sizeof(R) == 4) {
+    const R y = v - c;
+    const R t = s + y;
+    c = (t - s) - y;
+    s = t;
+  } else {
+    s += v;
+  }
+}
+
+// a chain's value: the FP32 sum with its carried correction
+template <class R>
+__device__ __forceinline__ R acc_value(R s, R c) {
+  if constexpr (sizeof(R) == 4) return s - c;
+  return s;
+}
+
+// Running sums of one lane: finishing (f) and starting (s) chains, with
+// their compensations (FP32 only).
+template <class R>
+struct Chains {
+  R f[3], fc[3], s[3], sc[3];
 };
 
 // One particle's contributions to the chains of quantity group kG: `upper`
@@ -676,66 +732,63 @@ struct Shape {
 //   start N = xi*fb,     Nx = ihx*fb,  Ny = xi*(ihy or mihy)
 // -- shp/shg of main/gpu_kernels.cpp:33-59 for those local nodes.  kFin off
 // runs the started chains alone (a unit's leading column).
-template <int kG, bool kFin>
-__device__ __forceinline__ void chain_step(double (&af)[3], double (&as)[3],
-                                           const P2GSmem& s, int l, bool upper,
-                                           const Shape& sh) {
-  const double xi = s.rec[0][l], eta = s.rec[1][l];
-  const double fa = 1.0 - xi;
-  const double fb = upper ? eta : (1.0 - eta);
-  const double Nf = fa * fb;
-  const double Ns = xi * fb;
+template <class R, int kG, bool kFin>
+__device__ __forceinline__ void chain_step(Chains<R>& a, const P2GSmemT<R>& s, int l,
+                                           bool upper, const ShapeT<R>& sh) {
+  const R xi = s.rec[0][l], eta = s.rec[1][l];
+  const R fa = R(1) - xi;
+  const R fb = upper ? eta : (R(1) - eta);
+  const R Nf = fa * fb;
+  const R Ns = xi * fb;
   if (kG == 0 || kG == 1) {
     const int o = kG == 0 ? 2 : 5;
-    const double q0 = s.rec[o][l], q1 = s.rec[o + 1][l], q2 = s.rec[o + 2][l];
+    const R q0 = s.rec[o][l], q1 = s.rec[o + 1][l], q2 = s.rec[o + 2][l];
     if (kFin) {
-      af[0] += Nf * q0;
-      af[1] += Nf * q1;
-      af[2] += Nf * q2;
+      acc_add(a.f[0], a.fc[0], Nf * q0);
+      acc_add(a.f[1], a.fc[1], Nf * q1);
+      acc_add(a.f[2], a.fc[2], Nf * q2);
     }
-    as[0] += Ns * q0;
-    as[1] += Ns * q1;
-    as[2] += Ns * q2;
+    acc_add(a.s[0], a.sc[0], Ns * q0);
+    acc_add(a.s[1], a.sc[1], Ns * q1);
+    acc_add(a.s[2], a.sc[2], Ns * q2);
   } else {
-    const double hy = upper ? sh.ihy : sh.mihy;
-    const double Nxs = sh.ihx * fb, Nys = xi * hy;
-    const double f12 = s.rec[10][l], vp = s.rec[12][l];
+    const R hy = upper ? sh.ihy : sh.mihy;
+    const R Nxs = sh.ihx * fb, Nys = xi * hy;
+    const R f12 = s.rec[10][l], vp = s.rec[12][l];
     if (kG == 2) {
-      const double q0 = s.rec[8][l], f11 = s.rec[9][l];
+      const R q0 = s.rec[8][l], f11 = s.rec[9][l];
       if (kFin) {
-        const double Nxf = sh.mihx * fb, Nyf = fa * hy;
-        af[0] += Nf * q0;
-        af[1] += (Nxf * f11 + Nyf * f12) * vp;
+        const R Nxf = sh.mihx * fb, Nyf = fa * hy;
+        acc_add(a.f[0], a.fc[0], Nf * q0);
+        acc_add(a.f[1], a.fc[1], (Nxf * f11 + Nyf * f12) * vp);
       }
-      as[0] += Ns * q0;
-      as[1] += (Nxs * f11 + Nys * f12) * vp;
+      acc_add(a.s[0], a.sc[0], Ns * q0);
+      acc_add(a.s[1], a.sc[1], (Nxs * f11 + Nys * f12) * vp);
     } else {
-      const double f22 = s.rec[11][l];
+      const R f22 = s.rec[11][l];
       if (kFin) {
-        const double Nxf = sh.mihx * fb, Nyf = fa * hy;
-        af[0] += (Nxf * f12 + Nyf * f22) * vp;
+        const R Nxf = sh.mihx * fb, Nyf = fa * hy;
+        acc_add(a.f[0], a.fc[0], (Nxf * f12 + Nyf * f22) * vp);
       }
-      as[0] += (Nxs * f12 + Nys * f22) * vp;
+      acc_add(a.s[0], a.sc[0], (Nxs * f12 + Nys * f22) * vp);
     }
   }
 }
 
 // The particles of cells (r-1, cc) and (r, cc) are the adjacent ranges
 // [a0, a1) and [a1, b1) of the sorted order: one walk in order.
-template <int kG, bool kFin>
-__device__ __forceinline__ void chain_range(double (&af)[3], double (&as)[3],
-                                            const P2GSmem& s, int a0, int a1,
-                                            int b1, int bb, int be,
-                                            const Shape& sh, bool own,
-                                            double& lp0, double& lp1,
-                                            double& lp2) {
+template <class R, int kG, bool kFin>
+__device__ __forceinline__ void chain_range(Chains<R>& a, const P2GSmemT<R>& s, int a0,
+                                            int a1, int b1, int bb, int be,
+                                            const ShapeT<R>& sh, bool own,
+                                            double& lp0, double& lp1, double& lp2) {
   const int j1 = min(b1, be);
   int j = max(a0, bb);
 #pragma unroll 2
   for (; j < j1; ++j) {
-    const int l = swz(j - bb);
+    const int l = swz<R>(j - bb);
     const bool upper = j < a1;
-    chain_step<kG, kFin>(af, as, s, l, upper, sh);
+    chain_step<R, kG, kFin>(a, s, l, upper, sh);
     if (kG == 0 && own && !upper) {  // particle ledger, once each
       lp0 += s.rec[2][l];
       lp1 += s.rec[3][l];
@@ -744,17 +797,15 @@ __device__ __forceinline__ void chain_range(double (&af)[3], double (&as)[3],
   }
 }
 
-template <int kG>
-__device__ __forceinline__ void chain_group(double (&af)[3], double (&as)[3],
-                                            const P2GSmem& s, bool lead, int a0,
-                                            int a1, int b1, int bb, int be,
-                                            const Shape& sh, bool own,
-                                            double& lp0, double& lp1,
-                                            double& lp2) {
+template <class R, int kG>
+__device__ __forceinline__ void chain_group(Chains<R>& a, const P2GSmemT<R>& s, bool lead,
+                                            int a0, int a1, int b1, int bb, int be,
+                                            const ShapeT<R>& sh, bool own, double& lp0,
+                                            double& lp1, double& lp2) {
   if (lead)
-    chain_range<kG, false>(af, as, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
+    chain_range<R, kG, false>(a, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
   else
-    chain_range<kG, true>(af, as, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
+    chain_range<R, kG, true>(a, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
 }
 
 }  // namespace
@@ -930,11 +981,12 @@ __global__ void __launch_bounds__(kPlanThreads)
   }
 }
 
+template <class R>
 __device__ __forceinline__ void p2g_unit(
-    const Particles& p, const int* __restrict__ perm,
-    const int* __restrict__ cstart, const Nodes& nodes,
+    const ParticlesT<R>& p, const int* __restrict__ perm,
+    const int* __restrict__ cstart, const NodesT<R>& nodes,
     double* __restrict__ led_part, const Geom& G, const Phys& P,
-    const Scalars* S, int record, P2GSmem& s, int slot, int4 unit) {
+    const Scalars* S, int record, P2GSmemT<R>& s, int slot, int4 unit) {
   const int nrows = G.nrows, ncols = G.ncols;
   const int r0 = unit.x * kTR;
   const int cA = unit.y;
@@ -952,14 +1004,16 @@ __device__ __forceinline__ void p2g_unit(
   const bool lane_ok = row < kTR;  // lanes kTR..31 idle
   const bool row_ok = lane_ok && (r <= nrows);
   const double dt = S->dt;
-  const Shape sh{1.0 / G.hx, -1.0 / G.hx, 1.0 / G.hy, -1.0 / G.hy};
+  const ShapeT<R> sh{R(1) / R(G.hx), -R(1) / R(G.hx), R(1) / R(G.hy), -R(1) / R(G.hy)};
   // exchange slots of each group's quantities: g0 0-2, g1 3-5, g2 6-7, g3 8
   const int slot0 = grp == 0 ? 0 : grp == 1 ? 3 : grp == 2 ? 6 : 8;
   const int nq = grp < 2 ? 3 : grp == 2 ? 2 : 1;
   const bool last_unit_col = (cB == ncols + 1);  // this unit closes node column ncols
 
   double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
-  double af[3] = {0, 0, 0}, as[3] = {0, 0, 0};
+  Chains<R> a;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) a.f[q] = a.fc[q] = a.s[q] = a.sc[q] = R(0);
 
   // prologue: row starts of the first two columns, sorted indices of batch 0
   for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
@@ -981,9 +1035,9 @@ __device__ __forceinline__ void p2g_unit(
     issue_gather(s, p, pf, cur);
     // while the copies fly: this batch's bookkeeping and the next batch's
     // sorted indices
-    const int* R = s.rowstart[cur.cc % 3];
-    const bool first_of_col = (cur.bb == R[0]);
-    const bool last_of_col = (cur.be == R[nrs - 1]);
+    const int* RS = s.rowstart[cur.cc % 3];
+    const bool first_of_col = (cur.bb == RS[0]);
+    const bool last_of_col = (cur.be == RS[nrs - 1]);
     int rs2 = 0;
     const bool has_rs2 = last_of_col && cur.cc + 2 <= ccLast && tid < nrs;
     if (has_rs2) rs2 = cstart[rlo + tid + (cur.cc + 2) * nrows];
@@ -992,9 +1046,9 @@ __device__ __forceinline__ void p2g_unit(
       a0 = a1 = b1 = 0;
       if (row_ok && r >= rlo && r <= rhi + 1) {
         const int k = r - rlo;  // row start of cell r (= end of cell r-1)
-        a1 = R[k];
-        a0 = (r - 1 >= rlo) ? R[k - 1] : a1;
-        b1 = (r <= rhi) ? R[k + 1] : a1;
+        a1 = RS[k];
+        a0 = (r - 1 >= rlo) ? RS[k - 1] : a1;
+        b1 = (r <= rhi) ? RS[k + 1] : a1;
       }
     }
     const Batch nxt = next_batch(cur, s, nrs, ccLast);
@@ -1004,42 +1058,44 @@ __device__ __forceinline__ void p2g_unit(
     const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA;
     const bool lead = cur.cc < cA;  // started chains only
     switch (grp) {
-      case 0: chain_group<0>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      case 1: chain_group<1>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      case 2: chain_group<2>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      default: chain_group<3>(af, as, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      case 0: chain_group<R, 0>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      case 1: chain_group<R, 1>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      case 2: chain_group<R, 2>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      default: chain_group<R, 3>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
     }
     if (last_of_col) {
       if (lane_ok)
-        for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = af[q];
+        for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = acc_value(a.f[q], a.fc[q]);
       if (has_rs2) s.rowstart[(cur.cc + 2) % 3][tid] = rs2;
     }
     __syncthreads();  // shared records free; finished sums exchanged
     if (last_of_col) {
       // ---- nodal update of node column cc ------------------------------
       if (warp == 0 && row_ok && cur.cc >= cA) {
-        const double (*X)[kTR] = s.xch;
-        nodal_update(af[0], af[1], af[2], X[3][row], X[4][row], X[5][row],
-                     X[6][row], X[7][row], X[8][row], r, cur.cc, G, P, dt, nodes,
-                     record, ln0, ln1, ln2);
+        const R (*X)[kTR] = s.xch;
+        nodal_update<R>(X[0][row], X[1][row], X[2][row], X[3][row], X[4][row],
+                        X[5][row], X[6][row], X[7][row], X[8][row], r, cur.cc, G, P,
+                        dt, nodes, record, ln0, ln1, ln2);
       }
       if (cur.cc == ncols - 1 && last_unit_col) {
         // node column ncols: its chains end with this column
         __syncthreads();  // warp 0 is done reading the exchange
         if (lane_ok)
-          for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = as[q];
+          for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = acc_value(a.s[q], a.sc[q]);
         __syncthreads();
         if (warp == 0 && row_ok) {
-          const double (*X)[kTR] = s.xch;
-          nodal_update(as[0], as[1], as[2], X[3][row], X[4][row], X[5][row],
-                       X[6][row], X[7][row], X[8][row], r, ncols, G, P, dt,
-                       nodes, record, ln0, ln1, ln2);
+          const R (*X)[kTR] = s.xch;
+          nodal_update<R>(X[0][row], X[1][row], X[2][row], X[3][row], X[4][row],
+                          X[5][row], X[6][row], X[7][row], X[8][row], r, ncols, G, P,
+                          dt, nodes, record, ln0, ln1, ln2);
         }
       }
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        af[q] = as[q];
-        as[q] = 0.0;
+        a.f[q] = a.s[q];
+        a.fc[q] = a.sc[q];
+        a.s[q] = R(0);
+        a.sc[q] = R(0);
       }
     }
     if (!nxt.valid) break;
@@ -1136,33 +1192,35 @@ __global__ void k_ledger_final(const double* __restrict__ led_part,
 // ---------------------------------------------------------------------------
 // One particle of G2P (the body of k_g2p and of the batched G2P).  key_off
 // is added to the cell key (the scenario's first cell in a batch).
+template <class R>
 __device__ __forceinline__ void g2p_particle(
-    const Particles& p, int i, const Nodes& nodes, const double* __restrict__ Z,
-    const Geom& G, const Phys& P, const Shape& sh, double dt, int record,
+    const ParticlesT<R>& p, int i, const NodesT<R>& nodes, const double* __restrict__ Z,
+    const Geom& G, const Phys& P, const ShapeT<R>& sh, double dtd, int record,
     int want_grad, int key_off, unsigned long long& m0, unsigned long long& m1,
     unsigned long long& m2) {
   const int nrows = G.nrows, ncols = G.ncols;
   const double hx = G.hx, hy = G.hy;
-  const double ihx = sh.ihx, mihx = sh.mihx;
-  const double ihy = sh.ihy, mihy = sh.mihy;
-  const double eps = 1e-10;
+  const R ihx = sh.ihx, mihx = sh.mihx;
+  const R ihy = sh.ihy, mihy = sh.mihy;
+  const R eps = R(1e-10);
+  const R dt = R(dtd);
   const int key = p.key[i] - key_off;
   const int r = key % nrows, c = key / nrows;
   int nd[4];
-  double vxn[4], vyn[4];
+  R vxn[4], vyn[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     nd[k] = node_of(k, c, r, nrows);
     vxn[k] = nodes.vvxL[nd[k]];
     vyn[k] = nodes.vvyL[nd[k]];
   }
-  double x = p.x[i], y = p.y[i];
-  double xi, eta;
+  R x = p.x[i], y = p.y[i];
+  R xi, eta;
   local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
-  double vxL = 0.0, vyL = 0.0;
+  R vxL = R(0), vyL = R(0);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const double N = shp(xi, eta, k);
+    const R N = shp(xi, eta, k);
     vxL += N * vxn[k];
     vyL += N * vyn[k];
   }
@@ -1170,51 +1228,52 @@ __device__ __forceinline__ void g2p_particle(
     // this step's intermediates as the reference's dprops hold them after
     // the step (main/optim_par.cpp:387-459,542): apx/apy, grad Z and the
     // gravity and friction forces of this step's P2G
-    double ax = 0.0, ay = 0.0, dzx = 0.0, dzy = 0.0;
+    R ax = R(0), ay = R(0);
+    double dzx = 0.0, dzy = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double N = shp(xi, eta, k);
+      const R N = shp(xi, eta, k);
       ax += N * nodes.avx[nd[k]];
       ay += N * nodes.avy[nd[k]];
       const double zn = Z[nd[k]];
-      dzx += shg_x(eta, k, ihx, mihx) * zn;
-      dzy += shg_y(xi, k, ihy, mihy) * zn;
+      dzx += double(shg_x(eta, k, ihx, mihx)) * zn;
+      dzy += double(shg_y(xi, k, ihy, mihy)) * zn;
     }
     p.apx[i] = ax;
     p.apy[i] = ay;
-    p.dZxp[i] = dzx;
-    p.dZyp[i] = dzy;
+    p.dZxp[i] = R(dzx);
+    p.dZyp[i] = R(dzy);
     p.Fpx[i] = p.qgx[i];
     p.Fpy[i] = p.qgy[i];
     p.Frx[i] = p.qfx[i];
     p.Fry[i] = p.qfy[i];
   }
-  const double vpx = vxL, vpy = vyL;
+  const R vpx = vxL, vpy = vyL;
   x = x + dt * vpx;
   y = y + dt * vpy;
   if (x < eps) x = eps;
-  if (x > G.Lx - eps) x = G.Lx - eps;
+  if (x > R(G.Lx) - eps) x = R(G.Lx) - eps;
   if (y < eps) y = eps;
-  if (y > G.Ly - eps) y = G.Ly - eps;
+  if (y > R(G.Ly) - eps) y = R(G.Ly) - eps;
   // g2pd {vvxL, vvyL} at the new position, old cell (main/optim_par.cpp:578)
   local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
-  double vxdx = 0.0, vydx = 0.0, vxdy = 0.0, vydy = 0.0;
+  R vxdx = R(0), vydx = R(0), vxdy = R(0), vydy = R(0);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const double Nx = shg_x(eta, k, ihx, mihx);
-    const double Ny = shg_y(xi, k, ihy, mihy);
+    const R Nx = shg_x(eta, k, ihx, mihx);
+    const R Ny = shg_y(xi, k, ihy, mihy);
     vxdx += Nx * vxn[k];
     vxdy += Ny * vxn[k];
     vydx += Nx * vyn[k];
     vydy += Ny * vyn[k];
   }
   // height from the strain rate (main/optim_par.cpp:595-599)
-  const double div = vxdx + vydy;
-  double hp = p.hp[i];
-  hp = hp / (1 + dt * div);
-  hp = hp < 1e-2 ? 1e-2 : hp;
-  double F11, F12, F22;
-  const double H = p.H[i];
+  const R div = vxdx + vydy;
+  R hp = p.hp[i];
+  hp = hp / (R(1) + dt * div);
+  hp = hp < R(1e-2) ? R(1e-2) : hp;
+  R F11, F12, F22;
+  const R H = p.H[i];
   bingham_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
   p.x[i] = x;
   p.y[i] = y;
@@ -1224,7 +1283,7 @@ __device__ __forceinline__ void g2p_particle(
   p.F11[i] = F11;
   p.F12[i] = F12;
   p.F22[i] = F22;
-  const int nr = cell_row(y, hy, nrows), ncl = cell_col(x, hx, ncols);
+  const int nr = cell_row(double(y), hy, nrows), ncl = cell_col(double(x), hx, ncols);
   p.key[i] = nr + ncl * nrows + key_off;
   if (want_grad) {
     p.vpx_dx[i] = vxdx;
@@ -1237,15 +1296,15 @@ __device__ __forceinline__ void g2p_particle(
   // the local coordinates and gravity force in the cell of the next
   // binning (:387,447-454)
   {
-    const double Mp = p.Mp[i], Vp = p.Vp[i];
+    const R Mp = p.Mp[i], Vp = p.Vp[i];
     p.mpx[i] = vpx * Mp;
     p.mpy[i] = vpy * Mp;
-    const double Ap = hp > 1.e-2 ? Vp / hp : 0.0;
-    double fbx, fby;
+    const R Ap = hp > R(1.e-2) ? Vp / hp : R(0);
+    R fbx, fby;
     voellmy(P, vpx, vpy, hp, fbx, fby);
     p.qfx[i] = Ap * fbx;
     p.qfy[i] = Ap * fby;
-    double qxi, qeta, qgx, qgy;
+    R qxi, qeta, qgx, qgy;
     next_record(G, P, Z, x, y, hp, H, Vp, qxi, qeta, qgx, qgy);
     p.qxi[i] = qxi;
     p.qeta[i] = qeta;
@@ -1256,13 +1315,13 @@ __device__ __forceinline__ void g2p_particle(
     // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
     double zp = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) zp += shp(xi, eta, k) * Z[nd[k]];
-    p.Zp[i] = zp;
-    p.hpZ[i] = hp + zp;
+    for (int k = 0; k < 4; ++k) zp += double(shp(xi, eta, k)) * Z[nd[k]];
+    p.Zp[i] = R(zp);
+    p.hpZ[i] = R(double(hp) + zp);
   }
-  m0 = max(m0, ordered_key(fabs(vpx)));
-  m1 = max(m1, ordered_key(fabs(vpy)));
-  m2 = max(m2, ordered_key(hp));
+  m0 = max(m0, ordered_key(double(fabs(vpx))));
+  m1 = max(m1, ordered_key(double(fabs(vpy))));
+  m2 = max(m2, ordered_key(double(hp)));
 }
 
 // Block reduction of the CFL maxima into one scenario's next-step slots.
@@ -1306,7 +1365,22 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
   cfl_block_max(m0, m1, m2, red, S);
 }
 
-size_t p2g_smem_bytes() { return sizeof(P2GSmem); }
+size_t p2g_smem_bytes() { return sizeof(P2GSmemT<double>); }
+size_t p2g_smem_bytes_f32() { return sizeof(P2GSmemT<float>); }
+
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b,
+                         long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = float(a[i]);
+}
+
+__global__ void k_to_f64(const float* __restrict__ a, double* __restrict__ b,
+                         long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = double(a[i]);
+}
 
 // ---------------------------------------------------------------------------
 // BATCH: the same step over many independent scenarios packed back to back.
@@ -1406,15 +1480,16 @@ __global__ void __launch_bounds__(kPlanThreads)
   }
 }
 
+template <class R>
 __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
-    k_b_p2g(Particles p, const int* __restrict__ perm, const int* __restrict__ cstart,
-            double* __restrict__ vvxL, double* __restrict__ vvyL,
+    k_b_p2g(ParticlesT<R> p, const int* __restrict__ perm, const int* __restrict__ cstart,
+            R* __restrict__ vvxL, R* __restrict__ vvyL,
             double* __restrict__ led_part, const Scn* __restrict__ scn, Scalars* S,
             const int4* __restrict__ ulist, const int* __restrict__ ucount,
             const Scalars* Sg) {
   if (!Sg->active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
+  P2GSmemT<R>& sm = *reinterpret_cast<P2GSmemT<R>*>(smem_raw);
   const int nunits = ucount[0];
   __shared__ int next_unit;
   while (true) {
@@ -1427,10 +1502,10 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     const Geom G = scn[u.x].G;
     const Phys P = scn[u.x].P;
     const int n_off = scn[u.x].n_off, c_off = scn[u.x].c_off;
-    Nodes nd{};
+    NodesT<R> nd{};
     nd.vvxL = vvxL + n_off;
     nd.vvyL = vvyL + n_off;
-    p2g_unit(p, perm, cstart + c_off, nd, led_part, G, P, &S[u.x], 0, sm, ui,
+    p2g_unit<R>(p, perm, cstart + c_off, nd, led_part, G, P, &S[u.x], 0, sm, ui,
              make_int4(u.y, u.z, u.w, 0));
   }
 }
@@ -1446,9 +1521,10 @@ __global__ void k_b_ledger(const double* __restrict__ led_part,
 }
 
 // gblk[b] = {scenario, its first particle handled by block b}
+template <class R>
 __global__ void __launch_bounds__(kG2PThreads, 3)
-    k_b_g2p(Particles p, const double* __restrict__ vvxL,
-            const double* __restrict__ vvyL, const double* __restrict__ Z,
+    k_b_g2p(ParticlesT<R> p, const R* __restrict__ vvxL,
+            const R* __restrict__ vvyL, const double* __restrict__ Z,
             const Scn* __restrict__ scn, Scalars* S, const int2* __restrict__ gblk,
             const Scalars* Sg) {
   if (!Sg->active) return;
@@ -1462,10 +1538,10 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
   const Phys P = scn[s].P;
   const int p_off = scn[s].p_off, np = scn[s].np;
   const int n_off = scn[s].n_off, c_off = scn[s].c_off;
-  Nodes nd{};
-  nd.vvxL = const_cast<double*>(vvxL) + n_off;
-  nd.vvyL = const_cast<double*>(vvyL) + n_off;
-  const Shape sh{1.0 / G.hx, -1.0 / G.hx, 1.0 / G.hy, -1.0 / G.hy};
+  NodesT<R> nd{};
+  nd.vvxL = const_cast<R*>(vvxL) + n_off;
+  nd.vvyL = const_cast<R*>(vvyL) + n_off;
+  const ShapeT<R> sh{R(1) / R(G.hx), -R(1) / R(G.hx), R(1) / R(G.hy), -R(1) / R(G.hy)};
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   const int li = e.y + threadIdx.x;
   if (li < np)
@@ -1477,15 +1553,16 @@ __global__ void __launch_bounds__(kG2PThreads, 3)
 // Compaction of a batch into the other half of its double buffer:
 // mblk[b] = {destination first particle, source first particle, count <= 256,
 // cell-key shift}.
-__global__ void k_b_move(Particles dst, Particles src, const int4* __restrict__ mblk) {
+template <class R>
+__global__ void k_b_move(ParticlesT<R> dst, ParticlesT<R> src, const int4* __restrict__ mblk) {
   const int4 m = mblk[blockIdx.x];
   if ((int)threadIdx.x >= m.z) return;
   const int i = m.y + threadIdx.x, o = m.x + threadIdx.x;
-  double* const* df[] = {&dst.x, &dst.y, &dst.vpx, &dst.vpy, &dst.hp, &dst.F11,
+  R* const* df[] = {&dst.x, &dst.y, &dst.vpx, &dst.vpy, &dst.hp, &dst.F11,
                          &dst.F12, &dst.F22, &dst.Mp, &dst.Vp, &dst.H, &dst.mpx,
                          &dst.mpy, &dst.qfx, &dst.qfy, &dst.qxi, &dst.qeta, &dst.qgx,
                          &dst.qgy, &dst.Ap, &dst.Fbx, &dst.Fby};
-  double* const* sf[] = {&src.x, &src.y, &src.vpx, &src.vpy, &src.hp, &src.F11,
+  R* const* sf[] = {&src.x, &src.y, &src.vpx, &src.vpy, &src.hp, &src.F11,
                          &src.F12, &src.F22, &src.Mp, &src.Vp, &src.H, &src.mpx,
                          &src.mpy, &src.qfx, &src.qfy, &src.qxi, &src.qeta, &src.qgx,
                          &src.qgy, &src.Ap, &src.Fbx, &src.Fby};
@@ -1540,5 +1617,74 @@ __global__ void k_hv(const Particles p, const int* __restrict__ perm,
     HV[n] = acc;
   }
 }
+
+// ---- host launchers: the FP64 path and the FP32 form -----------------------
+template <class R>
+void launch_init_particles(int grid, int block, cudaStream_t st, ParticlesT<R> p,
+                           const double* Z, const double* dZdx, const double* dZdy,
+                           Geom G, Phys P, Scalars* S, int np, int key_off) {
+  k_init_particles<R><<<grid, block, 0, st>>>(p, Z, dZdx, dZdy, G, P, S, np, key_off);
+}
+
+template <class R>
+void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const double* Z,
+                 Geom G, Phys P, const Scalars* S, int derive) {
+  k_prep<R><<<grid, block, 0, st>>>(p, Z, G, P, S, derive);
+}
+
+template <class R>
+void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
+                  const int* cstart, R* vvxL, R* vvyL, double* led_part, const Scn* scn,
+                  Scalars* S, const int4* ulist, const int* ucount, const Scalars* Sg) {
+  k_b_p2g<R><<<grid, kP2GThreads, sizeof(P2GSmemT<R>), st>>>(
+      p, perm, cstart, vvxL, vvyL, led_part, scn, S, ulist, ucount, Sg);
+}
+
+template <class R>
+int setup_b_p2g() {
+  const int smem = int(sizeof(P2GSmemT<R>));
+  if (cudaFuncSetAttribute(k_b_p2g<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem) != cudaSuccess)
+    return 0;
+  cudaFuncSetAttribute(k_b_p2g<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       int(cudaSharedmemCarveoutMaxShared));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_p2g<R>, kP2GThreads,
+                                                    smem) != cudaSuccess)
+    return 0;
+  return per_sm < 1 ? 1 : per_sm;
+}
+
+template <class R>
+void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const R* vvxL,
+                  const R* vvyL, const double* Z, const Scn* scn, Scalars* S,
+                  const int2* gblk, const Scalars* Sg) {
+  k_b_g2p<R><<<grid, kG2PThreads, 0, st>>>(p, vvxL, vvyL, Z, scn, S, gblk, Sg);
+}
+
+template <class R>
+void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> src,
+                   const int4* mblk) {
+  k_b_move<R><<<grid, kG2PThreads, 0, st>>>(dst, src, mblk);
+}
+
+#define DAMPM_INSTANTIATE(R)                                                          \
+  template void launch_init_particles<R>(int, int, cudaStream_t, ParticlesT<R>,       \
+                                         const double*, const double*, const double*, \
+                                         Geom, Phys, Scalars*, int, int);             \
+  template void launch_prep<R>(int, int, cudaStream_t, ParticlesT<R>, const double*,  \
+                               Geom, Phys, const Scalars*, int);                      \
+  template void launch_b_p2g<R>(int, cudaStream_t, ParticlesT<R>, const int*,         \
+                                const int*, R*, R*, double*, const Scn*, Scalars*,    \
+                                const int4*, const int*, const Scalars*);             \
+  template int setup_b_p2g<R>();                                                      \
+  template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, const R*, const R*, \
+                                const double*, const Scn*, Scalars*, const int2*,     \
+                                const Scalars*);                                      \
+  template void launch_b_move<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,     \
+                                 const int4*);
+DAMPM_INSTANTIATE(double)
+DAMPM_INSTANTIATE(float)
+#undef DAMPM_INSTANTIATE
 
 }  // namespace dampm

@@ -32,6 +32,8 @@ from .data import DATA
 # persistent state, sort and P2G scratch)
 BYTES_PER_PARTICLE = 390
 BYTES_PER_NODE = 56
+BYTES_PER_PARTICLE_F32 = 210
+BYTES_PER_NODE_F32 = 48
 _INT_MAX = 2**31 - 1
 
 
@@ -59,15 +61,18 @@ class Server:
 
     def __init__(self, budget_bytes: float, max_scenarios: int = 1024, tick: int = 16,
                  node_share: float = 0.45, result_fields: Sequence[str] = ("x", "y", "hp"),
-                 stream: Optional[int] = None):
-        pc = int(budget_bytes * (1.0 - node_share) / BYTES_PER_PARTICLE)
-        nc = int(budget_bytes * node_share / BYTES_PER_NODE)
+                 stream: Optional[int] = None, precision: str = "fp64"):
+        bpp, bpn = ((BYTES_PER_PARTICLE_F32, BYTES_PER_NODE_F32) if precision == "fp32"
+                    else (BYTES_PER_PARTICLE, BYTES_PER_NODE))
+        pc = int(budget_bytes * (1.0 - node_share) / bpp)
+        nc = int(budget_bytes * node_share / bpn)
         self.particle_cap = min(pc, _INT_MAX)
         self.node_cap = min(nc, _INT_MAX)
         self.max_scenarios = max_scenarios
         self.tick = tick
         self.fields = tuple(result_fields)
-        self.b = Batch(self.particle_cap, self.node_cap, max_scenarios, stream=stream)
+        self.b = Batch(self.particle_cap, self.node_cap, max_scenarios, stream=stream,
+                       precision=precision)
         self.compactions = 0
         self.ticks = 0
         self.occupancy: List[int] = []

@@ -264,7 +264,7 @@ def run_ensemble(args, world, rank, local):
     # end to end: host arrays in, all passes, final depths out
     _barrier(world)
     t0 = time.perf_counter()
-    b = Batch(P + 1024, N + 1024, n + 1, stream=stream.cuda_stream)
+    b = Batch(P + 1024, N + 1024, n + 1, stream=stream.cuda_stream, precision=args.precision)
     hs = [b.add(d) for d in ds]
     b.step(W)
     b.sync()
@@ -314,10 +314,11 @@ def run_ensemble(args, world, rank, local):
             "metric": "ensemble scenarios/s", "value": value, "unit": "scenarios/s",
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": el_ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
+            "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
             "config": {"workload": f"ensemble of {n} scenarios: side logU[64,512] cells, h=1 m, "
                                    "4 ppc, Bingham+Voellmy, dt=0.02 s",
                        "scenarios": n, "particles": P, "nodes": N, "passes": K,
+                       "precision": args.precision,
                        "parallelism": f"batch; replicas{world}",
                        "l2": f"state {P * 188 / 1e6:.0f} MB > 126 MB L2, no flush"},
             "particle_steps_per_s": P * K / (el_ms * 1e-3) * world,
@@ -360,7 +361,7 @@ def run_serving(args, world, rank, local):
     budget = min(args.budget_gb * 1e9, 0.8 * free)
     stream = torch.cuda.Stream()
     srv = Server(budget, max_scenarios=args.max_scenarios, tick=args.tick,
-                 stream=stream.cuda_stream)
+                 stream=stream.cuda_stream, precision=args.precision)
     # warm-up: one short request through the same server
     warm = scenarios.serving_request(999999, t_end=0.2)
     srv.run([Request(-1, warm, 0.0)])
@@ -399,11 +400,13 @@ def run_serving(args, world, rank, local):
             "metric": "serving scenarios/s", "value": value, "unit": "scenarios/s",
             "n_gpus": world, "steps": int(passes), "warmup": 1,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic",
             "config": {"workload": f"serving: {n} requests, Poisson {args.rate}/s, side "
                                    "logU[64,1024] cells, h=1 m, CFL 0.4 to t=60 s",
                        "requests": n, "rate_per_s": args.rate, "t_end_s": args.t_end,
                        "budget_gb": round(budget / 1e9, 1), "tick_passes": args.tick,
+                       "precision": args.precision,
                        "parallelism": f"continuous batching; replicas{world}",
                        "l2": "state > 126 MB L2 at full occupancy, no flush"},
             "latency": lat,
@@ -442,6 +445,8 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--max-scenarios", type=int, default=1024)
     ap.add_argument("--tick", type=int, default=16)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="ensemble and serving workloads: fp32 runs the FP32 form")
     ap.add_argument("--scenarios", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
