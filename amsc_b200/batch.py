@@ -9,6 +9,7 @@ this is that loop body applied to many scenarios at once.
 from __future__ import annotations
 
 import ctypes as C
+import time
 from typing import Dict, Optional
 
 import numpy as np
@@ -40,6 +41,7 @@ class Batch:
             raise DampmError(f"dampm_batch_create failed ({rc})")
         self.h = h
         self.np: Dict[int, int] = {}
+        self._tuning = (4, 192)  # the library's defaults
 
     def _check(self, rc: int):
         if rc != 0:
@@ -110,6 +112,51 @@ class Batch:
         out = np.empty(9, dtype=np.float64)
         self._check(self.lib.dampm_batch_ledgers(self.h, int(handle), _ptr(out)))
         return out
+
+    def tune(self, units_per_cta: int = 0, col_weight: int = 0, graphs: Optional[bool] = None):
+        """P2G units per CTA, column weight of the unit plan, CUDA-graph
+        replay of multi-pass steps (0 / None keeps a setting)."""
+        g = -1 if graphs is None else (1 if graphs else 0)
+        self._check(self.lib.dampm_batch_tune(self.h, int(units_per_cta), int(col_weight), g))
+
+    def autotune(self, passes: int = 16, units=(2, 4, 8), weights=(64, 192, 512),
+                 margin: float = 0.03) -> Dict:
+        """Coordinate search over the unit plan (units per CTA, then column
+        weight) from the current setting.  Each trial times `passes` passes
+        twice and keeps the better; a candidate replaces the current setting
+        only when it is more than `margin` faster, so noise cannot make the
+        choice worse.  The passes are real passes of the run: unit cuts
+        change no result, only time."""
+        def measure(u, w):
+            self.tune(u, w)
+            self.step(passes)  # capture of the graph for this setting
+            self.sync()
+            best = float("inf")
+            for _ in range(2):
+                t0 = time.perf_counter()
+                self.step(passes)
+                self.sync()
+                best = min(best, (time.perf_counter() - t0) / passes)
+            trials.append((u, w, round(1e3 * best, 4)))
+            return best
+
+        trials = []
+        cu, cw = self._tuning
+        cur = measure(cu, cw)
+        for u in units:
+            if u != cu:
+                t = measure(u, cw)
+                if t < cur * (1.0 - margin):
+                    cu, cur = u, t
+        for w in weights:
+            if w != cw:
+                t = measure(cu, w)
+                if t < cur * (1.0 - margin):
+                    cw, cur = w, t
+        self.tune(cu, cw)
+        self._tuning = (cu, cw)
+        return {"units_per_cta": cu, "col_weight": cw, "ms_per_pass": 1e3 * cur,
+                "passes": 3 * passes * len(trials), "trials": trials}
 
     def states(self) -> Dict[int, Dict[str, float]]:
         """Loop state of every live scenario, one synchronisation."""

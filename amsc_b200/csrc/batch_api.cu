@@ -67,6 +67,12 @@ struct dampm_batch {
   Scalars* Sh = nullptr;  // pinned mirror of S
   int p2g_grid = 1;
   long long launches = 0;
+  // tuning: P2G units per CTA and the weight of a column in the unit plan
+  int units_per_cta = kUnitsPerCta, col_weight = kColWeight;
+  // passes captured in a CUDA graph, replayed while the layout holds
+  int use_graphs = 1, graph_passes = 0;
+  bool graph_dirty = true;
+  cudaGraphExec_t graph = nullptr;
   std::vector<void*> allocs;
   std::string err;
 };
@@ -173,6 +179,7 @@ int upload_tables(dampm_batch* b) {
   g.active = 1;
   BCK(cudaMemcpyAsync(b->Sg, &g, sizeof(Scalars), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaStreamSynchronize(b->stream));  // host vectors die here
+  b->graph_dirty = true;  // launch sizes or buffers changed
   return DAMPM_OK;
 }
 
@@ -210,8 +217,8 @@ int enqueue_pass(dampm_batch* b) {
   k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
                                             b->slot, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
-      b->start, b->scn, b->S, b->strip_scn, b->Sg, kUnitsPerCta * b->p2g_grid, b->ustart,
-      b->upex, b->uplan, b->strip_n);
+      b->start, b->scn, b->S, b->strip_scn, b->Sg, b->units_per_cta * b->p2g_grid,
+      b->col_weight, b->ustart, b->upex, b->uplan, b->strip_n);
   k_b_units_flat<<<1, kPlanThreads, sizeof(int) * (b->strips_tot + 1), st>>>(
       b->strip_n, b->strips_tot, b->strip_scn, b->scn, nscn, b->uplan, b->ulist,
       b->ucount, b->scn_units, b->Sg);
@@ -393,6 +400,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
 int dampm_batch_destroy(dampm_batch* b) {
   if (!b) return DAMPM_ERR_ARG;
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
   for (void* q : b->allocs) cudaFree(q);
   if (b->Sh) cudaFreeHost(b->Sh);
   if (b->own_stream) cudaStreamDestroy(b->stream);
@@ -548,11 +556,51 @@ int dampm_batch_compact(dampm_batch* b) {
 
 int dampm_batch_step(dampm_batch* b, int nsteps) {
   if (!b || nsteps < 0) return DAMPM_ERR_ARG;
-  if (b->scns.empty()) return DAMPM_OK;
-  for (int k = 0; k < nsteps; ++k) {
-    int rc = enqueue_pass(b);
-    if (rc) return rc;
+  if (b->scns.empty() || nsteps == 0) return DAMPM_OK;
+  if (!b->use_graphs || nsteps < 2) {
+    for (int k = 0; k < nsteps; ++k) {
+      int rc = enqueue_pass(b);
+      if (rc) return rc;
+    }
+    return DAMPM_OK;
   }
+  // nsteps passes as one CUDA graph: captured after any change of layout or
+  // pass count, replayed otherwise (the launches' sizes and pointers depend
+  // only on the layout; every other change lives in device memory)
+  if (b->graph_dirty || b->graph_passes != nsteps || !b->graph) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const long long l0 = b->launches;
+    int rc = DAMPM_OK;
+    for (int k = 0; k < nsteps && rc == DAMPM_OK; ++k) rc = enqueue_pass(b);
+    b->launches = l0;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
+    b->graph_passes = nsteps;
+    b->graph_dirty = false;
+  }
+  BCK(cudaGraphLaunch(b->graph, b->stream));
+  b->launches += 15LL * nsteps;
+  return DAMPM_OK;
+}
+
+int dampm_batch_tune(dampm_batch* b, int units_per_cta, int col_weight, int use_graphs) {
+  if (!b || units_per_cta < 0 || col_weight < 0 || use_graphs < -1) return DAMPM_ERR_ARG;
+  if (units_per_cta > 0) b->units_per_cta = units_per_cta;
+  if (col_weight > 0) b->col_weight = col_weight;
+  if (use_graphs >= 0) b->use_graphs = use_graphs;
+  b->graph_dirty = true;
   return DAMPM_OK;
 }
 

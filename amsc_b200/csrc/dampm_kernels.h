@@ -130,8 +130,8 @@ __global__ void k_b_step_begin(const Scn* scn, Scalars* S, int nscn, Scalars* Sg
 __global__ void k_b_step_end(const Scn* scn, Scalars* S, int nscn);
 __global__ void k_b_units_plan(const int* cstart, const Scn* scn, const Scalars* S,
                                const int* strip_scn, const Scalars* Sg,
-                               int target_units, int* ustart, long long* upex,
-                               int2* plan, int* strip_n);
+                               int target_units, int col_weight, int* ustart,
+                               long long* upex, int2* plan, int* strip_n);
 __global__ void k_b_units_flat(const int* strip_n, int strips, const int* strip_scn,
                                const Scn* scn, int nscn, const int2* plan,
                                int4* ulist, int* ucount, int2* scn_units,

@@ -866,7 +866,7 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
                                           const Geom& G, long long T, int strip,
                                           int* __restrict__ st,
                                           long long* __restrict__ px,
-                                          int2* __restrict__ plan) {
+                                          int2* __restrict__ plan, int col_weight) {
   __shared__ long long wt_ll[32];
   __shared__ int wt_i[32];
   __shared__ long long last_id;
@@ -878,7 +878,7 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
   for (int base = 0; base <= ncols; base += blockDim.x) {
     const int nc = base + threadIdx.x;
     long long w = 0;
-    if (nc < ncols) w = column_count(cstart, rlo, rhi, nc, nrows) + kColWeight;
+    if (nc < ncols) w = column_count(cstart, rlo, rhi, nc, nrows) + col_weight;
     long long tot;
     const long long incl = block_incl_scan<long long>(w, wt_ll, tot);
     const long long pex = carry + incl - w;
@@ -913,7 +913,7 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
       const bool more = k + 1 < K;
       cB = more ? st[k + 1] : ncols + 1;
       const long long sumw = (more ? px[k + 1] : ptotal) - px[k];
-      const long long n = sumw - (long long)kColWeight * (min(cB, ncols) - cA) +
+      const long long n = sumw - (long long)col_weight * (min(cB, ncols) - cA) +
                           (cA > 0 ? column_count(cstart, rlo, rhi, cA - 1, nrows) : 0);
       flag = n > 0;
     }
@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(kPlanThreads)
   const int strip = blockIdx.x;
   const size_t b = (size_t)strip * seg;
   const int J = plan_strip(cstart, G, unit_weight(S, target_units), strip,
-                           ustart + b, upex + b, plan + b);
+                           ustart + b, upex + b, plan + b, kColWeight);
   if (threadIdx.x == 0) strip_n[strip] = J;
 }
 
@@ -1417,7 +1417,8 @@ __global__ void k_b_step_end(const Scn* __restrict__ scn, Scalars* S, int nscn) 
 __global__ void __launch_bounds__(kPlanThreads)
     k_b_units_plan(const int* __restrict__ cstart, const Scn* __restrict__ scn,
                    const Scalars* S, const int* __restrict__ strip_scn,
-                   const Scalars* Sg, int target_units, int* __restrict__ ustart,
+                   const Scalars* Sg, int target_units, int col_weight,
+                   int* __restrict__ ustart,
                    long long* __restrict__ upex, int2* __restrict__ plan,
                    int* __restrict__ strip_n) {
   const int b = blockIdx.x;
@@ -1430,7 +1431,7 @@ __global__ void __launch_bounds__(kPlanThreads)
   const int local = b - scn[s].strip_off;
   const size_t base = (size_t)scn[s].useg_off + (size_t)local * (G.ncols + 1);
   const int J = plan_strip(cstart + scn[s].c_off, G, unit_weight(Sg, target_units),
-                           local, ustart + base, upex + base, plan + base);
+                           local, ustart + base, upex + base, plan + base, col_weight);
   if (threadIdx.x == 0) strip_n[b] = J;
 }
 

@@ -102,6 +102,7 @@ def _declare(lib):
         "dampm_batch_states": (C.c_int, [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]),
         "dampm_batch_last_error": (C.c_char_p, [P]),
+        "dampm_batch_tune": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -61,7 +61,8 @@ class Server:
 
     def __init__(self, budget_bytes: float, max_scenarios: int = 1024, tick: int = 16,
                  node_share: float = 0.45, result_fields: Sequence[str] = ("x", "y", "hp"),
-                 stream: Optional[int] = None, precision: str = "fp64"):
+                 stream: Optional[int] = None, precision: str = "fp64",
+                 graphs: bool = True):
         bpp, bpn = ((BYTES_PER_PARTICLE_F32, BYTES_PER_NODE_F32) if precision == "fp32"
                     else (BYTES_PER_PARTICLE, BYTES_PER_NODE))
         pc = int(budget_bytes * (1.0 - node_share) / bpp)
@@ -73,6 +74,7 @@ class Server:
         self.fields = tuple(result_fields)
         self.b = Batch(self.particle_cap, self.node_cap, max_scenarios, stream=stream,
                        precision=precision)
+        self.b.tune(graphs=graphs)
         self.compactions = 0
         self.ticks = 0
         self.occupancy: List[int] = []

@@ -269,6 +269,7 @@ def run_ensemble(args, world, rank, local):
     b.step(W)
     b.sync()
     # timed region: K passes of every scenario, CUDA events on the batch stream
+    # (with --autotune, the tuner's passes are the first of the K)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -277,7 +278,12 @@ def run_ensemble(args, world, rank, local):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    b.step(K)
+    tuned = None
+    if args.autotune:
+        tuned = b.autotune(passes=8)
+        b.step(K - tuned["passes"])
+    else:
+        b.step(K)
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -327,6 +333,7 @@ def run_ensemble(args, world, rank, local):
                                      f"{K} passes each, device time"},
             "batch_vs_plain": (value / world) / plain_value if plain_value else None,
             "finished": done,
+            "autotune": tuned,
             "roofline": {"bound": "hbm", "kernel": "whole pass", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -361,7 +368,8 @@ def run_serving(args, world, rank, local):
     budget = min(args.budget_gb * 1e9, 0.8 * free)
     stream = torch.cuda.Stream()
     srv = Server(budget, max_scenarios=args.max_scenarios, tick=args.tick,
-                 stream=stream.cuda_stream, precision=args.precision)
+                 stream=stream.cuda_stream, precision=args.precision,
+                 graphs=not args.no_graphs)
     # warm-up: one short request through the same server
     warm = scenarios.serving_request(999999, t_end=0.2)
     srv.run([Request(-1, warm, 0.0)])
@@ -406,7 +414,7 @@ def run_serving(args, world, rank, local):
                                    "logU[64,1024] cells, h=1 m, CFL 0.4 to t=60 s",
                        "requests": n, "rate_per_s": args.rate, "t_end_s": args.t_end,
                        "budget_gb": round(budget / 1e9, 1), "tick_passes": args.tick,
-                       "precision": args.precision,
+                       "precision": args.precision, "cuda_graphs": not args.no_graphs,
                        "parallelism": f"continuous batching; replicas{world}",
                        "l2": "state > 126 MB L2 at full occupancy, no flush"},
             "latency": lat,
@@ -445,6 +453,10 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--max-scenarios", type=int, default=1024)
     ap.add_argument("--tick", type=int, default=16)
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="serving workload: enqueue each pass instead of replaying graphs")
+    ap.add_argument("--autotune", action="store_true",
+                    help="ensemble workload: tune the unit plan during the timed passes")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="ensemble and serving workloads: fp32 runs the FP32 form")
     ap.add_argument("--scenarios", type=int, default=512)

@@ -242,9 +242,20 @@ int dampm_batch_remove(dampm_batch* b, int handle);
 int dampm_batch_compact(dampm_batch* b);
 
 /* Enqueues nsteps passes of every live scenario (asynchronous); a scenario
- * whose loop condition fails does nothing in a pass. */
+ * whose loop condition fails does nothing in a pass.  With two or more
+ * passes they run as one CUDA graph, captured on the batch stream when the
+ * layout or the pass count changed since the last call and replayed
+ * otherwise (see dampm_batch_tune). */
 int dampm_batch_step(dampm_batch* b, int nsteps);
 int dampm_batch_sync(dampm_batch* b);
+
+/* Tuning, for an autotuner: P2G units per CTA of the unit plan and the
+ * weight (in particles) of a column in it, and whether dampm_batch_step
+ * replays its passes as a CUDA graph (captured after each change of layout;
+ * 1 by default).  0 (or -1 for use_graphs) keeps a setting.  None of these
+ * changes any result. */
+int dampm_batch_tune(dampm_batch* b, int units_per_cta, int col_weight,
+                     int use_graphs);
 
 /* Loop state of one scenario (synchronises): iteration, time, last dt,
  * whether its loop condition still holds, particle count. */
