@@ -91,3 +91,20 @@ def test_batch_full_is_an_error(cuda_lib):
         b.add(d)
         with pytest.raises(DampmError):
             b.add(d)
+
+
+@pytest.mark.gpu
+def test_graphs_and_tuning_change_no_result(cuda_lib):
+    ds = mix()[:3]
+    with Batch(200_000, 200_000, 8) as b:
+        hs = [b.add(d) for d in ds]
+        b.tune(units_per_cta=8, col_weight=64, graphs=False)
+        b.step(6)
+        b.tune(units_per_cta=2, col_weight=512, graphs=True)
+        b.step(6)
+        info = b.autotune(passes=2, units=(2, 4), weights=(192,))
+        assert info["units_per_cta"] in (2, 4) and info["passes"] > 0
+        b.sync()
+        total = 12 + info["passes"]
+        for h, d in zip(hs, ds):
+            check_same(b, h, d, total)
