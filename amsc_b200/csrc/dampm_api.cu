@@ -42,6 +42,7 @@ struct dampm_ctx {
   int4* ulist = nullptr;
   int *clist = nullptr, *clist_n = nullptr;  // cells with >= 2 particles
   int* cbig = nullptr;  // cells with more than 256 particles (capacity / 256)
+  double* ledger_log = nullptr;  // kLedgerLog rows {t, err_mass, err_mom}
   int p2g_grid = 0;
   Scalars* S = nullptr;
   Scalars* Sh = nullptr;  // pinned host mirror
@@ -228,7 +229,8 @@ int enqueue_pass(dampm_ctx* ctx) {
       ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount);
   ctx->launches += 2;
   ev_mark(ctx, 3);
-  k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S);
+  k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S,
+                                               ctx->ledger_log);
   ev_mark(ctx, 2);
   k_g2p<<<grid_for(ctx->cap, kG2PThreads), kG2PThreads, 0, ctx->stream>>>(
       ctx->p, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
@@ -353,6 +355,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   rc = rc ? rc : dalloc(ctx, &ctx->ulist, size_t(ctx->n_led));
   rc = rc ? rc : dalloc(ctx, &ctx->strip_n, size_t(ctx->strips));
   rc = rc ? rc : dalloc(ctx, &ctx->ucount, 2);
+  rc = rc ? rc : dalloc(ctx, &ctx->ledger_log, size_t(kLedgerLog) * 3);
   rc = rc ? rc : dalloc(ctx, &ctx->S, 1);
   if (rc == DAMPM_OK) {
     if (cudaMallocHost(&ctx->Sh, sizeof(Scalars)) != cudaSuccess) rc = DAMPM_ERR_CUDA;
@@ -653,6 +656,24 @@ int dampm_download_nodal(dampm_ctx* ctx, const char* field, double* out) {
   CK(cudaMemcpyAsync(out, src, sizeof(double) * ctx->nn, cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+int dampm_ledger_history(dampm_ctx* ctx, long long first_it, int n, double* out) {
+  if (!ctx || !out || n < 0 || first_it < 1 || n > kLedgerLog) return DAMPM_ERR_ARG;
+  int rc = sync_status(ctx);
+  if (rc) return rc;
+  const long long last = ctx->Sh->it;
+  if (first_it + n - 1 > last || last - first_it >= kLedgerLog)
+    return fail(ctx, DAMPM_ERR_ARG, "ledger rows outside the last 1024 steps");
+  std::vector<double> all(size_t(kLedgerLog) * 3);
+  CK(cudaMemcpyAsync(all.data(), ctx->ledger_log, sizeof(double) * all.size(),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < n; ++k) {
+    const double* row = all.data() + 3 * ((first_it + k - 1) % kLedgerLog);
+    for (int q = 0; q < 3; ++q) out[3 * k + q] = row[q];
+  }
   return DAMPM_OK;
 }
 

@@ -107,8 +107,9 @@ __global__ void k_p2g(Particles p, const int* perm, const int* cstart,
                       Nodes nodes, double* led_part, Geom G, Phys P,
                       const Scalars* S, int record, const int4* ulist,
                       const int* ucount);
+constexpr int kLedgerLog = 1024;  // rows of the per-step ledger log
 __global__ void k_ledger_final(const double* led_part, const int* ucount,
-                               Scalars* S);
+                               Scalars* S, double* log);
 __global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
                       Phys P, Scalars* S, int record, int want_grad);
 

@@ -1179,10 +1179,18 @@ __device__ __forceinline__ void ledger_reduce(const double* __restrict__ led_par
   }
 }
 
+// log: a ring of kLedgerLog rows {t, err_mass, err_mom}, row (it-1) % kLedgerLog
 __global__ void k_ledger_final(const double* __restrict__ led_part,
-                               const int* __restrict__ ucount, Scalars* S) {
+                               const int* __restrict__ ucount, Scalars* S,
+                               double* __restrict__ log) {
   if (!S->active) return;
   ledger_reduce(led_part, 0, ucount[0], S);
+  if (threadIdx.x == 0 && log) {
+    double* row = log + 3 * ((S->it - 1) % kLedgerLog);
+    row[0] = S->ledger[8];
+    row[1] = S->ledger[6];
+    row[2] = S->ledger[7];
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -79,6 +79,7 @@ def _declare(lib):
         "dampm_download_nodal": (C.c_int, [P, C.c_char_p, _DP]),
         "dampm_record_outputs": (C.c_int, [P, C.c_int]),
         "dampm_ledgers": (C.c_int, [P, _DP]),
+        "dampm_ledger_history": (C.c_int, [P, C.c_longlong, C.c_int, _DP]),
         "dampm_set_state": (C.c_int, [P, C.c_longlong, C.POINTER(_DP)] + [_DP] * 5),
         "dampm_get_state": (C.c_int, [P, C.POINTER(_DP)]),
         "dampm_last_launch_count": (C.c_longlong, [P]),
@@ -251,6 +252,12 @@ class Solver:
 
     def fields(self, names: Iterable[str]) -> Dict[str, np.ndarray]:
         return {k: self.download(k) for k in names}
+
+    def ledger_history(self, first_it: int, n: int) -> np.ndarray:
+        """Rows {t, err_mass, err_mom} of steps first_it .. first_it+n-1."""
+        out = np.empty((n, 3), dtype=np.float64)
+        self._check(self.lib.dampm_ledger_history(self.h, int(first_it), int(n), _ptr(out)))
+        return out
 
     def ledgers(self) -> np.ndarray:
         out = np.empty(9, dtype=np.float64)

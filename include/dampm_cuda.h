@@ -158,6 +158,11 @@ int dampm_record_outputs(dampm_ctx* ctx, int enable);
  *  err_mass, err_mom, t}. */
 int dampm_ledgers(dampm_ctx* ctx, double out[9]);
 
+/* The conservation_errors.csv rows of steps first_it .. first_it+n-1 (step
+ * numbers from 1; any of the last 1024 steps; synchronises): n rows of
+ * {t at the step's start, err_mass, err_mom} (main/optim_par.cpp:395-428). */
+int dampm_ledger_history(dampm_ctx* ctx, long long first_it, int n, double* out);
+
 /* Overwrites / reads the whole persistent particle state (checkpoint and
  * host round trip).  Arrays in reference index order, np values each:
  * x, y, vpx, vpy, hp, F_11, F_12, F_22, Mp, Vp, H.  set_state marks the
