@@ -351,6 +351,62 @@ def run_ensemble(args, world, rank, local):
     return 0
 
 
+def run_mudflow_fp32(args, world, rank, local):
+    """The mudflow in the FP32 form: a batch holding the one scenario."""
+    import torch
+    torch.cuda.set_device(local)
+    from amsc_b200 import scenarios
+    from amsc_b200.batch import Batch
+    d = scenarios.mudflow(N=2048, seed=12345 + rank)
+    stream = torch.cuda.Stream()
+    b = Batch(d.np + 1024, d.nnodes + 1024, 2, stream=stream.cuda_stream, precision="fp32")
+    h = b.add(d)
+    b.step(args.warmup)
+    b.sync()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = b.usage()["launches"]
+    _barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    el_ms = _allreduce(e0.elapsed_time(e1), world)
+    launches = b.usage()["launches"] - l0
+    q = b.query(h)
+    total = _allreduce(float(d.np), world, "sum")
+    value = total * args.steps / (el_ms * 1e-3)
+    peak, peak_kind = _peaks()
+    # FP32 algorithmic bytes of a pass: sort ~28 B, P2G 56 B (13 x 4 B record
+    # + index), G2P 96 B per particle
+    per_pass = 180.0 * d.np
+    achieved = per_pass / (el_ms / args.steps * 1e-3) / 1e9
+    b.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD + ", FP32 form (a batch of one scenario)",
+                       "particles": d.np, "grid": "2048x2048", "precision": "fp32",
+                       "parallelism": f"replicas{world}",
+                       "l2": "state 181 MB > 126 MB L2, no flush", "seed": 12345},
+            "roofline": {"bound": "hbm", "kernel": "whole pass", "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes_per_launch": per_pass},
+            "e2e": None, "gpu_launches": int(launches), "clocks": clocks,
+            "cpu_baseline": None, "state": {"it": q["it"], "t": q["t"], "dt": q["dt"]},
+        }), flush=True)
+    _barrier(world)
+    return 0
+
+
 def run_serving(args, world, rank, local):
     """--workload serving: requests arriving as a Poisson stream, served by
     continuous batching; scenarios/s and time-to-result percentiles."""
@@ -453,12 +509,14 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--max-scenarios", type=int, default=1024)
     ap.add_argument("--tick", type=int, default=16)
+    ap.add_argument("--merge-split", action="store_true",
+                    help="mudflow workload: merge/split every 10 steps")
     ap.add_argument("--no-graphs", action="store_true",
                     help="serving workload: enqueue each pass instead of replaying graphs")
     ap.add_argument("--autotune", action="store_true",
                     help="ensemble workload: tune the unit plan during the timed passes")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
-                    help="ensemble and serving workloads: fp32 runs the FP32 form")
+                    help="fp32 runs the FP32 form (mudflow: as a batch of one)")
     ap.add_argument("--scenarios", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -497,9 +555,11 @@ def main():
     from amsc_b200 import scenarios
     from amsc_b200.dampm import STATE_FIELDS, Solver
 
-    d = scenarios.mudflow(N=2048, seed=12345 + rank)
+    if args.precision == "fp32":
+        return run_mudflow_fp32(args, world, rank, local)
+    d = scenarios.mudflow(N=2048, seed=12345 + rank, merge_split=args.merge_split)
     np_ = d.np
-    s = Solver(d)
+    s = Solver(d, merge_split=args.merge_split)
     # warm-up
     s.step(args.warmup)
     s.sync()
@@ -578,7 +638,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": np_, "grid": "2048x2048",
+            "config": {"workload": WORKLOAD + (", merge/split every 10 steps"
+                                               if args.merge_split else ""),
+                       "particles": np_, "particles_end": st["np"], "grid": "2048x2048",
                        "precision": "fp64", "parallelism": f"replicas{world}",
                        "l2": "state 354 MB > 126 MB L2, no flush",
                        "seed": 12345},
