@@ -27,6 +27,10 @@ constexpr int kP2GThreads = 128;
 constexpr int kCap = 512;
 constexpr int kP2GMinBlocks = 4;
 constexpr int kG2PThreads = 256;
+#ifndef DAMPM_G2P_MIN_BLOCKS
+#define DAMPM_G2P_MIN_BLOCKS 4
+#endif
+constexpr int kG2PMinBlocks = DAMPM_G2P_MIN_BLOCKS;
 constexpr int kScanTile = 4096;
 constexpr int kScanThreads = 1024;
 

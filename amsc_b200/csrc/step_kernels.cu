@@ -1356,7 +1356,7 @@ __device__ __forceinline__ void cfl_block_max(unsigned long long m0,
   }
 }
 
-__global__ void __launch_bounds__(kG2PThreads, 3)
+__global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
     k_g2p(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
           Phys P, Scalars* S, int record, int want_grad) {
   if (!S->active) return;
@@ -1531,7 +1531,7 @@ __global__ void k_b_ledger(const double* __restrict__ led_part,
 
 // gblk[b] = {scenario, its first particle handled by block b}
 template <class R>
-__global__ void __launch_bounds__(kG2PThreads, 3)
+__global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
     k_b_g2p(ParticlesT<R> p, const R* __restrict__ vvxL,
             const R* __restrict__ vvyL, const double* __restrict__ Z,
             const Scn* __restrict__ scn, Scalars* S, const int2* __restrict__ gblk,
