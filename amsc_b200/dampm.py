@@ -104,6 +104,12 @@ def _declare(lib):
                                          C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]),
         "dampm_batch_last_error": (C.c_char_p, [P]),
         "dampm_batch_tune": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
+        "dampm_json_read": (C.c_int, [C.c_char_p, C.POINTER(P)]),
+        "dampm_json_size": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_longlong)]),
+        "dampm_json_kind": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_int)]),
+        "dampm_json_get": (C.c_int, [P, C.c_char_p, _DP]),
+        "dampm_json_error": (C.c_char_p, [P]),
+        "dampm_json_free": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

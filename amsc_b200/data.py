@@ -113,9 +113,34 @@ def from_dict(j: dict) -> DATA:
 
 
 def from_json(path: str) -> DATA:
-    """``DATA::DATA(const char*)`` (main/mpm_data.h:116-122)."""
-    with open(path, "r") as f:
-        return from_dict(json.load(f))
+    """``DATA::DATA(const char*)`` (main/mpm_data.h:116-122), through the
+    library's streaming reader (dampm_json_read): each number is parsed
+    straight into a float64 array, so DATA.json files of a gigabyte load
+    without per-number Python objects."""
+    import ctypes as C
+    from .dampm import DampmError, load_library
+    lib = load_library()
+    h = C.c_void_p()
+    rc = lib.dampm_json_read(path.encode(), C.byref(h))
+    try:
+        if rc != 0:
+            msg = lib.dampm_json_error(h).decode() if h else f"cannot open {path}"
+            raise DampmError(f"DATA: {msg}")
+        j = {}
+        for k in PARTICLE_KEYS + NODE_KEYS + tuple(REQUIRED_SCALARS) + tuple(OPTIONAL_DEFAULTS):
+            n = C.c_longlong()
+            lib.dampm_json_size(h, k.encode(), C.byref(n))
+            if n.value < 0:
+                continue
+            a = np.empty(max(n.value, 1), dtype=np.float64)
+            lib.dampm_json_get(h, k.encode(), a.ctypes.data_as(C.POINTER(C.c_double)))
+            kind = C.c_int()
+            lib.dampm_json_kind(h, k.encode(), C.byref(kind))
+            j[k] = a[:n.value] if kind.value else float(a[0])
+    finally:
+        if h:
+            lib.dampm_json_free(h)
+    return from_dict(j)
 
 
 def _fmt(v) -> str:

@@ -186,6 +186,23 @@ int dampm_last_timings(dampm_ctx* ctx, int enable_events, double out[5]);
 const char* dampm_last_error(dampm_ctx* ctx);
 const char* dampm_version(void);
 
+/* ---- DATA.json at scale ----------------------------------------------------
+ * Replaces DATA::DATA(const char*) (main/mpm_data.h:61-122, nlohmann::json)
+ * for large files: the file is streamed and each number parsed straight into
+ * a double array (std::from_chars: the same rounding as strtod), so a
+ * 1 GB DATA.json needs no per-number objects.  Values are numbers or
+ * (nested, flattened) arrays of numbers; anything else is an error whose
+ * message dampm_json_error gives (free the handle afterwards). */
+typedef struct dampm_json dampm_json;
+int dampm_json_read(const char* path, dampm_json** out);
+/* *n = number of values (a scalar counts 1), or -1 when the key is absent */
+int dampm_json_size(const dampm_json* j, const char* key, long long* n);
+/* *is_array = 1 for an array value, 0 for a scalar */
+int dampm_json_kind(const dampm_json* j, const char* key, int* is_array);
+int dampm_json_get(const dampm_json* j, const char* key, double* out);
+const char* dampm_json_error(const dampm_json* j);
+int dampm_json_free(dampm_json* j);
+
 /* CFL time step from particle arrays held by the caller on the current
  * device, computed on the device without allocating any device memory.
  * No counterpart in the reference: its GPU driver copies vpx, vpy and hp to
