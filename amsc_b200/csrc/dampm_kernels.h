@@ -167,7 +167,6 @@ __global__ void k_b_move_nodes(double* dst, const double* src, const int4* nblk)
 __global__ void k_hv(const Particles p, const int* perm, const int* cstart,
                      double* HV, Geom G, const Scalars* S);
 
-size_t p2g_smem_bytes();       // FP64 P2G staging
-size_t p2g_smem_bytes_f32();   // FP32 P2G staging
+size_t p2g_smem_bytes();  // FP64 P2G staging (the single-scenario path)
 
 }  // namespace dampm

@@ -1374,7 +1374,6 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
 }
 
 size_t p2g_smem_bytes() { return sizeof(P2GSmemT<double>); }
-size_t p2g_smem_bytes_f32() { return sizeof(P2GSmemT<float>); }
 
 __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b,
                          long long n) {
