@@ -121,10 +121,14 @@ const int* keys_of(dampm_batch* b) {
 // the persistent per-particle arrays of one half of the double buffer
 template <class R>
 int alloc_particles(dampm_batch* b, ParticlesT<R>& p) {
-  R** f[] = {&p.x,   &p.y,   &p.vpx, &p.vpy, &p.hp,  &p.F11, &p.F12, &p.F22,
-             &p.Mp,  &p.Vp,  &p.H,   &p.mpx, &p.mpy, &p.qfx, &p.qfy, &p.qxi,
-             &p.qeta, &p.qgx, &p.qgy, &p.Ap,  &p.Fbx, &p.Fby};
+  R** f[] = {&p.x,  &p.y,  &p.vpx, &p.vpy, &p.hp, &p.F11, &p.F12,
+             &p.F22, &p.Mp, &p.Vp,  &p.H,   &p.Ap, &p.Fbx, &p.Fby};
   for (R** q : f) {
+    int rc = balloc(b, q, size_t(b->P_cap));
+    if (rc) return rc;
+  }
+  V2<R>** f2[] = {&p.mp, &p.qf, &p.xe, &p.qg};
+  for (V2<R>** q : f2) {
     int rc = balloc(b, q, size_t(b->P_cap));
     if (rc) return rc;
   }
@@ -139,10 +143,12 @@ int alloc_particles(dampm_batch* b, ParticlesT<R>& p) {
 template <class R>
 ParticlesT<R> shifted(const ParticlesT<R>& p, long long off) {
   ParticlesT<R> q = p;
-  R** f[] = {&q.x,   &q.y,   &q.vpx, &q.vpy, &q.hp,  &q.F11, &q.F12, &q.F22,
-             &q.Mp,  &q.Vp,  &q.H,   &q.mpx, &q.mpy, &q.qfx, &q.qfy, &q.qxi,
-             &q.qeta, &q.qgx, &q.qgy, &q.Ap,  &q.Fbx, &q.Fby};
+  R** f[] = {&q.x,  &q.y,  &q.vpx, &q.vpy, &q.hp, &q.F11, &q.F12,
+             &q.F22, &q.Mp, &q.Vp,  &q.H,   &q.Ap, &q.Fbx, &q.Fby};
   for (R** d : f)
+    if (*d) *d += off;
+  V2<R>** f2[] = {&q.mp, &q.qf, &q.xe, &q.qg};
+  for (V2<R>** d : f2)
     if (*d) *d += off;
   int** fi[] = {&q.label, &q.level, &q.key};
   for (int** d : fi)
@@ -253,20 +259,23 @@ template <class R>
 int upload_scenario(dampm_batch* b, const Scn& d, int pos, long long np,
                     const double* const* in, double* Zs) {
   ParticlesT<R> p = shifted(halves<R>(b)[b->cur], d.p_off);
-  R* dst[10] = {p.x, p.y, p.Mp, p.Ap, p.vpx, p.vpy, p.hp, p.mpx, p.mpy, p.Vp};
+  // in: x, y, Mp, Ap, vpx, vpy, hp, mom_px, mom_py, Vp
+  R* dst[10] = {p.x, p.y, p.Mp, p.Ap, p.vpx, p.vpy, p.hp, nullptr, nullptr, p.Vp};
   cudaStream_t st = b->stream;
-  std::vector<R> tmp;
+  std::vector<R> tmp, tmp2;
+  auto host_r = [&](int k, std::vector<R>& t) -> const R* {
+    if (sizeof(R) == sizeof(double)) return reinterpret_cast<const R*>(in[k]);
+    t.assign(in[k], in[k] + np);
+    return t.data();
+  };
   for (int k = 0; k < 10; ++k) {
-    const R* src;
-    if (sizeof(R) == sizeof(double)) {
-      src = reinterpret_cast<const R*>(in[k]);
-    } else {
-      tmp.assign(in[k], in[k] + np);
-      src = tmp.data();
-    }
-    BCK(cudaMemcpyAsync(dst[k], src, sizeof(R) * size_t(np), cudaMemcpyHostToDevice, st));
+    if (!dst[k]) continue;
+    BCK(cudaMemcpyAsync(dst[k], host_r(k, tmp), sizeof(R) * size_t(np),
+                        cudaMemcpyHostToDevice, st));
     if (sizeof(R) != sizeof(double)) BCK(cudaStreamSynchronize(st));  // tmp is reused
   }
+  BCK(upload_pair(p.mp, host_r(7, tmp), host_r(8, tmp2), np, st));
+  BCK(cudaStreamSynchronize(st));
   // (the terrain gradients only feed recorded outputs, which a batch does
   // not keep, so Z stands in for them)
   launch_init_particles<R>(grid_blocks(np, 256), 256, st, p, Zs, Zs, Zs, d.G, d.P,
@@ -281,6 +290,7 @@ template <class R>
 int download_field(dampm_batch* b, const Scn& d, const std::string& f, double* out) {
   const ParticlesT<R> p = shifted(halves<R>(b)[b->cur], d.p_off);
   const R* src = nullptr;
+  int pair_half = -1;  // mom_px / mom_py: one half of the momentum pair
   if (f == "x") src = p.x;
   else if (f == "y") src = p.y;
   else if (f == "vpx") src = p.vpx;
@@ -292,20 +302,23 @@ int download_field(dampm_batch* b, const Scn& d, const std::string& f, double* o
   else if (f == "Mp") src = p.Mp;
   else if (f == "Vp") src = p.Vp;
   else if (f == "H") src = p.H;
-  else if (f == "mom_px") src = p.mpx;
-  else if (f == "mom_py") src = p.mpy;
-  if (!src) return bfail(b, DAMPM_ERR_UNKNOWN_FIELD, "unknown batch field " + f);
-  if (sizeof(R) == sizeof(double)) {
-    BCK(cudaMemcpyAsync(out, src, sizeof(double) * size_t(d.np), cudaMemcpyDeviceToHost,
-                        b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-  } else {
-    std::vector<R> tmp(size_t(d.np));
-    BCK(cudaMemcpyAsync(tmp.data(), src, sizeof(R) * size_t(d.np), cudaMemcpyDeviceToHost,
-                        b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-    for (int i = 0; i < d.np; ++i) out[i] = double(tmp[i]);
+  else if (f == "mom_px" || f == "mom_py") pair_half = f == "mom_px" ? 0 : 1;
+  if (!src && pair_half < 0)
+    return bfail(b, DAMPM_ERR_UNKNOWN_FIELD, "unknown batch field " + f);
+  R* hout = reinterpret_cast<R*>(out);
+  std::vector<R> tmp;
+  if (sizeof(R) != sizeof(double)) {
+    tmp.resize(size_t(d.np));
+    hout = tmp.data();
   }
+  if (pair_half >= 0)
+    BCK(download_pair_half(hout, p.mp, pair_half, d.np, b->stream));
+  else
+    BCK(cudaMemcpyAsync(hout, src, sizeof(R) * size_t(d.np), cudaMemcpyDeviceToHost,
+                        b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  if (sizeof(R) != sizeof(double))
+    for (int i = 0; i < d.np; ++i) out[i] = double(tmp[i]);
   return DAMPM_OK;
 }
 

@@ -139,16 +139,20 @@ int alloc_record(dampm_ctx* ctx) {
 int alloc_particles(dampm_ctx* ctx, long long cap) {
   ctx->cap = cap;
   Particles& p = ctx->p;
-  double** f[] = {&p.x,     &p.y,     &p.vpx,    &p.vpy,    &p.hp,
-                  &p.F11,   &p.F12,   &p.F22,    &p.Mp,     &p.Vp,
-                  &p.H,     &p.Ap,    &p.mpx,    &p.mpy,    &p.Fbx,
-                  &p.Fby,   &p.vpx_dx, &p.vpx_dy, &p.vpy_dx, &p.vpy_dy,
-                  &p.xp,    &p.yp,    &p.qfx,    &p.qfy,    &p.qxi,
-                  &p.qeta,  &p.qgx,   &p.qgy};
+  double** f[] = {&p.x,     &p.y,      &p.vpx,    &p.vpy,    &p.hp,
+                  &p.F11,   &p.F12,    &p.F22,    &p.Mp,     &p.Vp,
+                  &p.H,     &p.Ap,     &p.Fbx,    &p.Fby,    &p.vpx_dx,
+                  &p.vpx_dy, &p.vpy_dx, &p.vpy_dy, &p.xp,     &p.yp};
   for (double** q : f) {
     int rc = dalloc(ctx, q, cap);
     if (rc) return rc;
     CK(cudaMemsetAsync(*q, 0, cap * sizeof(double), ctx->stream));
+  }
+  double2** f2[] = {&p.mp, &p.qf, &p.xe, &p.qg};
+  for (double2** q : f2) {
+    int rc = dalloc(ctx, q, cap);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(*q, 0, cap * sizeof(double2), ctx->stream));
   }
   int** fi[] = {&p.label, &p.level, &p.key, &ctx->slot, &ctx->perm};
   for (int** q : fi) {
@@ -439,8 +443,7 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
     CK(cudaMemcpyAsync(p.vpx, vpx, b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(p.vpy, vpy, b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(p.hp, hp, b, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(p.mpx, mom_px, b, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(p.mpy, mom_py, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(upload_pair(p.mp, mom_px, mom_py, np, ctx->stream));
     CK(cudaMemcpyAsync(p.Vp, Vp, b, cudaMemcpyHostToDevice, ctx->stream));
   }
   Scalars s0{};
@@ -570,6 +573,7 @@ int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
   const double* src = nullptr;
   const int* isrc = nullptr;
   int derived = -1;
+  int pair_half = -1;  // mom_px / mom_py: one half of the momentum pair
   if (f == "x") src = p.x;
   else if (f == "y") src = p.y;
   else if (f == "Mp") src = p.Mp;
@@ -590,8 +594,7 @@ int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
   else if (f == "label") isrc = p.label;
   else if (f == "level") isrc = p.level;
   else if (f == "Ap") { if (fresh) src = p.Ap; else derived = 0; }
-  else if (f == "mom_px") src = p.mpx;
-  else if (f == "mom_py") src = p.mpy;
+  else if (f == "mom_px" || f == "mom_py") pair_half = f == "mom_px" ? 0 : 1;
   else if (f == "Fb_x") { if (fresh) src = p.Fbx; else derived = 3; }
   else if (f == "Fb_y") { if (fresh) src = p.Fby; else derived = 4; }
   else if (ctx->record_alloc) {
@@ -606,9 +609,14 @@ int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
     else if (f == "Fric_px") src = p.Frx;
     else if (f == "Fric_py") src = p.Fry;
   }
-  if (!src && !isrc && derived < 0)
+  if (!src && !isrc && derived < 0 && pair_half < 0)
     return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown particle field " + f);
   if (np == 0) return DAMPM_OK;
+  if (pair_half >= 0) {
+    CK(download_pair_half(out, p.mp, pair_half, np, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DAMPM_OK;
+  }
   if (isrc || derived >= 0) {
     // reuse the merge/split scratch as a staging buffer
     double* tmp = ctx->msb.stage;
@@ -702,8 +710,7 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
   const bool fresh = Ap && mom_px && mom_py && Fb_x && Fb_y;
   if (fresh) {
     CK(cudaMemcpyAsync(p.Ap, Ap, b, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(p.mpx, mom_px, b, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(p.mpy, mom_py, b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(upload_pair(p.mp, mom_px, mom_py, np, ctx->stream));
     CK(cudaMemcpyAsync(p.Fbx, Fb_x, b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(p.Fby, Fb_y, b, cudaMemcpyHostToDevice, ctx->stream));
   }

@@ -34,6 +34,20 @@ constexpr int kG2PMinBlocks = DAMPM_G2P_MIN_BLOCKS;
 constexpr int kScanTile = 4096;
 constexpr int kScanThreads = 1024;
 
+// Two values of R side by side (one 16-byte load in FP64, 8 in FP32).
+template <class R>
+struct Vec2T;
+template <>
+struct Vec2T<double> {
+  using type = double2;
+};
+template <>
+struct Vec2T<float> {
+  using type = float2;
+};
+template <class R>
+using V2 = typename Vec2T<R>::type;
+
 // Particle SoA in reference index order; R = double is the FP64 path,
 // R = float the FP32 form (batches).
 template <class R>
@@ -42,14 +56,15 @@ struct ParticlesT {
   R *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
   int *label, *level, *key;
   // the record the next P2G transfers, written by G2P (or by k_prep after an
-  // upload, a state upload or a merge/split):
-  //   mpx, mpy  momentum v*Mp and qfx, qfy friction force Ap*Fb, as the
-  //             reference stores them at the end of a step
-  //             (main/optim_par.cpp:456-459,600-626);
-  //   qxi, qeta local coordinates in the cell of the next binning;
-  //   qgx, qgy  gravity force -g*Vp*rho*grad(Z)*(1 - H/hp) there
-  //             (main/optim_par.cpp:387,447-454).
-  R *mpx, *mpy, *qfx, *qfy, *qxi, *qeta, *qgx, *qgy;
+  // upload, a state upload or a merge/split), as pairs that P2G gathers
+  // with one copy each:
+  //   mp = (mom_px, mom_py)  momentum v*Mp, and qf = (Ap*Fb_x, Ap*Fb_y) the
+  //        friction force, as the reference stores them at the end of a
+  //        step (main/optim_par.cpp:456-459,600-626);
+  //   xe = (xi, eta)  local coordinates in the cell of the next binning;
+  //   qg = gravity force -g*Vp*rho*grad(Z)*(1 - H/hp) there
+  //        (main/optim_par.cpp:387,447-454).
+  V2<R> *mp, *qf, *xe, *qg;
   // Ap and Fb as stored at upload / merge/split (valid while Scalars::fresh
   // is set; otherwise they are derived from the state)
   R *Ap, *Fbx, *Fby;

@@ -44,6 +44,28 @@ inline Phys make_phys(const dampm_params& d) {
   return P;
 }
 
+// Host halves (a, b) of n pairs into a pair array: two strided copies.
+template <class T, class V>
+cudaError_t upload_pair(V* dst, const T* a, const T* b, long long n, cudaStream_t st) {
+  static_assert(sizeof(V) == 2 * sizeof(T), "pair of T");
+  if (n <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemcpy2DAsync(dst, sizeof(V), a, sizeof(T), sizeof(T), size_t(n),
+                                    cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy2DAsync(reinterpret_cast<T*>(dst) + 1, sizeof(V), b, sizeof(T),
+                           sizeof(T), size_t(n), cudaMemcpyHostToDevice, st);
+}
+
+// Half `half` (0: first, 1: second) of n pairs to the host.
+template <class T, class V>
+cudaError_t download_pair_half(T* out, const V* src, int half, long long n,
+                               cudaStream_t st) {
+  static_assert(sizeof(V) == 2 * sizeof(T), "pair of T");
+  if (n <= 0) return cudaSuccess;
+  return cudaMemcpy2DAsync(out, sizeof(T), reinterpret_cast<const T*>(src) + half, sizeof(V),
+                           sizeof(T), size_t(n), cudaMemcpyDeviceToHost, st);
+}
+
 inline int grid_blocks(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;

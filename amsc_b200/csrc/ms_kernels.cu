@@ -32,20 +32,38 @@ struct MsCfg {
   int use_step_dt;
 };
 
-__global__ void k_ms_materialize(Particles p, Phys P, const Scalars* S) {
-  if (!S->active || S->fresh) return;
+__global__ void k_ms_materialize(Particles p, Phys P, const Scalars* S,
+                                 double* __restrict__ mx, double* __restrict__ my) {
+  if (!S->active) return;
+  const bool fresh = S->fresh != 0;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
+    if (fresh) {  // uploaded Ap, momentum and Fb stand as they are
+      const double2 m = p.mp[i];
+      mx[i] = m.x;
+      my[i] = m.y;
+      continue;
+    }
     const double hp = p.hp[i];
     p.Ap[i] = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
-    p.mpx[i] = p.vpx[i] * p.Mp[i];
-    p.mpy[i] = p.vpy[i] * p.Mp[i];
+    mx[i] = p.vpx[i] * p.Mp[i];
+    my[i] = p.vpy[i] * p.Mp[i];
     double fx, fy;
     voellmy(P, p.vpx[i], p.vpy[i], hp, fx, fy);
     p.Fbx[i] = fx;
     p.Fby[i] = fy;
   }
+}
+
+// the momentum of the particles after the emit, back into its pair
+__global__ void k_ms_pair_mom(const double* __restrict__ mx, const double* __restrict__ my,
+                              Particles p, const Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x)
+    p.mp[i] = make_double2(mx[i], my[i]);
 }
 
 __global__ void k_ms_mark(Particles p, Geom G, MsCfg c, int* act, int cap,
@@ -421,7 +439,7 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   const int gp = grid_for(cap, 256);
   const int ic = int(cap);
   k_ms_reset_counts<<<1, 1, 0, st>>>(S);
-  k_ms_materialize<<<gp, 256, 0, st>>>(p, P, S);
+  k_ms_materialize<<<gp, 256, 0, st>>>(p, P, S, m.mx, m.my);
   n += 2;
   k_ms_mark<<<gp, 256, 0, st>>>(p, G, c, m.act, ic, S);
   k_ms_init_partner<<<gp, 256, 0, st>>>(m.partner, ic, S);
@@ -440,7 +458,7 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   Fields in{}, out{};
   double* pf[kMsFields] = {p.x,   p.y,   p.vpx, p.vpy, p.hp,     p.F11,
                            p.F12, p.F22, p.Mp,  p.Vp,  p.H,      p.Ap,
-                           p.mpx, p.mpy, p.Fbx, p.Fby, p.vpx_dx, p.vpx_dy,
+                           m.mx,  m.my,  p.Fbx, p.Fby, p.vpx_dx, p.vpx_dy,
                            p.vpy_dx, p.vpy_dy, p.xp, p.yp};
   for (int k = 0; k < kMsFields; ++k) {
     in.f[k] = pf[k];
@@ -453,8 +471,9 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
   k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
+  k_ms_pair_mom<<<gp, 256, 0, st>>>(m.mx, m.my, p, S);
   launch_prep<double>(gp, 256, st, p, Z, G, P, S, 0);
-  n += 4;
+  n += 5;
   return n;
 }
 

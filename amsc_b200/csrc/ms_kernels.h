@@ -18,6 +18,7 @@ struct MsBuffers {
   long long cap = 0;
   double* stage = nullptr;  // one field of scratch (also a download staging area)
   double* sd[kMsFields] = {};
+  double *mx = nullptr, *my = nullptr;  // the momentum pair as two fields
   int *slabel = nullptr, *slevel = nullptr;
 };
 
@@ -39,6 +40,10 @@ int ms_alloc(MsBuffers& m, long long cap, int /*ncells*/, Alloc alloc) {
     rc = alloc((void**)&m.sd[k], sizeof(double) * size_t(cap));
     if (rc) return rc;
   }
+  rc = alloc((void**)&m.mx, sizeof(double) * size_t(cap));
+  if (rc) return rc;
+  rc = alloc((void**)&m.my, sizeof(double) * size_t(cap));
+  if (rc) return rc;
   return 0;
 }
 

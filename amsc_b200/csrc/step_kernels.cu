@@ -215,21 +215,17 @@ __global__ void k_prep(ParticlesT<R> p, const double* __restrict__ Z, Geom G,
     if (derive) {
       Ap = hp > R(1.e-2) ? p.Vp[i] / hp : R(0);
       voellmy<R>(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
-      p.mpx[i] = p.vpx[i] * p.Mp[i];
-      p.mpy[i] = p.vpy[i] * p.Mp[i];
+      p.mp[i] = V2<R>{p.vpx[i] * p.Mp[i], p.vpy[i] * p.Mp[i]};
     } else {
       Ap = p.Ap[i];
       fbx = p.Fbx[i];
       fby = p.Fby[i];
     }
-    p.qfx[i] = Ap * fbx;
-    p.qfy[i] = Ap * fby;
+    p.qf[i] = V2<R>{Ap * fbx, Ap * fby};
     R xi, eta, gx, gy;
     next_record<R>(G, P, Z, p.x[i], p.y[i], hp, p.H[i], p.Vp[i], xi, eta, gx, gy);
-    p.qxi[i] = xi;
-    p.qeta[i] = eta;
-    p.qgx[i] = gx;
-    p.qgy[i] = gy;
+    p.xe[i] = V2<R>{xi, eta};
+    p.qg[i] = V2<R>{gx, gy};
   }
 }
 
@@ -524,50 +520,60 @@ __global__ void __launch_bounds__(1024)
 // of cells (rlo..rhi, cc) are one contiguous range of the sorted order,
 // processed in batches of at most kCap particles.  Each particle's record
 // (local coordinates and the nine transferred quantities, built by the
-// previous step's G2P) is copied with cp.async into shared memory; the sorted
-// indices of the next batch are loaded while the copies fly.  Four CTAs share
-// an SM, so one CTA's copies overlap the others' transfers.
+// previous step's G2P) is copied with cp.async into shared memory: the four
+// record pairs (xi, eta), (mom_x, mom_y), gravity and friction force with
+// one 16-byte copy each, Mp, F11, F12, F22 and Vp with one 8-byte copy each.
+// The sorted indices of the next batch are loaded while the copies fly.
+// Four CTAs share an SM, so one CTA's copies overlap the others' transfers.
 //
 // Node row r is served by lane r of four warps, one per quantity group
-// (warp-uniform code) g0 {Mv, mom_x, mom_y}, g1 {FPx, FPy, Fric_x},
-// g2 {Fric_y, Fint_x}, g3 {Fint_y}; each lane carries two chains per
-// quantity:
+// (warp-uniform code) g0 {Mv, mom_x, mom_y}, g1 {FPx, FPy, Fric_x, Fric_y},
+// g2 {Fint_x}, g3 {Fint_y}; each lane carries two chains per quantity:
 //   fin   node (r, cc)   -- local node 1 of cell (r-1,cc), then 0 of (r,cc);
 //         it already holds cells (r-1,cc-1), (r,cc-1);
 //   start node (r, cc+1) -- local node 3 of cell (r-1,cc), then 2 of (r,cc).
 // That is each node's contributions in quadgrid's cell-sweep order, so every
 // nodal sum equals the reference's sequential sum bit for bit.  At the end of
-// a column the finished sums go through shared memory to warp 0, which
-// applies the nodal update to node column cc, and each lane's started chains
-// become its finishing ones.  Records are stored SoA with an XOR swizzle of
-// the low four index bits so that lanes of consecutive rows (records ~ppc
-// apart) hit distinct banks.
+// a column the finished sums go through shared memory to warp kNodalWarp,
+// which applies the nodal update to node column cc, and each lane's started
+// chains become its finishing ones.  Records are stored SoA with an XOR
+// swizzle of the low index bits so that lanes of consecutive rows (records
+// ~ppc apart) hit distinct banks.
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kRec = 13;  // xi eta Mp mpx mpy FPx FPy Frx Fry F11 F12 F22 Vp
 constexpr int kPf = (kCap + kP2GThreads - 1) / kP2GThreads;
 
+// The staged records of one batch: the four record pairs and five single
+// values of each particle (13 values of R).
 template <class R>
 struct P2GSmemT {
-  R rec[kRec][kCap];
-  R xch[9][kTR];  // finished sums per quantity
+  V2<R> pr[4][kCap];  // xe, mp, qg, qf
+  R sg[5][kCap];      // Mp, F11, F12, F22, Vp
+  R xch[9][kTR];      // finished sums per quantity
   double led[6][kP2GThreads / 32];
   int rowstart[3][kTR + 2];
 };
 using P2GSmem = P2GSmemT<double>;
 
-// Record slot of batch position j: an XOR of the bank-selecting low bits by
-// the next ones (16 eight-byte or 32 four-byte slots span the 32 banks).
+// Slot of batch position j: an XOR of the bank-selecting low bits by the
+// next ones, so that lanes reading cells 16 records apart hit distinct banks
+// (8 sixteen-byte, 16 eight-byte or 32 four-byte slots span the 32 banks).
 template <class R>
-__device__ __forceinline__ int swz(int j) {
+__device__ __forceinline__ int swz_pair(int j) {
+  return sizeof(R) == 8 ? (j ^ ((j >> 4) & 7)) : (j ^ ((j >> 4) & 15));
+}
+template <class R>
+__device__ __forceinline__ int swz_one(int j) {
   return sizeof(R) == 8 ? (j ^ ((j >> 4) & 15)) : (j ^ ((j >> 5) & 31));
 }
 
 template <int kBytes>
 __device__ __forceinline__ void cp_async(void* dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  if (kBytes == 8)
+  if (kBytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else if (kBytes == 8)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
@@ -612,26 +618,22 @@ template <class R>
 __device__ __forceinline__ void issue_gather(P2GSmemT<R>& s, const ParticlesT<R>& p,
                                              const int (&pf)[kPf],
                                              const Batch& b) {
-  constexpr int kB = sizeof(R);
+  constexpr int kB = sizeof(R), kB2 = sizeof(V2<R>);
 #pragma unroll
   for (int u = 0; u < kPf; ++u) {
     const int j = b.bb + threadIdx.x + u * kP2GThreads;
     if (j >= b.be) break;
     const int i = pf[u];
-    const int l = swz<R>(j - b.bb);
-    cp_async<kB>(&s.rec[0][l], p.qxi + i);
-    cp_async<kB>(&s.rec[1][l], p.qeta + i);
-    cp_async<kB>(&s.rec[2][l], p.Mp + i);
-    cp_async<kB>(&s.rec[3][l], p.mpx + i);
-    cp_async<kB>(&s.rec[4][l], p.mpy + i);
-    cp_async<kB>(&s.rec[5][l], p.qgx + i);
-    cp_async<kB>(&s.rec[6][l], p.qgy + i);
-    cp_async<kB>(&s.rec[7][l], p.qfx + i);
-    cp_async<kB>(&s.rec[8][l], p.qfy + i);
-    cp_async<kB>(&s.rec[9][l], p.F11 + i);
-    cp_async<kB>(&s.rec[10][l], p.F12 + i);
-    cp_async<kB>(&s.rec[11][l], p.F22 + i);
-    cp_async<kB>(&s.rec[12][l], p.Vp + i);
+    const int l2 = swz_pair<R>(j - b.bb), l1 = swz_one<R>(j - b.bb);
+    cp_async<kB2>(&s.pr[0][l2], p.xe + i);
+    cp_async<kB2>(&s.pr[1][l2], p.mp + i);
+    cp_async<kB2>(&s.pr[2][l2], p.qg + i);
+    cp_async<kB2>(&s.pr[3][l2], p.qf + i);
+    cp_async<kB>(&s.sg[0][l1], p.Mp + i);
+    cp_async<kB>(&s.sg[1][l1], p.F11 + i);
+    cp_async<kB>(&s.sg[2][l1], p.F12 + i);
+    cp_async<kB>(&s.sg[3][l1], p.F22 + i);
+    cp_async<kB>(&s.sg[4][l1], p.Vp + i);
   }
   cp_async_commit();
 }
@@ -719,10 +721,16 @@ __device__ __forceinline__ R acc_value(R s, R c) {
 }
 
 // Running sums of one lane: finishing (f) and starting (s) chains, with
-// their compensations (FP32 only).
+// their compensations (FP32 only).  Quantity groups (one warp each):
+//   0: Mv, mom_x, mom_y         1: FPx, FPy, Fric_x, Fric_y
+//   2: F_int_x                   3: F_int_y
+// about the same FP64 work per particle in each; the lightest (3) also runs
+// the nodal update.
+constexpr int kMaxQ = 4;
+constexpr int kNodalWarp = 3;
 template <class R>
 struct Chains {
-  R f[3], fc[3], s[3], sc[3];
+  R f[kMaxQ], fc[kMaxQ], s[kMaxQ], sc[kMaxQ];
 };
 
 // One particle's contributions to the chains of quantity group kG: `upper`
@@ -731,47 +739,58 @@ struct Chains {
 //   fin   N = (1-xi)*fb, Nx = mihx*fb, Ny = (1-xi)*(ihy or mihy)
 //   start N = xi*fb,     Nx = ihx*fb,  Ny = xi*(ihy or mihy)
 // -- shp/shg of main/gpu_kernels.cpp:33-59 for those local nodes.  kFin off
-// runs the started chains alone (a unit's leading column).
+// runs the started chains alone (a unit's leading column).  Group 0 also
+// adds Mp and the momentum to the particle ledger (`led`, once per particle).
 template <class R, int kG, bool kFin>
-__device__ __forceinline__ void chain_step(Chains<R>& a, const P2GSmemT<R>& s, int l,
-                                           bool upper, const ShapeT<R>& sh) {
-  const R xi = s.rec[0][l], eta = s.rec[1][l];
+__device__ __forceinline__ void chain_step(Chains<R>& a, const P2GSmemT<R>& s, int j,
+                                           bool upper, const ShapeT<R>& sh, bool led,
+                                           double& lp0, double& lp1, double& lp2) {
+  const int l2 = swz_pair<R>(j), l1 = swz_one<R>(j);
+  const V2<R> xe = s.pr[0][l2];
+  const R xi = xe.x, eta = xe.y;
   const R fa = R(1) - xi;
   const R fb = upper ? eta : (R(1) - eta);
-  const R Nf = fa * fb;
-  const R Ns = xi * fb;
-  if (kG == 0 || kG == 1) {
-    const int o = kG == 0 ? 2 : 5;
-    const R q0 = s.rec[o][l], q1 = s.rec[o + 1][l], q2 = s.rec[o + 2][l];
-    if (kFin) {
-      acc_add(a.f[0], a.fc[0], Nf * q0);
-      acc_add(a.f[1], a.fc[1], Nf * q1);
-      acc_add(a.f[2], a.fc[2], Nf * q2);
+  if constexpr (kG == 0 || kG == 1) {
+    constexpr int nq = kG == 0 ? 3 : 4;
+    const R Nf = fa * fb;
+    const R Ns = xi * fb;
+    R q[nq];
+    if constexpr (kG == 0) {
+      const V2<R> m = s.pr[1][l2];
+      q[0] = s.sg[0][l1];
+      q[1] = m.x;
+      q[2] = m.y;
+      if (led) {
+        lp0 += q[0];
+        lp1 += q[1];
+        lp2 += q[2];
+      }
+    } else {
+      const V2<R> g = s.pr[2][l2], f = s.pr[3][l2];
+      q[0] = g.x;
+      q[1] = g.y;
+      q[2] = f.x;
+      q[3] = f.y;
     }
-    acc_add(a.s[0], a.sc[0], Ns * q0);
-    acc_add(a.s[1], a.sc[1], Ns * q1);
-    acc_add(a.s[2], a.sc[2], Ns * q2);
+    if (kFin) {
+#pragma unroll
+      for (int k = 0; k < nq; ++k) acc_add(a.f[k], a.fc[k], Nf * q[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < nq; ++k) acc_add(a.s[k], a.sc[k], Ns * q[k]);
   } else {
     const R hy = upper ? sh.ihy : sh.mihy;
     const R Nxs = sh.ihx * fb, Nys = xi * hy;
-    const R f12 = s.rec[10][l], vp = s.rec[12][l];
-    if (kG == 2) {
-      const R q0 = s.rec[8][l], f11 = s.rec[9][l];
-      if (kFin) {
-        const R Nxf = sh.mihx * fb, Nyf = fa * hy;
-        acc_add(a.f[0], a.fc[0], Nf * q0);
-        acc_add(a.f[1], a.fc[1], (Nxf * f11 + Nyf * f12) * vp);
-      }
-      acc_add(a.s[0], a.sc[0], Ns * q0);
-      acc_add(a.s[1], a.sc[1], (Nxs * f11 + Nys * f12) * vp);
-    } else {
-      const R f22 = s.rec[11][l];
-      if (kFin) {
-        const R Nxf = sh.mihx * fb, Nyf = fa * hy;
-        acc_add(a.f[0], a.fc[0], (Nxf * f12 + Nyf * f22) * vp);
-      }
-      acc_add(a.s[0], a.sc[0], (Nxs * f12 + Nys * f22) * vp);
+    const R f12 = s.sg[2][l1], vp = s.sg[4][l1];
+    const R fo = kG == 2 ? s.sg[1][l1] : s.sg[3][l1];  // F11 or F22
+    // F_int_x: (Nx*F11 + Ny*F12)*Vp;  F_int_y: (Nx*F12 + Ny*F22)*Vp
+    if (kFin) {
+      const R Nxf = sh.mihx * fb, Nyf = fa * hy;
+      const R v = kG == 2 ? (Nxf * fo + Nyf * f12) : (Nxf * f12 + Nyf * fo);
+      acc_add(a.f[0], a.fc[0], v * vp);
     }
+    const R v = kG == 2 ? (Nxs * fo + Nys * f12) : (Nxs * f12 + Nys * fo);
+    acc_add(a.s[0], a.sc[0], v * vp);
   }
 }
 
@@ -786,14 +805,9 @@ __device__ __forceinline__ void chain_range(Chains<R>& a, const P2GSmemT<R>& s, 
   int j = max(a0, bb);
 #pragma unroll 2
   for (; j < j1; ++j) {
-    const int l = swz<R>(j - bb);
     const bool upper = j < a1;
-    chain_step<R, kG, kFin>(a, s, l, upper, sh);
-    if (kG == 0 && own && !upper) {  // particle ledger, once each
-      lp0 += s.rec[2][l];
-      lp1 += s.rec[3][l];
-      lp2 += s.rec[4][l];
-    }
+    chain_step<R, kG, kFin>(a, s, j - bb, upper, sh, kG == 0 && own && !upper, lp0, lp1,
+                            lp2);
   }
 }
 
@@ -1005,15 +1019,15 @@ __device__ __forceinline__ void p2g_unit(
   const bool row_ok = lane_ok && (r <= nrows);
   const double dt = S->dt;
   const ShapeT<R> sh{R(1) / R(G.hx), -R(1) / R(G.hx), R(1) / R(G.hy), -R(1) / R(G.hy)};
-  // exchange slots of each group's quantities: g0 0-2, g1 3-5, g2 6-7, g3 8
-  const int slot0 = grp == 0 ? 0 : grp == 1 ? 3 : grp == 2 ? 6 : 8;
-  const int nq = grp < 2 ? 3 : grp == 2 ? 2 : 1;
+  // exchange slots of each group's quantities: g0 0-2, g1 3-6, g2 7, g3 8
+  const int slot0 = grp == 0 ? 0 : grp == 1 ? 3 : grp == 2 ? 7 : 8;
+  const int nq = grp == 0 ? 3 : grp == 1 ? 4 : 1;
   const bool last_unit_col = (cB == ncols + 1);  // this unit closes node column ncols
 
   double lp0 = 0, lp1 = 0, lp2 = 0, ln0 = 0, ln1 = 0, ln2 = 0;
   Chains<R> a;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) a.f[q] = a.fc[q] = a.s[q] = a.sc[q] = R(0);
+  for (int q = 0; q < kMaxQ; ++q) a.f[q] = a.fc[q] = a.s[q] = a.sc[q] = R(0);
 
   // prologue: row starts of the first two columns, sorted indices of batch 0
   for (int q = tid; q < 2 * nrs; q += kP2GThreads) {
@@ -1071,7 +1085,7 @@ __device__ __forceinline__ void p2g_unit(
     __syncthreads();  // shared records free; finished sums exchanged
     if (last_of_col) {
       // ---- nodal update of node column cc ------------------------------
-      if (warp == 0 && row_ok && cur.cc >= cA) {
+      if (warp == kNodalWarp && row_ok && cur.cc >= cA) {
         const R (*X)[kTR] = s.xch;
         nodal_update<R>(X[0][row], X[1][row], X[2][row], X[3][row], X[4][row],
                         X[5][row], X[6][row], X[7][row], X[8][row], r, cur.cc, G, P,
@@ -1083,7 +1097,7 @@ __device__ __forceinline__ void p2g_unit(
         if (lane_ok)
           for (int q = 0; q < nq; ++q) s.xch[slot0 + q][row] = acc_value(a.s[q], a.sc[q]);
         __syncthreads();
-        if (warp == 0 && row_ok) {
+        if (warp == kNodalWarp && row_ok) {
           const R (*X)[kTR] = s.xch;
           nodal_update<R>(X[0][row], X[1][row], X[2][row], X[3][row], X[4][row],
                           X[5][row], X[6][row], X[7][row], X[8][row], r, ncols, G, P,
@@ -1091,7 +1105,7 @@ __device__ __forceinline__ void p2g_unit(
         }
       }
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
+      for (int q = 0; q < kMaxQ; ++q) {
         a.f[q] = a.s[q];
         a.fc[q] = a.sc[q];
         a.s[q] = R(0);
@@ -1251,10 +1265,11 @@ __device__ __forceinline__ void g2p_particle(
     p.apy[i] = ay;
     p.dZxp[i] = R(dzx);
     p.dZyp[i] = R(dzy);
-    p.Fpx[i] = p.qgx[i];
-    p.Fpy[i] = p.qgy[i];
-    p.Frx[i] = p.qfx[i];
-    p.Fry[i] = p.qfy[i];
+    const V2<R> qg = p.qg[i], qf = p.qf[i];
+    p.Fpx[i] = qg.x;
+    p.Fpy[i] = qg.y;
+    p.Frx[i] = qf.x;
+    p.Fry[i] = qf.y;
   }
   const R vpx = vxL, vpy = vyL;
   x = x + dt * vpx;
@@ -1305,19 +1320,15 @@ __device__ __forceinline__ void g2p_particle(
   // binning (:387,447-454)
   {
     const R Mp = p.Mp[i], Vp = p.Vp[i];
-    p.mpx[i] = vpx * Mp;
-    p.mpy[i] = vpy * Mp;
+    p.mp[i] = V2<R>{vpx * Mp, vpy * Mp};
     const R Ap = hp > R(1.e-2) ? Vp / hp : R(0);
     R fbx, fby;
     voellmy(P, vpx, vpy, hp, fbx, fby);
-    p.qfx[i] = Ap * fbx;
-    p.qfy[i] = Ap * fby;
+    p.qf[i] = V2<R>{Ap * fbx, Ap * fby};
     R qxi, qeta, qgx, qgy;
     next_record(G, P, Z, x, y, hp, H, Vp, qxi, qeta, qgx, qgy);
-    p.qxi[i] = qxi;
-    p.qeta[i] = qeta;
-    p.qgx[i] = qgx;
-    p.qgy[i] = qgy;
+    p.xe[i] = V2<R>{qxi, qeta};
+    p.qg[i] = V2<R>{qgx, qgy};
   }
   if (record) {
     // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
@@ -1566,16 +1577,16 @@ __global__ void k_b_move(ParticlesT<R> dst, ParticlesT<R> src, const int4* __res
   const int4 m = mblk[blockIdx.x];
   if ((int)threadIdx.x >= m.z) return;
   const int i = m.y + threadIdx.x, o = m.x + threadIdx.x;
-  R* const* df[] = {&dst.x, &dst.y, &dst.vpx, &dst.vpy, &dst.hp, &dst.F11,
-                         &dst.F12, &dst.F22, &dst.Mp, &dst.Vp, &dst.H, &dst.mpx,
-                         &dst.mpy, &dst.qfx, &dst.qfy, &dst.qxi, &dst.qeta, &dst.qgx,
-                         &dst.qgy, &dst.Ap, &dst.Fbx, &dst.Fby};
-  R* const* sf[] = {&src.x, &src.y, &src.vpx, &src.vpy, &src.hp, &src.F11,
-                         &src.F12, &src.F22, &src.Mp, &src.Vp, &src.H, &src.mpx,
-                         &src.mpy, &src.qfx, &src.qfy, &src.qxi, &src.qeta, &src.qgx,
-                         &src.qgy, &src.Ap, &src.Fbx, &src.Fby};
+  R* const* df[] = {&dst.x,  &dst.y,  &dst.vpx, &dst.vpy, &dst.hp, &dst.F11, &dst.F12,
+                    &dst.F22, &dst.Mp, &dst.Vp, &dst.H, &dst.Ap, &dst.Fbx, &dst.Fby};
+  R* const* sf[] = {&src.x,  &src.y,  &src.vpx, &src.vpy, &src.hp, &src.F11, &src.F12,
+                    &src.F22, &src.Mp, &src.Vp, &src.H, &src.Ap, &src.Fbx, &src.Fby};
 #pragma unroll
-  for (int f = 0; f < 22; ++f) (*df[f])[o] = (*sf[f])[i];
+  for (int f = 0; f < 14; ++f) (*df[f])[o] = (*sf[f])[i];
+  V2<R>* const* dv[] = {&dst.mp, &dst.qf, &dst.xe, &dst.qg};
+  V2<R>* const* sv[] = {&src.mp, &src.qf, &src.xe, &src.qg};
+#pragma unroll
+  for (int f = 0; f < 4; ++f) (*dv[f])[o] = (*sv[f])[i];
   dst.label[o] = src.label[i];
   dst.level[o] = src.level[i];
   dst.key[o] = src.key[i] + m.w;
