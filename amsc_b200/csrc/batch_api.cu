@@ -54,6 +54,7 @@ struct dampm_batch {
   void *vvxL = nullptr, *vvyL = nullptr;  // real type of the precision
   int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr;
   int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr, *cbig = nullptr;
+  int* cmid = nullptr;  // cells with more than 16 particles
   int* ustart = nullptr;
   long long* upex = nullptr;
   int2* uplan = nullptr;
@@ -203,7 +204,8 @@ int read_scalars(dampm_batch* b) {
   return DAMPM_OK;
 }
 
-// One pass of every live scenario.
+// One pass of every live scenario: kPassLaunches kernel launches.
+constexpr int kPassLaunches = 16;
 int enqueue_pass(dampm_batch* b) {
   cudaStream_t st = b->stream;
   const int nscn = int(b->scns.size());
@@ -218,8 +220,10 @@ int enqueue_pass(dampm_batch* b) {
   k_scan_apply<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(
       b->count, int(b->C_tot), b->tile_sum, b->start, b->clist, b->clist_n, b->Sg);
   k_scatter<<<gp, 256, 0, st>>>(keys_of(b), b->slot, b->start, b->perm, b->Sg);
-  k_segment_order<<<148 * 8, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
-                                            b->cbig, b->Sg);
+  k_segment_order<<<148 * 4, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
+                                            b->cmid, b->Sg);
+  k_segment_order_mid<<<148 * 8, 256, 0, st>>>(b->start, b->cmid, b->clist_n, b->perm,
+                                                b->cbig, b->Sg);
   k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
                                             b->slot, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
@@ -247,7 +251,7 @@ int enqueue_pass(dampm_batch* b) {
                          static_cast<const double*>(b->vvyL), b->Z[b->cur], b->scn, b->S,
                          b->gblk, b->Sg);
   k_b_step_end<<<1, 1024, 0, st>>>(b->scn, b->S, nscn);
-  b->launches += 15;
+  b->launches += kPassLaunches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
   return DAMPM_OK;
@@ -369,6 +373,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   rc = rc ? rc : balloc(b, &b->slot, pc);
   rc = rc ? rc : balloc(b, &b->perm, pc);
   rc = rc ? rc : balloc(b, &b->cbig, pc / 256 + 4);
+  rc = rc ? rc : balloc(b, &b->cmid, pc / 17 + 4);
   const size_t us = size_t(b->USEG_cap);
   rc = rc ? rc : balloc(b, &b->ustart, us);
   rc = rc ? rc : balloc(b, &b->upex, us);
@@ -604,7 +609,7 @@ int dampm_batch_step(dampm_batch* b, int nsteps) {
     b->graph_dirty = false;
   }
   BCK(cudaGraphLaunch(b->graph, b->stream));
-  b->launches += 15LL * nsteps;
+  b->launches += (long long)kPassLaunches * nsteps;
   return DAMPM_OK;
 }
 

@@ -42,6 +42,7 @@ struct dampm_ctx {
   int4* ulist = nullptr;
   int *clist = nullptr, *clist_n = nullptr;  // cells with >= 2 particles
   int* cbig = nullptr;  // cells with more than 256 particles (capacity / 256)
+  int* cmid = nullptr;  // cells with more than 16 particles (capacity / 17)
   double* ledger_log = nullptr;  // kLedgerLog rows {t, err_mass, err_mom}
   int p2g_grid = 0;
   Scalars* S = nullptr;
@@ -162,6 +163,8 @@ int alloc_particles(dampm_ctx* ctx, long long cap) {
   {
     int rc = dalloc(ctx, &ctx->cbig, size_t(cap / 256 + 4));
     if (rc) return rc;
+    rc = dalloc(ctx, &ctx->cmid, size_t(cap / 17 + 4));
+    if (rc) return rc;
   }
   int rc = ms_alloc(ctx->msb, cap, ctx->nc, [&](void** q, size_t bytes) {
     return dalloc(ctx, reinterpret_cast<unsigned char**>(q), bytes);
@@ -184,12 +187,15 @@ void enqueue_sort(dampm_ctx* ctx) {
       ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S);
   k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->slot, ctx->start,
                                          ctx->perm, ctx->S);
-  k_segment_order<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,
-                                                   ctx->clist_n, ctx->perm, ctx->cbig,
+  k_segment_order<<<148 * 4, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,
+                                                   ctx->clist_n, ctx->perm, ctx->cmid,
                                                    ctx->S);
+  k_segment_order_mid<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->cmid,
+                                                       ctx->clist_n, ctx->perm, ctx->cbig,
+                                                       ctx->S);
   k_segment_order_big<<<148, 1024, 0, ctx->stream>>>(ctx->start, ctx->cbig, ctx->clist_n,
                                                      ctx->perm, ctx->slot, ctx->S);
-  ctx->launches += 8;
+  ctx->launches += 9;
 }
 
 int enqueue_pass(dampm_ctx* ctx) {

@@ -112,7 +112,9 @@ __global__ void k_list_reset(int* list_n, const Scalars* S);
 __global__ void k_scatter(const int* key, const int* slot, const int* start,
                           int* perm, const Scalars* S);
 __global__ void k_segment_order(const int* start, const int* list, int* list_n,
-                                int* perm, int* big, const Scalars* S);
+                                int* perm, int* mid, const Scalars* S);
+__global__ void k_segment_order_mid(const int* start, const int* mid, int* list_n,
+                                    int* perm, int* big, const Scalars* S);
 __global__ void k_segment_order_big(const int* start, const int* big,
                                     const int* list_n, int* perm, int* tmp,
                                     const Scalars* S);

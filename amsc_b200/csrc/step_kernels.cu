@@ -233,13 +233,26 @@ __global__ void k_prep(ParticlesT<R> p, const double* __restrict__ Z, Geom G,
 // SORT: stable counting sort by cell, (cell, particle index) order
 // (init_particle_mesh + cell_start/cell_ptcls, main/gpu_offload.cpp:243-249)
 // ---------------------------------------------------------------------------
+// Particle i takes slot[i] among its cell's particles: one atomic per cell
+// and warp (the lanes of a warp that share a cell take consecutive slots in
+// index order).
 __global__ void k_count(const int* __restrict__ key, int* __restrict__ count,
                         int* __restrict__ slot, const Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
-       i += gridDim.x * blockDim.x)
-    slot[i] = atomicAdd(&count[key[i]], 1);
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < np; i0 += stride) {
+    const int i = i0 + lane;
+    const bool ok = i < np;
+    const int k = ok ? key[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (ok && lane == leader) base = atomicAdd(&count[k], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (ok) slot[i] = base + __popc(peers & ((1u << lane) - 1u));
+  }
 }
 
 // Exclusive scan of count[0..n) into start[0..n] in two passes over tiles of
@@ -348,10 +361,26 @@ __global__ void __launch_bounds__(kScanThreads)
       }
   }
   if (list) {
+    // one atomic per warp: the warp's listed cells go to consecutive slots
     const int cv[4] = {c.x, c.y, c.z, c.w};
+    int mine = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mine += cv[k] >= 2 ? 1 : 0;
+    const int lane = threadIdx.x & 31;
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+    int base = 0;
+    if (lane == 31 && wtot > 0) base = atomicAdd(list_n, wtot);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int q = base + incl - mine;
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (cv[k] >= 2) list[atomicAdd(list_n, 1)] = i0 + k;
+      if (cv[k] >= 2) list[q++] = i0 + k;
   }
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[n] = tile_sum[gridDim.x];
 }
@@ -368,77 +397,143 @@ __global__ void k_scatter(const int* __restrict__ key,
 }
 
 // list_n[0]: cells with two or more particles; list_n[1]: crowded cells
-// handed on to k_segment_order_big
+// handed on to k_segment_order_big; list_n[2]: cells of more than
+// kThreadSort particles handed on to k_segment_order_mid
 __global__ void k_list_reset(int* list_n, const Scalars* S) {
   if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) {
     list_n[0] = 0;
     list_n[1] = 0;
+    list_n[2] = 0;
   }
 }
 
 // Orders each listed cell's segment by ascending particle index (the atomics
-// of k_count hand out slots in arbitrary order).  One warp per cell: a
-// register bitonic sort for up to 32 particles; a rank sort for up to
-// 32 * kRankPer (each lane holds kRankPer indices and counts, over all the
-// cell's indices broadcast lane by lane, those below each of its own).
-// Particle indices are unique, so the ranks are a permutation of [0, m).
-// Larger cells are listed in `big` for k_segment_order_big.
+// of k_count hand out slots in arbitrary order).  k_segment_order: each lane
+// sorts a cell of up to kThreadSort particles in registers (a bitonic
+// network over static indices) and hands larger cells on to `mid`.
+// k_segment_order_mid, one warp per cell: a register bitonic sort across the
+// lanes for up to 32 particles, a rank sort for up to 32 * kRankPer (each
+// lane holds kRankPer indices and counts, over all the cell's indices
+// broadcast lane by lane, those below each of its own; particle indices are
+// unique, so the ranks are a permutation of [0, m)); larger cells go on to
+// `big` for k_segment_order_big.
+constexpr int kThreadSort = 16;
 constexpr int kRankPer = 8;
 constexpr int kBigRun = 8192;
 
-// (eight resident blocks per SM for the common small cells; the rank sort's
-// registers may spill for the rare crowded ones)
-__global__ void __launch_bounds__(256, 8) k_segment_order(const int* __restrict__ start,
+__device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m) {
+  int v[kThreadSort];
+#pragma unroll
+  for (int k = 0; k < kThreadSort; ++k) v[k] = k < m ? seg[k] : 0x7fffffff;
+#pragma unroll
+  for (int k = 2; k <= kThreadSort; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < kThreadSort; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const int a = v[i], b = v[l];
+          const bool up = (i & k) == 0;
+          v[i] = up ? min(a, b) : max(a, b);
+          v[l] = up ? max(a, b) : min(a, b);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kThreadSort; ++k)
+    if (k < m) seg[k] = v[k];
+}
+
+__device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b, int m,
+                                                  int c, int lane, int* __restrict__ big,
+                                                  int* __restrict__ list_n) {
+  if (m <= 32) {
+    int v = (lane < m) ? perm[b + lane] : 0x7fffffff;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const int o = __shfl_xor_sync(0xffffffffu, v, j);
+        const bool up = ((lane & k) == 0);
+        const bool lower = ((lane & j) == 0);
+        // keep the min in the lower lane of an ascending pair
+        v = (lower == up) ? min(v, o) : max(v, o);
+      }
+    }
+    if (lane < m) perm[b + lane] = v;
+  } else if (m <= 32 * kRankPer) {
+    int v[kRankPer], rank[kRankPer];
+#pragma unroll
+    for (int t = 0; t < kRankPer; ++t) {
+      const int q = lane + 32 * t;
+      v[t] = (q < m) ? perm[b + q] : 0x7fffffff;
+      rank[t] = 0;
+    }
+#pragma unroll
+    for (int t2 = 0; t2 < kRankPer; ++t2) {
+      if (32 * t2 >= m) break;  // warp-uniform
+      for (int src = 0; src < 32; ++src) {
+        const int o = __shfl_sync(0xffffffffu, v[t2], src);
+#pragma unroll
+        for (int t = 0; t < kRankPer; ++t) rank[t] += (o < v[t]) ? 1 : 0;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kRankPer; ++t)
+      if (lane + 32 * t < m) perm[b + rank[t]] = v[t];
+  } else if (lane == 0) {
+    big[atomicAdd(&list_n[1], 1)] = c;
+  }
+}
+
+// (four resident blocks per SM: registers for a lane's whole cell)
+__global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict__ start,
                                 const int* __restrict__ list,
                                 int* __restrict__ list_n,
-                                int* __restrict__ perm, int* __restrict__ big,
+                                int* __restrict__ perm, int* __restrict__ mid,
                                 const Scalars* S) {
   if (!S->active) return;
   const int lane = threadIdx.x & 31;
-  const int nl = *list_n;
-  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nl;
-       w += (gridDim.x * blockDim.x) >> 5) {
-    const int c = list[w];
-    const int b = start[c], e = start[c + 1];
-    const int m = e - b;
-    if (m <= 32) {
-      int v = (lane < m) ? perm[b + lane] : 0x7fffffff;
-#pragma unroll
-      for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          const int o = __shfl_xor_sync(0xffffffffu, v, j);
-          const bool up = ((lane & k) == 0);
-          const bool lower = ((lane & j) == 0);
-          // keep the min in the lower lane of an ascending pair
-          v = (lower == up) ? min(v, o) : max(v, o);
-        }
-      }
-      if (lane < m) perm[b + lane] = v;
-    } else if (m <= 32 * kRankPer) {
-      int v[kRankPer], rank[kRankPer];
-#pragma unroll
-      for (int t = 0; t < kRankPer; ++t) {
-        const int q = lane + 32 * t;
-        v[t] = (q < m) ? perm[b + q] : 0x7fffffff;
-        rank[t] = 0;
-      }
-#pragma unroll
-      for (int t2 = 0; t2 < kRankPer; ++t2) {
-        if (32 * t2 >= m) break;  // warp-uniform
-        for (int src = 0; src < 32; ++src) {
-          const int o = __shfl_sync(0xffffffffu, v[t2], src);
-#pragma unroll
-          for (int t = 0; t < kRankPer; ++t) rank[t] += (o < v[t]) ? 1 : 0;
-        }
-      }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < kRankPer; ++t)
-        if (lane + 32 * t < m) perm[b + rank[t]] = v[t];
-    } else if (lane == 0) {
-      big[atomicAdd(&list_n[1], 1)] = c;
+  const int nl = list_n[0];
+  for (int w0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; w0 < nl;
+       w0 += ((gridDim.x * blockDim.x) >> 5) * 32) {
+    const int q = w0 + lane;
+    int c = 0, b = 0, m = 0;
+    if (q < nl) {
+      c = list[q];
+      b = start[c];
+      m = start[c + 1] - b;
     }
+    if (m <= kThreadSort) {
+      if (m >= 2) thread_sort_segment(perm + b, m);
+    }
+    // larger cells: one atomic per warp
+    const unsigned larger = __ballot_sync(0xffffffffu, m > kThreadSort);
+    if (larger) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&list_n[2], __popc(larger));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (m > kThreadSort) mid[base + __popc(larger & ((1u << lane) - 1u))] = c;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256, 8) k_segment_order_mid(const int* __restrict__ start,
+                                    const int* __restrict__ mid,
+                                    int* __restrict__ list_n,
+                                    int* __restrict__ perm, int* __restrict__ big,
+                                    const Scalars* S) {
+  if (!S->active) return;
+  const int lane = threadIdx.x & 31;
+  const int nm = list_n[2];
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nm;
+       w += (gridDim.x * blockDim.x) >> 5) {
+    const int c = mid[w];
+    const int b = start[c];
+    warp_sort_segment(perm, b, start[c + 1] - b, c, lane, big, list_n);
   }
 }
 
