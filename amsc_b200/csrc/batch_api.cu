@@ -51,7 +51,7 @@ struct dampm_batch {
   ParticlesT<float> p32[2]{};   // FP32 form
   double* Z[2] = {nullptr, nullptr};
   int cur = 0;
-  void *vvxL = nullptr, *vvyL = nullptr;  // real type of the precision
+  void* vvL = nullptr;  // pairs (vvxL, vvyL) of the precision's real type
   int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr;
   int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr, *cbig = nullptr;
   int* cmid = nullptr;  // cells with more than 16 particles
@@ -234,21 +234,21 @@ int enqueue_pass(dampm_batch* b) {
       b->ucount, b->scn_units, b->Sg);
   if (b->precision == DAMPM_FP32)
     launch_b_p2g<float>(b->p2g_grid, st, b->p32[b->cur], b->perm, b->start,
-                        static_cast<float*>(b->vvxL), static_cast<float*>(b->vvyL),
+                        static_cast<float2*>(b->vvL),
                         b->led_part, b->scn, b->S, b->ulist, b->ucount, b->Sg);
   else
     launch_b_p2g<double>(b->p2g_grid, st, b->p64[b->cur], b->perm, b->start,
-                         static_cast<double*>(b->vvxL), static_cast<double*>(b->vvyL),
+                         static_cast<double2*>(b->vvL),
                          b->led_part, b->scn, b->S, b->ulist, b->ucount, b->Sg);
   k_b_ledger<<<nscn, 256, 0, st>>>(b->led_part, b->scn_units, b->scn, b->S, nscn,
                                    b->Sg);
   if (b->precision == DAMPM_FP32)
-    launch_b_g2p<float>(b->nblk, st, b->p32[b->cur], static_cast<const float*>(b->vvxL),
-                        static_cast<const float*>(b->vvyL), b->Z[b->cur], b->scn, b->S,
+    launch_b_g2p<float>(b->nblk, st, b->p32[b->cur], static_cast<const float2*>(b->vvL),
+                        b->Z[b->cur], b->scn, b->S,
                         b->gblk, b->Sg);
   else
-    launch_b_g2p<double>(b->nblk, st, b->p64[b->cur], static_cast<const double*>(b->vvxL),
-                         static_cast<const double*>(b->vvyL), b->Z[b->cur], b->scn, b->S,
+    launch_b_g2p<double>(b->nblk, st, b->p64[b->cur], static_cast<const double2*>(b->vvL),
+                         b->Z[b->cur], b->scn, b->S,
                          b->gblk, b->Sg);
   k_b_step_end<<<1, 1024, 0, st>>>(b->scn, b->S, nscn);
   b->launches += kPassLaunches;
@@ -362,8 +362,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   const size_t nn = size_t(node_cap), pc = size_t(particle_cap);
   rc = rc ? rc : balloc(b, &b->Z[0], nn);
   rc = rc ? rc : balloc(b, &b->Z[1], nn);
-  rc = rc ? rc : balloc(b, reinterpret_cast<unsigned char**>(&b->vvxL), nn * rsz);
-  rc = rc ? rc : balloc(b, reinterpret_cast<unsigned char**>(&b->vvyL), nn * rsz);
+  rc = rc ? rc : balloc(b, reinterpret_cast<unsigned char**>(&b->vvL), 2 * nn * rsz);
   // cells of all scenarios: fewer than their nodes
   rc = rc ? rc : balloc(b, &b->count, nn + 4);
   rc = rc ? rc : balloc(b, &b->start, nn + 1);
@@ -395,8 +394,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
     rc = bfail(b, DAMPM_ERR_CUDA, "cudaMallocHost failed");
   if (rc == DAMPM_OK) {
     cudaMemsetAsync(b->count, 0, sizeof(int) * (nn + 4), b->stream);
-    cudaMemsetAsync(b->vvxL, 0, rsz * nn, b->stream);
-    cudaMemsetAsync(b->vvyL, 0, rsz * nn, b->stream);
+    cudaMemsetAsync(b->vvL, 0, 2 * rsz * nn, b->stream);
     cudaMemsetAsync(b->S, 0, sizeof(Scalars) * size_t(scenario_cap), b->stream);
     cudaMemsetAsync(b->Sg, 0, sizeof(Scalars), b->stream);
     const int per_sm = f32 ? setup_b_p2g<float>() : setup_b_p2g<double>();

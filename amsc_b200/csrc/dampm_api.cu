@@ -229,10 +229,11 @@ int enqueue_pass(dampm_ctx* ctx) {
       ctx->strip_n, ctx->strips, ctx->useg, ctx->uplan, ctx->ulist, ctx->ucount, ctx->S);
   if (ctx->record) {
     Nodes& n = ctx->nodes;
-    double* nf[] = {n.vvxL, n.vvyL, n.Mv,  n.mvx,  n.mvy,   n.avx,   n.avy, n.vvx,
-                    n.vvy,  n.FPxv, n.FPyv, n.Fricx, n.Fricy, n.Fintx, n.Finty};
+    double* nf[] = {n.Mv,  n.mvx,  n.mvy,   n.avx,   n.avy,  n.vvx, n.vvy,
+                    n.FPxv, n.FPyv, n.Fricx, n.Fricy, n.Fintx, n.Finty};
     for (double* q : nf)
       cudaMemsetAsync(q, 0, sizeof(double) * ctx->nn, ctx->stream);
+    cudaMemsetAsync(n.vvL, 0, sizeof(double2) * ctx->nn, ctx->stream);
   }
   k_p2g<<<ctx->p2g_grid, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
       ctx->p, ctx->perm, ctx->start, ctx->nodes, ctx->led_part, ctx->G, ctx->P,
@@ -345,8 +346,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   rc = rc ? rc : dalloc(ctx, &ctx->Z, nn);
   rc = rc ? rc : dalloc(ctx, &ctx->dZdx, nn);
   rc = rc ? rc : dalloc(ctx, &ctx->dZdy, nn);
-  rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvxL, nn);
-  rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvyL, nn);
+  rc = rc ? rc : dalloc(ctx, &ctx->nodes.vvL, nn);
   ctx->ntiles = (ctx->nc + kScanTile - 1) / kScanTile;
   rc = rc ? rc : dalloc(ctx, &ctx->count, size_t(ctx->nc) + 4);
   rc = rc ? rc : dalloc(ctx, &ctx->clist, size_t(ctx->nc) + 4);
@@ -372,8 +372,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   }
   if (rc == DAMPM_OK) {
     cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream);
-    cudaMemsetAsync(ctx->nodes.vvxL, 0, sizeof(double) * nn, ctx->stream);
-    cudaMemsetAsync(ctx->nodes.vvyL, 0, sizeof(double) * nn, ctx->stream);
+    cudaMemsetAsync(ctx->nodes.vvL, 0, sizeof(double2) * nn, ctx->stream);
     cudaMemsetAsync(ctx->S, 0, sizeof(Scalars), ctx->stream);
     const size_t smem = p2g_smem_bytes();
     if (cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -645,9 +644,12 @@ int dampm_download_nodal(dampm_ctx* ctx, const char* field, double* out) {
   const std::string f(field);
   const double* src = nullptr;
   Nodes& n = ctx->nodes;
-  if (f == "vvxL") src = n.vvxL;
-  else if (f == "vvyL") src = n.vvyL;
-  else if (f == "Z") src = ctx->Z;
+  if (f == "vvxL" || f == "vvyL") {
+    CK(download_pair_half(out, n.vvL, f == "vvxL" ? 0 : 1, ctx->nn, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DAMPM_OK;
+  }
+  if (f == "Z") src = ctx->Z;
   else if (f == "dZdx") src = ctx->dZdx;
   else if (f == "dZdy") src = ctx->dZdy;
   else if (ctx->record_alloc) {

@@ -79,7 +79,7 @@ using Particles = ParticlesT<double>;
 // Nodal fields, quadgrid node order.
 template <class R>
 struct NodesT {
-  R *vvxL, *vvyL;
+  V2<R>* vvL;  // (vvxL, vvyL): the velocities G2P interpolates, one load per node
   // recorded only on output steps
   R *Mv, *mvx, *mvy, *avx, *avy, *vvx, *vvy, *FPxv, *FPyv, *Fricx,
       *Fricy, *Fintx, *Finty, *HV;
@@ -160,7 +160,7 @@ __global__ void k_b_units_flat(const int* strip_n, int strips, const int* strip_
                                const Scalars* Sg);
 template <class R>
 void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
-                  const int* cstart, R* vvxL, R* vvyL, double* led_part, const Scn* scn,
+                  const int* cstart, V2<R>* vvL, double* led_part, const Scn* scn,
                   Scalars* S, const int4* ulist, const int* ucount, const Scalars* Sg);
 // sets the batched P2G kernel's shared-memory attributes; returns the
 // resident CTAs per SM (0 on failure)
@@ -170,8 +170,8 @@ __global__ void k_b_ledger(const double* led_part, const int2* scn_units,
                            const Scn* scn, Scalars* S, int nscn,
                            const Scalars* Sg);
 template <class R>
-void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const R* vvxL,
-                  const R* vvyL, const double* Z, const Scn* scn, Scalars* S,
+void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const V2<R>* vvL,
+                  const double* Z, const Scn* scn, Scalars* S,
                   const int2* gblk, const Scalars* Sg);
 template <class R>
 void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> src,

@@ -767,8 +767,7 @@ __device__ __forceinline__ void nodal_update(
       avy = R(0); vvy = R(0); vvyL = R(0); momy = R(0);
     }
   }
-  nodes.vvxL[n] = vvxL;
-  nodes.vvyL[n] = vvyL;
+  nodes.vvL[n] = V2<R>{vvxL, vvyL};
   if (record) {
     nodes.Mv[n] = Mv;
     nodes.mvx[n] = momx;
@@ -1328,8 +1327,9 @@ __device__ __forceinline__ void g2p_particle(
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     nd[k] = node_of(k, c, r, nrows);
-    vxn[k] = nodes.vvxL[nd[k]];
-    vyn[k] = nodes.vvyL[nd[k]];
+    const V2<R> v = nodes.vvL[nd[k]];
+    vxn[k] = v.x;
+    vyn[k] = v.y;
   }
   R x = p.x[i], y = p.y[i];
   R xi, eta;
@@ -1597,7 +1597,7 @@ __global__ void __launch_bounds__(kPlanThreads)
 template <class R>
 __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     k_b_p2g(ParticlesT<R> p, const int* __restrict__ perm, const int* __restrict__ cstart,
-            R* __restrict__ vvxL, R* __restrict__ vvyL,
+            V2<R>* __restrict__ vvL,
             double* __restrict__ led_part, const Scn* __restrict__ scn, Scalars* S,
             const int4* __restrict__ ulist, const int* __restrict__ ucount,
             const Scalars* Sg) {
@@ -1617,8 +1617,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     const Phys P = scn[u.x].P;
     const int n_off = scn[u.x].n_off, c_off = scn[u.x].c_off;
     NodesT<R> nd{};
-    nd.vvxL = vvxL + n_off;
-    nd.vvyL = vvyL + n_off;
+    nd.vvL = vvL + n_off;
     p2g_unit<R>(p, perm, cstart + c_off, nd, led_part, G, P, &S[u.x], 0, sm, ui,
              make_int4(u.y, u.z, u.w, 0));
   }
@@ -1637,8 +1636,7 @@ __global__ void k_b_ledger(const double* __restrict__ led_part,
 // gblk[b] = {scenario, its first particle handled by block b}
 template <class R>
 __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
-    k_b_g2p(ParticlesT<R> p, const R* __restrict__ vvxL,
-            const R* __restrict__ vvyL, const double* __restrict__ Z,
+    k_b_g2p(ParticlesT<R> p, const V2<R>* __restrict__ vvL, const double* __restrict__ Z,
             const Scn* __restrict__ scn, Scalars* S, const int2* __restrict__ gblk,
             const Scalars* Sg) {
   if (!Sg->active) return;
@@ -1653,8 +1651,7 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   const int p_off = scn[s].p_off, np = scn[s].np;
   const int n_off = scn[s].n_off, c_off = scn[s].c_off;
   NodesT<R> nd{};
-  nd.vvxL = const_cast<R*>(vvxL) + n_off;
-  nd.vvyL = const_cast<R*>(vvyL) + n_off;
+  nd.vvL = const_cast<V2<R>*>(vvL) + n_off;
   const ShapeT<R> sh{R(1) / R(G.hx), -R(1) / R(G.hx), R(1) / R(G.hy), -R(1) / R(G.hy)};
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   const int li = e.y + threadIdx.x;
@@ -1748,10 +1745,10 @@ void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const do
 
 template <class R>
 void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
-                  const int* cstart, R* vvxL, R* vvyL, double* led_part, const Scn* scn,
+                  const int* cstart, V2<R>* vvL, double* led_part, const Scn* scn,
                   Scalars* S, const int4* ulist, const int* ucount, const Scalars* Sg) {
   k_b_p2g<R><<<grid, kP2GThreads, sizeof(P2GSmemT<R>), st>>>(
-      p, perm, cstart, vvxL, vvyL, led_part, scn, S, ulist, ucount, Sg);
+      p, perm, cstart, vvL, led_part, scn, S, ulist, ucount, Sg);
 }
 
 template <class R>
@@ -1770,10 +1767,10 @@ int setup_b_p2g() {
 }
 
 template <class R>
-void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const R* vvxL,
-                  const R* vvyL, const double* Z, const Scn* scn, Scalars* S,
+void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const V2<R>* vvL,
+                  const double* Z, const Scn* scn, Scalars* S,
                   const int2* gblk, const Scalars* Sg) {
-  k_b_g2p<R><<<grid, kG2PThreads, 0, st>>>(p, vvxL, vvyL, Z, scn, S, gblk, Sg);
+  k_b_g2p<R><<<grid, kG2PThreads, 0, st>>>(p, vvL, Z, scn, S, gblk, Sg);
 }
 
 template <class R>
@@ -1789,10 +1786,10 @@ void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> s
   template void launch_prep<R>(int, int, cudaStream_t, ParticlesT<R>, const double*,  \
                                Geom, Phys, const Scalars*, int);                      \
   template void launch_b_p2g<R>(int, cudaStream_t, ParticlesT<R>, const int*,         \
-                                const int*, R*, R*, double*, const Scn*, Scalars*,    \
+                                const int*, V2<R>*, double*, const Scn*, Scalars*,    \
                                 const int4*, const int*, const Scalars*);             \
   template int setup_b_p2g<R>();                                                      \
-  template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, const R*, const R*, \
+  template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, const V2<R>*,       \
                                 const double*, const Scn*, Scalars*, const int2*,     \
                                 const Scalars*);                                      \
   template void launch_b_move<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,     \
