@@ -243,9 +243,9 @@ int enqueue_pass(dampm_ctx* ctx) {
   k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S,
                                                ctx->ledger_log);
   ev_mark(ctx, 2);
-  k_g2p<<<grid_for(ctx->cap, kG2PThreads), kG2PThreads, 0, ctx->stream>>>(
-      ctx->p, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
-      (grad_next || ctx->record) ? 1 : 0);
+  launch_g2p(grid_for(ctx->cap, kG2PThreads), ctx->stream, ctx->p, ctx->nodes, ctx->Z,
+             ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
+             (grad_next || ctx->record) ? 1 : 0);
   if (ctx->record) {
     k_hv<<<grid_for(ctx->nn, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->perm, ctx->start,
                                                            ctx->nodes.HV, ctx->G, ctx->S);

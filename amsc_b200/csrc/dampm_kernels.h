@@ -131,8 +131,9 @@ __global__ void k_p2g(Particles p, const int* perm, const int* cstart,
 constexpr int kLedgerLog = 1024;  // rows of the per-step ledger log
 __global__ void k_ledger_final(const double* led_part, const int* ucount,
                                Scalars* S, double* log);
-__global__ void k_g2p(Particles p, Nodes nodes, const double* Z, Geom G,
-                      Phys P, Scalars* S, int record, int want_grad);
+// G2P of the single-scenario step (k_g2p_t specialised for the two flags)
+void launch_g2p(int grid, cudaStream_t st, Particles p, Nodes nodes, const double* Z,
+                Geom G, Phys P, Scalars* S, int record, int want_grad);
 
 // ---- batches of independent scenarios --------------------------------------
 // One scenario of a batch: its geometry, physics and place in the packed

@@ -1462,9 +1462,12 @@ __device__ __forceinline__ void cfl_block_max(unsigned long long m0,
   }
 }
 
+// kRecord / kGrad: the output fields and the velocity gradients are
+// written (compiled out of the plain step)
+template <bool kRecord, bool kGrad>
 __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
-    k_g2p(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
-          Phys P, Scalars* S, int record, int want_grad) {
+    k_g2p_t(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
+            Phys P, Scalars* S) {
   if (!S->active) return;
   __shared__ unsigned long long red[3];
   if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
@@ -1475,8 +1478,19 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x)
-    g2p_particle(p, i, nodes, Z, G, P, sh, dt, record, want_grad, 0, m0, m1, m2);
+    g2p_particle(p, i, nodes, Z, G, P, sh, dt, kRecord ? 1 : 0, kGrad ? 1 : 0, 0, m0, m1,
+                 m2);
   cfl_block_max(m0, m1, m2, red, S);
+}
+
+void launch_g2p(int grid, cudaStream_t st, Particles p, Nodes nodes, const double* Z,
+                Geom G, Phys P, Scalars* S, int record, int want_grad) {
+  if (record)
+    k_g2p_t<true, true><<<grid, kG2PThreads, 0, st>>>(p, nodes, Z, G, P, S);
+  else if (want_grad)
+    k_g2p_t<false, true><<<grid, kG2PThreads, 0, st>>>(p, nodes, Z, G, P, S);
+  else
+    k_g2p_t<false, false><<<grid, kG2PThreads, 0, st>>>(p, nodes, Z, G, P, S);
 }
 
 size_t p2g_smem_bytes() { return sizeof(P2GSmemT<double>); }
