@@ -235,9 +235,9 @@ int enqueue_pass(dampm_ctx* ctx) {
       cudaMemsetAsync(q, 0, sizeof(double) * ctx->nn, ctx->stream);
     cudaMemsetAsync(n.vvL, 0, sizeof(double2) * ctx->nn, ctx->stream);
   }
-  k_p2g<<<ctx->p2g_grid, kP2GThreads, p2g_smem_bytes(), ctx->stream>>>(
-      ctx->p, ctx->perm, ctx->start, ctx->nodes, ctx->led_part, ctx->G, ctx->P,
-      ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->ucount);
+  launch_p2g(ctx->p2g_grid, ctx->stream, ctx->p, ctx->perm, ctx->start, ctx->nodes,
+             ctx->led_part, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0, ctx->ulist,
+             ctx->ucount);
   ctx->launches += 2;
   ev_mark(ctx, 3);
   k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S,
@@ -374,16 +374,10 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
     cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream);
     cudaMemsetAsync(ctx->nodes.vvL, 0, sizeof(double2) * nn, ctx->stream);
     cudaMemsetAsync(ctx->S, 0, sizeof(Scalars), ctx->stream);
-    const size_t smem = p2g_smem_bytes();
-    if (cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem)) != cudaSuccess)
-      rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
-    cudaFuncSetAttribute(k_p2g, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         int(cudaSharedmemCarveoutMaxShared));
-    int per_sm = 0, nsm = 0, dev = 0;
+    int per_sm = setup_p2g(), nsm = 0, dev = 0;
+    if (per_sm == 0) rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g, kP2GThreads, smem);
     if (per_sm < 1) per_sm = 1;
     ctx->p2g_grid = std::max(1, std::min(nsm * per_sm, ctx->n_led));
   }

@@ -124,10 +124,13 @@ __global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
 __global__ void k_units_flat(const int* strip_n, int strips, int seg,
                              const int2* plan, int4* ulist, int* ucount,
                              const Scalars* S);
-__global__ void k_p2g(Particles p, const int* perm, const int* cstart,
-                      Nodes nodes, double* led_part, Geom G, Phys P,
-                      const Scalars* S, int record, const int4* ulist,
-                      const int* ucount);
+// P2G of the single-scenario step (k_p2g specialised for recorded outputs);
+// setup_p2g sets its shared-memory attributes and returns the resident CTAs
+// per SM (0 on failure)
+void launch_p2g(int grid, cudaStream_t st, Particles p, const int* perm, const int* cstart,
+                Nodes nodes, double* led_part, Geom G, Phys P, const Scalars* S, int record,
+                const int4* ulist, const int* ucount);
+int setup_p2g();
 constexpr int kLedgerLog = 1024;  // rows of the per-step ledger log
 __global__ void k_ledger_final(const double* led_part, const int* ucount,
                                Scalars* S, double* log);

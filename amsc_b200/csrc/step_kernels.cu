@@ -1228,12 +1228,15 @@ __device__ __forceinline__ void p2g_unit(
   }
 }
 
+// kRecord: the nodal output fields are written (compiled out of the plain
+// step)
+template <bool kRecord>
 __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     k_p2g(Particles p, const int* __restrict__ perm,
           const int* __restrict__ cstart, Nodes nodes,
           double* __restrict__ led_part, Geom G, Phys P, const Scalars* S,
-          int record, const int4* __restrict__ ulist,
-          const int* __restrict__ ucount) {
+          const int4* __restrict__ ulist, const int* __restrict__ ucount) {
+  constexpr int record = kRecord ? 1 : 0;
   if (!S->active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmem& s = *reinterpret_cast<P2GSmem*>(smem_raw);
@@ -1249,6 +1252,31 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     if (ui >= nunits) break;
     p2g_unit(p, perm, cstart, nodes, led_part, G, P, S, record, s, ui, ulist[ui]);
   }
+}
+
+int setup_p2g() {
+  const size_t smem = p2g_smem_bytes();
+  for (const void* f : {(const void*)k_p2g<false>, (const void*)k_p2g<true>}) {
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+        cudaSuccess)
+      return 0;
+    cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         int(cudaSharedmemCarveoutMaxShared));
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g<false>, kP2GThreads, smem);
+  return per_sm < 1 ? 1 : per_sm;
+}
+
+void launch_p2g(int grid, cudaStream_t st, Particles p, const int* perm, const int* cstart,
+                Nodes nodes, double* led_part, Geom G, Phys P, const Scalars* S, int record,
+                const int4* ulist, const int* ucount) {
+  if (record)
+    k_p2g<true><<<grid, kP2GThreads, p2g_smem_bytes(), st>>>(p, perm, cstart, nodes, led_part,
+                                                             G, P, S, ulist, ucount);
+  else
+    k_p2g<false><<<grid, kP2GThreads, p2g_smem_bytes(), st>>>(p, perm, cstart, nodes, led_part,
+                                                              G, P, S, ulist, ucount);
 }
 
 // Block reduction, in a fixed order, of the ledger partials of units
