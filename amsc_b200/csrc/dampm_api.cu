@@ -56,6 +56,13 @@ struct dampm_ctx {
   long long launches = 0;
   std::string err;
   std::vector<void*> allocs;
+  // CUDA graph of kGraphPasses identical passes, valid while graph_key (the
+  // values the captured launches took by value) is unchanged
+  bool use_graphs = true;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
+  unsigned char graph_key[sizeof(Particles) + sizeof(Nodes) + sizeof(Geom) + sizeof(Phys) +
+                          sizeof(long long) + sizeof(int)] = {};
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -260,6 +267,70 @@ int enqueue_pass(dampm_ctx* ctx) {
   return DAMPM_OK;
 }
 
+// Passes that are all alike (no merge/split cadence, no recorded outputs, no
+// event timing) can be replayed from a graph; not while the stream is being
+// captured by the caller.
+constexpr int kGraphPasses = 16;
+
+bool graph_eligible(dampm_ctx* ctx) {
+  if (!ctx->use_graphs || ctx->timing || ctx->record) return false;
+  if (ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 && ctx->ms.call_interval > 0)
+    return false;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusNone)
+    return false;
+  return true;
+}
+
+void graph_key_of(const dampm_ctx* ctx, unsigned char* k) {
+  size_t o = 0;
+  auto put = [&](const void* v, size_t n) {
+    std::memcpy(k + o, v, n);
+    o += n;
+  };
+  put(&ctx->p, sizeof(Particles));
+  put(&ctx->nodes, sizeof(Nodes));
+  put(&ctx->G, sizeof(Geom));
+  put(&ctx->P, sizeof(Phys));
+  put(&ctx->cap, sizeof(long long));
+  put(&ctx->p2g_grid, sizeof(int));
+}
+
+// (Re)captures kGraphPasses passes unless the graph in hand was captured
+// with the same buffers and parameters.
+int ensure_graph(dampm_ctx* ctx) {
+  unsigned char key[sizeof(ctx->graph_key)];
+  graph_key_of(ctx, key);
+  if (ctx->graph && std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) return DAMPM_OK;
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  const long long it0 = ctx->it_host, l0 = ctx->launches;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = DAMPM_OK;
+  for (int k = 0; k < kGraphPasses && rc == DAMPM_OK; ++k) rc = enqueue_pass(ctx);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->graph_launches = ctx->launches - l0;
+  ctx->it_host = it0;
+  ctx->launches = l0;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  const cudaError_t ei = cudaGraphInstantiate(&ctx->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    ctx->graph = nullptr;
+    return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
+  }
+  std::memcpy(ctx->graph_key, key, sizeof(key));
+  return DAMPM_OK;
+}
+
 int sync_status(dampm_ctx* ctx) {
   CK(cudaMemcpyAsync(ctx->Sh, ctx->S, sizeof(Scalars), cudaMemcpyDeviceToHost,
                      ctx->stream));
@@ -394,6 +465,7 @@ int dampm_ctx_destroy(dampm_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* q : ctx->allocs) cudaFree(q);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   if (ctx->Sh) cudaFreeHost(ctx->Sh);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -482,11 +554,28 @@ int dampm_step(dampm_ctx* ctx, int nsteps) {
   if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
   ctx->launches = 0;
   ctx->evused = 0;
-  for (int s = 0; s < nsteps; ++s) {
+  int s = 0;
+  if (graph_eligible(ctx)) {
+    // captured on the first eligible call, whatever its length
+    int rc = ensure_graph(ctx);
+    if (rc) return rc;
+    for (; s + kGraphPasses <= nsteps; s += kGraphPasses) {
+      CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+      ctx->it_host += kGraphPasses;
+      ctx->launches += ctx->graph_launches;
+    }
+  }
+  for (; s < nsteps; ++s) {
     int rc = enqueue_pass(ctx);
     if (rc) return rc;
   }
   ev_mark(ctx, 3);
+  return DAMPM_OK;
+}
+
+int dampm_set_graphs(dampm_ctx* ctx, int enable) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  ctx->use_graphs = enable != 0;
   return DAMPM_OK;
 }
 

@@ -78,6 +78,7 @@ def _declare(lib):
         "dampm_download": (C.c_int, [P, C.c_char_p, _DP]),
         "dampm_download_nodal": (C.c_int, [P, C.c_char_p, _DP]),
         "dampm_record_outputs": (C.c_int, [P, C.c_int]),
+        "dampm_set_graphs": (C.c_int, [P, C.c_int]),
         "dampm_ledgers": (C.c_int, [P, _DP]),
         "dampm_ledger_history": (C.c_int, [P, C.c_longlong, C.c_int, _DP]),
         "dampm_set_state": (C.c_int, [P, C.c_longlong, C.POINTER(_DP)] + [_DP] * 5),
@@ -212,6 +213,11 @@ class Solver:
         self.close()
 
     # -- stepping -------------------------------------------------------------
+    def set_graphs(self, enable: bool):
+        """Runs of 16 identical passes replay a CUDA graph (default) or, with
+        False, every pass is launched plainly; the results are the same."""
+        self._check(self.lib.dampm_set_graphs(self.h, 1 if enable else 0))
+
     def step(self, n: int = 1):
         """Enqueues n passes of the loop body (asynchronous)."""
         self._check(self.lib.dampm_step(self.h, int(n)))

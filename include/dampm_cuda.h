@@ -109,8 +109,18 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
  * gpu_offload cadence when MERGE_SPLIT_ON and enabled, sort, P2G + nodal
  * update, G2P + rheology, t += dt).  A pass whose loop condition
  * (fixed ? it < NSTEPS : t < T) fails on the device does nothing, so this
- * never overshoots.  Asynchronous: returns once the work is enqueued. */
+ * never overshoots.  Asynchronous: returns once the work is enqueued.
+ * Runs of 16 identical passes (no merge/split, no recorded outputs, no
+ * event timing) are replayed from a CUDA graph; the graph is captured by the
+ * first call in that mode, whatever its nsteps (a few milliseconds of host
+ * time, nothing runs), and again whenever the buffers or parameters change.
+ * The results are the same as with plain launches.  Called while the
+ * context's stream is itself being captured, it launches plainly. */
 int dampm_step(dampm_ctx* ctx, int nsteps);
+
+/* enable = 0: every pass is launched plainly (no CUDA graph); 1 (default):
+ * graphs as described at dampm_step.  No counterpart in the reference. */
+int dampm_set_graphs(dampm_ctx* ctx, int enable);
 
 /* Runs until the loop condition fails (or max_steps passes), synchronising
  * every `chunk` steps.  *steps_done (may be NULL) receives the count. */
