@@ -56,13 +56,17 @@ struct dampm_ctx {
   long long launches = 0;
   std::string err;
   std::vector<void*> allocs;
-  // CUDA graph of kGraphPasses identical passes, valid while graph_key (the
-  // values the captured launches took by value) is unchanged
+  // CUDA graph of graph_passes passes (kGraphPasses identical ones, or one
+  // merge/split cycle from a given phase), valid while graph_key (the values
+  // the captured launches took by value, the cycle and its phase) is
+  // unchanged
   bool use_graphs = true;
   cudaGraphExec_t graph = nullptr;
+  int graph_passes = 0, graph_phase = 0;
   long long graph_launches = 0;
   unsigned char graph_key[sizeof(Particles) + sizeof(Nodes) + sizeof(Geom) + sizeof(Phys) +
-                          sizeof(long long) + sizeof(int)] = {};
+                          sizeof(long long) + sizeof(int) + sizeof(dampm_ms_params) +
+                          3 * sizeof(int)] = {};
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -267,15 +271,29 @@ int enqueue_pass(dampm_ctx* ctx) {
   return DAMPM_OK;
 }
 
-// Passes that are all alike (no merge/split cadence, no recorded outputs, no
-// event timing) can be replayed from a graph; not while the stream is being
-// captured by the caller.
+// Passes can be replayed from a graph when they repeat: kGraphPasses alike
+// without merge/split, or the call_interval passes of one merge/split cycle
+// (which begin at the same phase of the cycle); not with recorded outputs or
+// event timing, nor while the caller is capturing the stream.
 constexpr int kGraphPasses = 16;
+constexpr int kMaxGraphCycle = 64;
+
+bool ms_cadence(const dampm_ctx* ctx) {
+  return ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 && ctx->ms.call_interval > 0;
+}
+
+// passes per graph (0: no graph) and the cycle phase the graph starts at
+int graph_shape(const dampm_ctx* ctx, int* phase) {
+  *phase = 0;
+  if (!ms_cadence(ctx)) return kGraphPasses;
+  const int L = ctx->ms.call_interval;
+  if (L < 2 || L > kMaxGraphCycle) return 0;
+  *phase = int(ctx->it_host % L);
+  return L;
+}
 
 bool graph_eligible(dampm_ctx* ctx) {
   if (!ctx->use_graphs || ctx->timing || ctx->record) return false;
-  if (ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 && ctx->ms.call_interval > 0)
-    return false;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess ||
       cs != cudaStreamCaptureStatusNone)
@@ -283,7 +301,7 @@ bool graph_eligible(dampm_ctx* ctx) {
   return true;
 }
 
-void graph_key_of(const dampm_ctx* ctx, unsigned char* k) {
+void graph_key_of(const dampm_ctx* ctx, int passes, int phase, unsigned char* k) {
   size_t o = 0;
   auto put = [&](const void* v, size_t n) {
     std::memcpy(k + o, v, n);
@@ -295,13 +313,16 @@ void graph_key_of(const dampm_ctx* ctx, unsigned char* k) {
   put(&ctx->P, sizeof(Phys));
   put(&ctx->cap, sizeof(long long));
   put(&ctx->p2g_grid, sizeof(int));
+  put(&ctx->ms, sizeof(dampm_ms_params));
+  const int cyc[3] = {ms_cadence(ctx) ? 1 : 0, passes, phase};
+  put(cyc, sizeof(cyc));
 }
 
-// (Re)captures kGraphPasses passes unless the graph in hand was captured
-// with the same buffers and parameters.
-int ensure_graph(dampm_ctx* ctx) {
+// (Re)captures `passes` passes from the current pass unless the graph in
+// hand was captured with the same buffers, parameters, cycle and phase.
+int ensure_graph(dampm_ctx* ctx, int passes, int phase) {
   unsigned char key[sizeof(ctx->graph_key)];
-  graph_key_of(ctx, key);
+  graph_key_of(ctx, passes, phase, key);
   if (ctx->graph && std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) return DAMPM_OK;
   if (ctx->graph) {
     cudaGraphExecDestroy(ctx->graph);
@@ -310,7 +331,7 @@ int ensure_graph(dampm_ctx* ctx) {
   const long long it0 = ctx->it_host, l0 = ctx->launches;
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   int rc = DAMPM_OK;
-  for (int k = 0; k < kGraphPasses && rc == DAMPM_OK; ++k) rc = enqueue_pass(ctx);
+  for (int k = 0; k < passes && rc == DAMPM_OK; ++k) rc = enqueue_pass(ctx);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
   ctx->graph_launches = ctx->launches - l0;
@@ -328,6 +349,8 @@ int ensure_graph(dampm_ctx* ctx) {
     return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
   }
   std::memcpy(ctx->graph_key, key, sizeof(key));
+  ctx->graph_passes = passes;
+  ctx->graph_phase = phase;
   return DAMPM_OK;
 }
 
@@ -555,14 +578,32 @@ int dampm_step(dampm_ctx* ctx, int nsteps) {
   ctx->launches = 0;
   ctx->evused = 0;
   int s = 0;
-  if (graph_eligible(ctx)) {
-    // captured on the first eligible call, whatever its length
-    int rc = ensure_graph(ctx);
-    if (rc) return rc;
-    for (; s + kGraphPasses <= nsteps; s += kGraphPasses) {
-      CK(cudaGraphLaunch(ctx->graph, ctx->stream));
-      ctx->it_host += kGraphPasses;
-      ctx->launches += ctx->graph_launches;
+  int phase = 0;
+  const int len = graph_eligible(ctx) ? graph_shape(ctx, &phase) : 0;
+  if (len > 0) {
+    bool aligned = true;
+    if (ms_cadence(ctx)) {
+      // a graph of this cycle in hand: plain passes up to its phase
+      if (ctx->graph && ctx->graph_passes == len) {
+        unsigned char key[sizeof(ctx->graph_key)];
+        graph_key_of(ctx, len, ctx->graph_phase, key);
+        if (std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) phase = ctx->graph_phase;
+      }
+      for (; s < nsteps && int(ctx->it_host % len) != phase; ++s) {
+        int rc = enqueue_pass(ctx);
+        if (rc) return rc;
+      }
+      aligned = int(ctx->it_host % len) == phase;
+    }
+    if (aligned) {
+      // captured on the first eligible call, whatever its length
+      int rc = ensure_graph(ctx, len, phase);
+      if (rc) return rc;
+      for (; s + len <= nsteps; s += len) {
+        CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+        ctx->it_host += len;
+        ctx->launches += ctx->graph_launches;
+      }
     }
   }
   for (; s < nsteps; ++s) {

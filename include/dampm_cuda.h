@@ -110,12 +110,14 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
  * update, G2P + rheology, t += dt).  A pass whose loop condition
  * (fixed ? it < NSTEPS : t < T) fails on the device does nothing, so this
  * never overshoots.  Asynchronous: returns once the work is enqueued.
- * Runs of 16 identical passes (no merge/split, no recorded outputs, no
- * event timing) are replayed from a CUDA graph; the graph is captured by the
- * first call in that mode, whatever its nsteps (a few milliseconds of host
- * time, nothing runs), and again whenever the buffers or parameters change.
- * The results are the same as with plain launches.  Called while the
- * context's stream is itself being captured, it launches plainly. */
+ * Without recorded outputs or event timing, passes are replayed from a CUDA
+ * graph: 16 at a time, or with merge/split one cycle of call_interval passes
+ * at a time from the cycle phase the graph was captured at (passes before
+ * that phase run plainly).  The graph is captured by the first call in that
+ * mode, whatever its nsteps (a few milliseconds of host time, nothing runs),
+ * and again whenever the buffers or parameters change.  The results are the
+ * same as with plain launches.  Called while the context's stream is itself
+ * being captured, it launches plainly. */
 int dampm_step(dampm_ctx* ctx, int nsteps);
 
 /* enable = 0: every pass is launched plainly (no CUDA graph); 1 (default):

@@ -47,3 +47,23 @@ def test_graph_recaptured_when_buffers_change(cuda_lib):
             out.append({k: s.download(k) for k in FIELDS})
     for k in FIELDS:
         np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
+
+
+@pytest.mark.gpu
+def test_graph_merge_split_cycles_bitwise(cuda_lib):
+    """With merge/split every 10 passes, whole cycles replay from a graph
+    captured at the phase of the first call; calls that start at another
+    phase run plainly up to it."""
+    d = scenarios.mudflow(N=256, merge_split=True)
+    out = []
+    for graphs in (True, False):
+        with Solver(d, merge_split=True) as s:
+            s.set_graphs(graphs)
+            for n in (5, 23, 3, 31):  # phases 0, 5, 8, 1 at the calls
+                s.step(n)
+            st = s.status()
+            assert st["it"] == 62
+            out.append((st, {k: s.download(k) for k in FIELDS + ("label",)}))
+    assert out[0][0]["np"] == out[1][0]["np"] and out[0][0]["t"] == out[1][0]["t"]
+    for k in FIELDS + ("label",):
+        np.testing.assert_array_equal(out[0][1][k], out[1][1][k], err_msg=k)
