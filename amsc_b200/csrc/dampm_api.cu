@@ -318,6 +318,15 @@ void graph_key_of(const dampm_ctx* ctx, int passes, int phase, unsigned char* k)
   put(cyc, sizeof(cyc));
 }
 
+// A stream that cannot be captured (or a graph that cannot be built): the
+// context launches plainly from then on.
+int graphs_off(dampm_ctx* ctx) {
+  cudaGetLastError();  // the capture's error is not the step's
+  ctx->use_graphs = false;
+  ctx->graph = nullptr;
+  return DAMPM_OK;
+}
+
 // (Re)captures `passes` passes from the current pass unless the graph in
 // hand was captured with the same buffers, parameters, cycle and phase.
 int ensure_graph(dampm_ctx* ctx, int passes, int phase) {
@@ -329,7 +338,8 @@ int ensure_graph(dampm_ctx* ctx, int passes, int phase) {
     ctx->graph = nullptr;
   }
   const long long it0 = ctx->it_host, l0 = ctx->launches;
-  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return graphs_off(ctx);
   int rc = DAMPM_OK;
   for (int k = 0; k < passes && rc == DAMPM_OK; ++k) rc = enqueue_pass(ctx);
   cudaGraph_t g = nullptr;
@@ -341,13 +351,13 @@ int ensure_graph(dampm_ctx* ctx, int passes, int phase) {
     if (g) cudaGraphDestroy(g);
     return rc;
   }
-  if (e != cudaSuccess) return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return graphs_off(ctx);
+  }
   const cudaError_t ei = cudaGraphInstantiate(&ctx->graph, g, 0);
   cudaGraphDestroy(g);
-  if (ei != cudaSuccess) {
-    ctx->graph = nullptr;
-    return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
-  }
+  if (ei != cudaSuccess) return graphs_off(ctx);
   std::memcpy(ctx->graph_key, key, sizeof(key));
   ctx->graph_passes = passes;
   ctx->graph_phase = phase;
@@ -599,7 +609,7 @@ int dampm_step(dampm_ctx* ctx, int nsteps) {
       // captured on the first eligible call, whatever its length
       int rc = ensure_graph(ctx, len, phase);
       if (rc) return rc;
-      for (; s + len <= nsteps; s += len) {
+      for (; ctx->graph && s + len <= nsteps; s += len) {
         CK(cudaGraphLaunch(ctx->graph, ctx->stream));
         ctx->it_host += len;
         ctx->launches += ctx->graph_launches;

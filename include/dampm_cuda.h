@@ -117,7 +117,8 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
  * mode, whatever its nsteps (a few milliseconds of host time, nothing runs),
  * and again whenever the buffers or parameters change.  The results are the
  * same as with plain launches.  Called while the context's stream is itself
- * being captured, it launches plainly. */
+ * being captured, it launches plainly; a stream that cannot be captured, or
+ * a graph that cannot be built, turns graphs off for the context. */
 int dampm_step(dampm_ctx* ctx, int nsteps);
 
 /* enable = 0: every pass is launched plainly (no CUDA graph); 1 (default):

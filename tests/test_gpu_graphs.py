@@ -67,3 +67,18 @@ def test_graph_merge_split_cycles_bitwise(cuda_lib):
     assert out[0][0]["np"] == out[1][0]["np"] and out[0][0]["t"] == out[1][0]["t"]
     for k in FIELDS + ("label",):
         np.testing.assert_array_equal(out[0][1][k], out[1][1][k], err_msg=k)
+
+
+@pytest.mark.gpu
+def test_graph_falls_back_on_an_uncapturable_stream(cuda_lib):
+    """On the legacy default stream (handle 1), which CUDA cannot capture, the
+    context launches plainly and gives the same state."""
+    d = scenarios.dam_break_flat(nsteps=200)
+    out = []
+    for stream in (None, 1):
+        with Solver(d, stream=stream) as s:
+            s.step(40)
+            assert s.status()["it"] == 40
+            out.append({k: s.download(k) for k in FIELDS})
+    for k in FIELDS:
+        np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
