@@ -10,7 +10,6 @@
 // (an OpenMP `target data` region, a framework's memory pool) or whose step
 // loop must not stall the device (cudaFree synchronises it) can call it on
 // every step.
-#include <atomic>
 #include <climits>
 
 #include <cuda_runtime.h>
@@ -27,15 +26,11 @@ constexpr int kCflThreads = 256;
 // Partial-maximum slots: up to 8 blocks per SM of a 148-SM B200; larger
 // particle counts are covered by the grid-stride loop.
 constexpr int kCflMaxBlocks = 8 * 148;
-constexpr int kMaxDevices = 64;
 
 // 3 ordered keys (max |vpx|, max |vpy|, max hp) per block: 28,416 bytes.
 // Every slot the final kernel reads was written by the same call's first
 // kernel, so nothing here needs to start at zero.
 static __device__ __align__(256) unsigned long long g_cfl_scratch[3 * kCflMaxBlocks];
-
-// Scratch address per device, looked up by the first call on that device.
-std::atomic<unsigned long long*> g_scratch_of[kMaxDevices];
 
 __device__ __forceinline__ void block_max3(unsigned long long& m0,
                                            unsigned long long& m1,
@@ -112,20 +107,33 @@ __global__ void __launch_bounds__(kCflThreads)
   }
 }
 
-int scratch_for_current_device(unsigned long long** out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess) return DAMPM_ERR_CUDA;
-  if (dev < 0 || dev >= kMaxDevices) return DAMPM_ERR_DEVICE;
-  unsigned long long* p = g_scratch_of[dev].load(std::memory_order_acquire);
-  if (!p) {
-    void* q = nullptr;
-    if (cudaGetSymbolAddress(&q, g_cfl_scratch) != cudaSuccess || !q)
-      return DAMPM_ERR_CUDA;
-    p = static_cast<unsigned long long*>(q);
-    g_scratch_of[dev].store(p, std::memory_order_release);
+// The scratch array's device address in the current context.  The address
+// belongs to a CUDA context, not to a device number: it changes after
+// cudaDeviceReset or when another context is made current on the device, so
+// it is looked up on every call (a host-side query that allocates nothing).
+// The first lookup in a context may load this library's kernels into it,
+// which is why the first call should come before any stream capture.
+int scratch_for_current_context(unsigned long long** out) {
+  void* q = nullptr;
+  if (cudaGetSymbolAddress(&q, g_cfl_scratch) != cudaSuccess || !q) {
+    cudaGetLastError();  // the lookup's error is reported by the return code
+    return DAMPM_ERR_CUDA;
   }
-  *out = p;
+  *out = static_cast<unsigned long long*>(q);
   return DAMPM_OK;
+}
+
+// A stream created on another device than the current one would receive the
+// current device's scratch address: refused.
+int check_stream_device(cudaStream_t st) {
+  if (st == nullptr) return DAMPM_OK;  // the legacy stream of the current device
+  int dev = -1, sdev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DAMPM_ERR_CUDA;
+  if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+    cudaGetLastError();
+    return DAMPM_ERR_CUDA;
+  }
+  return sdev == dev ? DAMPM_OK : DAMPM_ERR_DEVICE;
 }
 
 }  // namespace
@@ -138,10 +146,12 @@ extern "C" int dampm_cfl_dt_noalloc(const double* vpx, const double* vpy,
   if (!(hx > 0.0) || !(hy > 0.0)) return DAMPM_ERR_ARG;
   if (np < 1) return DAMPM_ERR_ARG;  // the maxima of no particles are undefined
   if (np > (long long)INT_MAX) return DAMPM_ERR_CAPACITY;
-  unsigned long long* part = nullptr;
-  int rc = scratch_for_current_device(&part);
-  if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  int rc = check_stream_device(st);
+  if (rc) return rc;
+  unsigned long long* part = nullptr;
+  rc = scratch_for_current_context(&part);
+  if (rc) return rc;
   const long long want = (np + kCflThreads - 1) / kCflThreads;
   const int nb = (int)(want < kCflMaxBlocks ? want : kCflMaxBlocks);
   k_cfl_partial<<<nb, kCflThreads, 0, st>>>(vpx, vpy, hp, np, part);

@@ -225,15 +225,23 @@ int dampm_json_free(dampm_json* j);
  * vpx, vpy, hp: np device values each (1 <= np <= 2^31-1; np beyond that
  * returns DAMPM_ERR_CAPACITY, np < 1 DAMPM_ERR_ARG).  out: 5 doubles in
  * device-writable memory, written asynchronously on cuda_stream (NULL = the
- * legacy default stream, which must belong to the current device):
+ * legacy default stream of the current device; a non-NULL stream must
+ * belong to the current device, else DAMPM_ERR_DEVICE):
  * {CFL*min(hx,hy)/(1e-2+cel), cel, max|vpx|, max|vpy|, max hp} with
  * cel = |max(sqrt(g*hmax)+max|vpx|, sqrt(g*hmax)+max|vpy|)|, the step's own
  * dt formula (main/optim_par.cpp:289-304).
  *
+ * Non-finite input: any NaN in vpx or vpy, or a NaN with a clear sign bit in
+ * hp, makes the maxima and dt NaN (a sign-set NaN in hp is ignored).  The
+ * reference's std::max_element keeps a NaN only where it is the first
+ * element, so on a diverged state the two differ; dt is then meaningless
+ * either way.
+ *
  * The reduction scratch is a fixed 28,416-byte array inside this library,
- * one copy per device; nothing in it has to start at zero.  The first call
- * on a device looks up that array's address (cudaGetSymbolAddress, with
- * that device current), so make it before any stream capture.  Calls whose
+ * one copy per device; nothing in it has to start at zero.  Its address is
+ * looked up in the current context on every call (cudaGetSymbolAddress, a
+ * host-side query); the first lookup in a context may load the library's
+ * kernels, so make the first call before any stream capture.  Calls whose
  * work can overlap on one device (other streams, other host threads) share
  * the scratch and race: order them on one stream.  Returns DAMPM_ERR_CUDA
  * if the lookup or a launch fails. */

@@ -29,9 +29,21 @@ def available() -> bool:
     return os.path.exists(OPTIM_PAR) and os.path.exists(MS_HARNESS)
 
 
-def build(ref_root: str = "/root/reference") -> bool:
+def reference_root() -> Optional[str]:
+    """The reference checkout: $DAMPM_REFERENCE, else a checkout named
+    ``reference`` beside this repository; None when neither holds main/."""
+    cands = [os.environ.get("DAMPM_REFERENCE", ""),
+             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "main")):
+            return os.path.abspath(c)
+    return None
+
+
+def build(ref_root: Optional[str] = None) -> bool:
     """Builds _ref/ from the reference sources when they are present."""
-    if not os.path.isdir(os.path.join(ref_root, "main")):
+    ref_root = ref_root or reference_root()
+    if ref_root is None:
         return available()
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
     return available()

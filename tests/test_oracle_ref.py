@@ -38,7 +38,8 @@ def test_bench_generator_matches_shipped_fixtures():
     import json
     import os
     for N in (1000, 3000, 10000, 30000):
-        path = f"/root/reference/data/performance/DATA_bench_{N}.json"
+        path = os.path.join(refrun.reference_root() or "", "data", "performance",
+                            f"DATA_bench_{N}.json")
         if not os.path.exists(path):
             pytest.skip("fixtures absent")
         ref = json.load(open(path))

@@ -73,6 +73,29 @@ def test_cfl_dt_noalloc_matches_step_dt(cuda_lib):
                                                         st["hp"][:m], g, CFL, hx, hy)
 
 
+def test_cfl_dt_noalloc_leaves_device_memory_alone(cuda_lib):
+    """The point of the entry point: a call allocates and frees nothing, so the
+    device's free memory is the same before and after a run of calls."""
+    import torch
+    f = _bind(cuda_lib)
+    n = 3_000_000  # more blocks than the scratch holds partials for
+    v = torch.rand(n, dtype=torch.float64, device="cuda")
+    out = torch.empty(5, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert f(v.data_ptr(), v.data_ptr(), v.data_ptr(), n, 9.81, 0.4, 0.5, 0.5,
+             out.data_ptr(), stream) == 0  # first call in this context
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(50):
+        assert f(v.data_ptr(), v.data_ptr(), v.data_ptr(), n, 9.81, 0.4, 0.5, 0.5,
+                 out.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    host = v.cpu().numpy()
+    assert tuple(out.cpu().numpy()) == _host_dt(host, host, host, 9.81, 0.4, 0.5, 0.5)
+
+
 def test_cfl_dt_noalloc_rejects_bad_sizes(cuda_lib):
     import torch
     f = _bind(cuda_lib)
