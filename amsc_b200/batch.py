@@ -159,13 +159,16 @@ class Batch:
                 "passes": 3 * passes * len(trials), "trials": trials}
 
     def states(self) -> Dict[int, Dict[str, float]]:
-        """Loop state of every live scenario, one synchronisation."""
+        """Loop state of every live scenario, one synchronisation.  "failed":
+        the scenario's state diverged (non-finite or negative) and its status
+        word stopped it; the others are unaffected."""
         cap = max(len(self.np), 1)
         hs, run, its = (C.c_int * cap)(), (C.c_int * cap)(), (C.c_int * cap)()
         ts = (C.c_double * cap)()
         n = C.c_int()
         self._check(self.lib.dampm_batch_states(self.h, cap, hs, run, its, ts, C.byref(n)))
-        return {hs[k]: {"running": bool(run[k]), "it": its[k], "t": ts[k]}
+        return {hs[k]: {"running": run[k] == 1, "failed": run[k] < 0, "it": its[k],
+                        "t": ts[k]}
                 for k in range(n.value)}
 
     def usage(self) -> Dict[str, int]:

@@ -47,12 +47,19 @@ struct dampm_batch {
   int next_handle = 0;
   // device
   int precision = DAMPM_FP64;
-  ParticlesT<double> p64[2]{};  // FP64: the two halves of the double buffer
+  // the two halves of the double buffer of the moving particle fields: each
+  // pass's G2P reads half `cur` and writes the other, and so does a
+  // compaction; the fields that only an upload uses are shared
+  ParticlesT<double> p64[2]{};  // FP64
   ParticlesT<float> p32[2]{};   // FP32 form
   double* Z[2] = {nullptr, nullptr};
-  int cur = 0;
+  int cur = 0;  // half holding the particles; also the terrain's half
+  int zcur = 0;
   void* vvL = nullptr;  // pairs (vvxL, vvyL) of the precision's real type
-  int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr;
+  double* stage = nullptr;  // one field in reference order, for downloads
+  unsigned long long* sortbuf = nullptr;  // 2 x capacity: crowded cells' order
+  int *count = nullptr, *start = nullptr, *perm = nullptr;
+  int* skey = nullptr;  // the cell key of each sorted position
   int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr, *cbig = nullptr;
   int* cmid = nullptr;  // cells with more than 16 particles
   int* ustart = nullptr;
@@ -70,10 +77,12 @@ struct dampm_batch {
   long long launches = 0;
   // tuning: P2G units per CTA and the weight of a column in the unit plan
   int units_per_cta = kUnitsPerCta, col_weight = kColWeight;
-  // passes captured in a CUDA graph, replayed while the layout holds
-  int use_graphs = 1, graph_passes = 0;
-  bool graph_dirty = true;
-  cudaGraphExec_t graph = nullptr;
+  // passes captured in a CUDA graph, replayed while the layout holds; one
+  // graph per half the passes start from (an odd pass count alternates)
+  int use_graphs = 1;
+  int graph_passes[2] = {0, 0};
+  bool graph_dirty[2] = {true, true};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
   std::vector<void*> allocs;
   std::string err;
 };
@@ -115,43 +124,60 @@ ParticlesT<double>* halves<double>(dampm_batch* b) { return b->p64; }
 template <>
 ParticlesT<float>* halves<float>(dampm_batch* b) { return b->p32; }
 
-const int* keys_of(dampm_batch* b) {
-  return b->precision == DAMPM_FP32 ? b->p32[b->cur].key : b->p64[b->cur].key;
-}
-
-// the persistent per-particle arrays of one half of the double buffer
+// the particle arrays of both halves: the moving fields of each half, and
+// the fields only an upload uses (Ap, Fb, label, level) shared
 template <class R>
-int alloc_particles(dampm_batch* b, ParticlesT<R>& p) {
-  R** f[] = {&p.x,  &p.y,  &p.vpx, &p.vpy, &p.hp, &p.F11, &p.F12,
-             &p.F22, &p.Mp, &p.Vp,  &p.H,   &p.Ap, &p.Fbx, &p.Fby};
+int alloc_particles(dampm_batch* b, ParticlesT<R>* h) {
+  for (int k = 0; k < 2; ++k) {
+    MovingRefs<R> m = moving_refs(h[k]);
+    for (int f = 0; f < kMovingR; ++f) {
+      if (m.r[f] == &h[k].vpx_dx || m.r[f] == &h[k].vpx_dy || m.r[f] == &h[k].vpy_dx ||
+          m.r[f] == &h[k].vpy_dy)
+        continue;  // no gradients in a batch (no merge/split)
+      int rc = balloc(b, m.r[f], size_t(b->P_cap));
+      if (rc) return rc;
+    }
+    for (int f = 0; f < kMovingI; ++f) {
+      int rc = balloc(b, m.i[f], size_t(b->P_cap));
+      if (rc) return rc;
+    }
+    for (int f = 0; f < kMovingV; ++f) {
+      int rc = balloc(b, m.v[f], size_t(b->P_cap));
+      if (rc) return rc;
+    }
+  }
+  R** f[] = {&h[0].Ap, &h[0].Fbx, &h[0].Fby};
   for (R** q : f) {
     int rc = balloc(b, q, size_t(b->P_cap));
     if (rc) return rc;
   }
-  V2<R>** f2[] = {&p.mp, &p.qf, &p.xe, &p.qg};
-  for (V2<R>** q : f2) {
-    int rc = balloc(b, q, size_t(b->P_cap));
-    if (rc) return rc;
-  }
-  int** fi[] = {&p.label, &p.level, &p.key};
+  int** fi[] = {&h[0].label, &h[0].level};
   for (int** q : fi) {
     int rc = balloc(b, q, size_t(b->P_cap));
     if (rc) return rc;
   }
+  h[1].Ap = h[0].Ap;
+  h[1].Fbx = h[0].Fbx;
+  h[1].Fby = h[0].Fby;
+  h[1].label = h[0].label;
+  h[1].level = h[0].level;
   return DAMPM_OK;
 }
 
 template <class R>
 ParticlesT<R> shifted(const ParticlesT<R>& p, long long off) {
   ParticlesT<R> q = p;
-  R** f[] = {&q.x,  &q.y,  &q.vpx, &q.vpy, &q.hp, &q.F11, &q.F12,
-             &q.F22, &q.Mp, &q.Vp,  &q.H,   &q.Ap, &q.Fbx, &q.Fby};
+  MovingRefs<R> m = moving_refs(q);
+  for (R** d : m.r)
+    if (*d) *d += off;
+  for (int** d : m.i)
+    if (*d) *d += off;
+  for (V2<R>** d : m.v)
+    if (*d) *d += off;
+  R** f[] = {&q.Ap, &q.Fbx, &q.Fby};
   for (R** d : f)
     if (*d) *d += off;
-  V2<R>** f2[] = {&q.mp, &q.qf, &q.xe, &q.qg};
-  for (V2<R>** d : f2)
-    if (*d) *d += off;
-  int** fi[] = {&q.label, &q.level, &q.key};
+  int** fi[] = {&q.label, &q.level};
   for (int** d : fi)
     if (*d) *d += off;
   return q;
@@ -184,9 +210,14 @@ int upload_tables(dampm_batch* b) {
   Scalars g{};
   g.np = int(b->P_tot);
   g.active = 1;
+  // the next sort scans every cell of the new layout
+  g.krange[0] = 0x7fffffff;
+  g.krange[1] = -1;
+  g.knext[0] = 0;
+  g.knext[1] = int(std::max<long long>(b->C_tot, 1)) - 1;
   BCK(cudaMemcpyAsync(b->Sg, &g, sizeof(Scalars), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaStreamSynchronize(b->stream));  // host vectors die here
-  b->graph_dirty = true;  // launch sizes or buffers changed
+  b->graph_dirty[0] = b->graph_dirty[1] = true;  // launch sizes or buffers changed
   return DAMPM_OK;
 }
 
@@ -205,27 +236,30 @@ int read_scalars(dampm_batch* b) {
 }
 
 // One pass of every live scenario: kPassLaunches kernel launches.
-constexpr int kPassLaunches = 16;
+constexpr int kPassLaunches = 13;
 int enqueue_pass(dampm_batch* b) {
   cudaStream_t st = b->stream;
   const int nscn = int(b->scns.size());
-  const int ntiles = int((b->C_tot + kScanTile - 1) / kScanTile);
+  const int ncell = int(std::max<long long>(b->C_tot, 1));
+  const int ntiles = (ncell + kScanTile - 1) / kScanTile;
+  const int nxt = 1 - b->cur;
+  const int* key = b->precision == DAMPM_FP32 ? b->p32[b->cur].key : b->p64[b->cur].key;
+  const int* slot = b->precision == DAMPM_FP32 ? b->p32[b->cur].slot : b->p64[b->cur].slot;
+  const int* idx = b->precision == DAMPM_FP32 ? b->p32[b->cur].idx : b->p64[b->cur].idx;
   k_b_step_begin<<<1, 1024, 0, st>>>(b->scn, b->S, nscn, b->Sg);
   const int gp = grid_blocks(b->P_tot, 256);
-  k_count<<<gp, 256, 0, st>>>(keys_of(b), b->count, b->slot, b->Sg);
-  k_scan_tiles<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(b->count, int(b->C_tot),
-                                                               b->tile_sum, b->Sg);
-  k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(b->tile_sum, ntiles, b->Sg);
-  k_list_reset<<<1, 1, 0, st>>>(b->clist_n, b->Sg);
-  k_scan_apply<<<std::max(ntiles, 1), kScanThreads, 0, st>>>(
-      b->count, int(b->C_tot), b->tile_sum, b->start, b->clist, b->clist_n, b->Sg);
-  k_scatter<<<gp, 256, 0, st>>>(keys_of(b), b->slot, b->start, b->perm, b->Sg);
-  k_segment_order<<<148 * 4, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
+  // the counting sort of every scenario at once (G2P counted the keys)
+  k_scan_sums<<<ntiles, kScanThreads, 0, st>>>(b->count, ncell, b->tile_sum, b->clist_n,
+                                               b->Sg, 1);
+  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(b->count, ncell, b->tile_sum, b->start,
+                                                b->clist, b->clist_n, b->Sg, 1);
+  k_scatter<<<gp, 256, 0, st>>>(key, slot, b->start, b->perm, b->skey, b->Sg);
+  k_segment_order<<<148 * 4, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm, idx,
                                             b->cmid, b->Sg);
-  k_segment_order_mid<<<148 * 8, 256, 0, st>>>(b->start, b->cmid, b->clist_n, b->perm,
+  k_segment_order_mid<<<148 * 8, 256, 0, st>>>(b->start, b->cmid, b->clist_n, b->perm, idx,
                                                 b->cbig, b->Sg);
-  k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
-                                            b->slot, b->Sg);
+  k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm, idx,
+                                            b->sortbuf, b->P_cap, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
       b->start, b->scn, b->S, b->strip_scn, b->Sg, b->units_per_cta * b->p2g_grid,
       b->col_weight, b->ustart, b->upex, b->uplan, b->strip_n);
@@ -243,14 +277,15 @@ int enqueue_pass(dampm_batch* b) {
   k_b_ledger<<<nscn, 256, 0, st>>>(b->led_part, b->scn_units, b->scn, b->S, nscn,
                                    b->Sg);
   if (b->precision == DAMPM_FP32)
-    launch_b_g2p<float>(b->nblk, st, b->p32[b->cur], static_cast<const float2*>(b->vvL),
-                        b->Z[b->cur], b->scn, b->S,
-                        b->gblk, b->Sg);
+    launch_b_g2p<float>(b->nblk, st, b->p32[b->cur], b->p32[nxt], b->perm, b->skey,
+                        static_cast<const float2*>(b->vvL), b->Z[b->zcur], b->scn, b->S,
+                        b->gblk, b->Sg, b->count);
   else
-    launch_b_g2p<double>(b->nblk, st, b->p64[b->cur], static_cast<const double2*>(b->vvL),
-                         b->Z[b->cur], b->scn, b->S,
-                         b->gblk, b->Sg);
+    launch_b_g2p<double>(b->nblk, st, b->p64[b->cur], b->p64[nxt], b->perm, b->skey,
+                         static_cast<const double2*>(b->vvL), b->Z[b->zcur], b->scn, b->S,
+                         b->gblk, b->Sg, b->count);
   k_b_step_end<<<1, 1024, 0, st>>>(b->scn, b->S, nscn);
+  b->cur = nxt;
   b->launches += kPassLaunches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
@@ -284,10 +319,31 @@ int upload_scenario(dampm_batch* b, const Scn& d, int pos, long long np,
   // not keep, so Z stands in for them)
   launch_init_particles<R>(grid_blocks(np, 256), 256, st, p, Zs, Zs, Zs, d.G, d.P,
                            b->S + pos, int(np), d.c_off);
+  // the new keys join the counts the last pass left for the next sort
+  k_count_n<<<grid_blocks(np, 256), 256, 0, st>>>(p.key, b->count, p.slot, int(np));
   launch_prep<R>(grid_blocks(np, 256), 256, st, p, Zs, d.G, d.P, b->S + pos, 0);
-  b->launches += 2;
+  b->launches += 3;
   BCK(cudaGetLastError());
   return DAMPM_OK;
+}
+
+// out[idx[j]] = a[j] over one scenario's n particles (idx: its reference
+// index), converted to double
+template <class R>
+__global__ void k_b_to_ref(const R* __restrict__ a, const int* __restrict__ idx,
+                           double* __restrict__ out, int n) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    out[idx[j]] = double(a[j]);
+}
+
+template <class R>
+__global__ void k_b_pair_to_ref(const V2<R>* __restrict__ a, int half,
+                                const int* __restrict__ idx, double* __restrict__ out,
+                                int n) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const V2<R> v = a[j];
+    out[idx[j]] = double(half ? v.y : v.x);
+  }
 }
 
 template <class R>
@@ -309,20 +365,16 @@ int download_field(dampm_batch* b, const Scn& d, const std::string& f, double* o
   else if (f == "mom_px" || f == "mom_py") pair_half = f == "mom_px" ? 0 : 1;
   if (!src && pair_half < 0)
     return bfail(b, DAMPM_ERR_UNKNOWN_FIELD, "unknown batch field " + f);
-  R* hout = reinterpret_cast<R*>(out);
-  std::vector<R> tmp;
-  if (sizeof(R) != sizeof(double)) {
-    tmp.resize(size_t(d.np));
-    hout = tmp.data();
-  }
+  if (d.np == 0) return DAMPM_OK;
+  const int gp = grid_blocks(d.np, 256);
   if (pair_half >= 0)
-    BCK(download_pair_half(hout, p.mp, pair_half, d.np, b->stream));
+    k_b_pair_to_ref<R><<<gp, 256, 0, b->stream>>>(p.mp, pair_half, p.idx, b->stage, d.np);
   else
-    BCK(cudaMemcpyAsync(hout, src, sizeof(R) * size_t(d.np), cudaMemcpyDeviceToHost,
-                        b->stream));
+    k_b_to_ref<R><<<gp, 256, 0, b->stream>>>(src, p.idx, b->stage, d.np);
+  BCK(cudaGetLastError());
+  BCK(cudaMemcpyAsync(out, b->stage, sizeof(double) * size_t(d.np), cudaMemcpyDeviceToHost,
+                      b->stream));
   BCK(cudaStreamSynchronize(b->stream));
-  if (sizeof(R) != sizeof(double))
-    for (int i = 0; i < d.np; ++i) out[i] = double(tmp[i]);
   return DAMPM_OK;
 }
 
@@ -357,9 +409,10 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
     }
     b->own_stream = true;
   }
-  int rc = f32 ? alloc_particles(b, b->p32[0]) : alloc_particles(b, b->p64[0]);
-  if (!rc) rc = f32 ? alloc_particles(b, b->p32[1]) : alloc_particles(b, b->p64[1]);
+  int rc = f32 ? alloc_particles(b, b->p32) : alloc_particles(b, b->p64);
   const size_t nn = size_t(node_cap), pc = size_t(particle_cap);
+  rc = rc ? rc : balloc(b, &b->stage, pc);
+  rc = rc ? rc : balloc(b, &b->sortbuf, 2 * pc);
   rc = rc ? rc : balloc(b, &b->Z[0], nn);
   rc = rc ? rc : balloc(b, &b->Z[1], nn);
   rc = rc ? rc : balloc(b, reinterpret_cast<unsigned char**>(&b->vvL), 2 * nn * rsz);
@@ -369,8 +422,8 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   rc = rc ? rc : balloc(b, &b->clist, nn + 4);
   rc = rc ? rc : balloc(b, &b->clist_n, 4);
   rc = rc ? rc : balloc(b, &b->tile_sum, nn / kScanTile + 2);
-  rc = rc ? rc : balloc(b, &b->slot, pc);
   rc = rc ? rc : balloc(b, &b->perm, pc);
+  rc = rc ? rc : balloc(b, &b->skey, pc);
   rc = rc ? rc : balloc(b, &b->cbig, pc / 256 + 4);
   rc = rc ? rc : balloc(b, &b->cmid, pc / 17 + 4);
   const size_t us = size_t(b->USEG_cap);
@@ -416,7 +469,8 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
 int dampm_batch_destroy(dampm_batch* b) {
   if (!b) return DAMPM_ERR_ARG;
   if (b->stream) cudaStreamSynchronize(b->stream);
-  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (cudaGraphExec_t g : b->graph)
+    if (g) cudaGraphExecDestroy(g);
   for (void* q : b->allocs) cudaFree(q);
   if (b->Sh) cudaFreeHost(b->Sh);
   if (b->own_stream) cudaStreamDestroy(b->stream);
@@ -466,7 +520,7 @@ int dampm_batch_add(dampm_batch* b, const dampm_grid* grid, const dampm_params* 
   const int pos = int(b->scns.size());
   // particles and terrain into the current half
   cudaStream_t st = b->stream;
-  double* Zs = b->Z[b->cur] + d.n_off;
+  double* Zs = b->Z[b->zcur] + d.n_off;
   BCK(cudaMemcpyAsync(Zs, Z, sizeof(double) * size_t(h.nn), cudaMemcpyHostToDevice, st));
   Scalars s0{};
   s0.fresh = 1;
@@ -539,7 +593,11 @@ int dampm_batch_compact(dampm_batch* b) {
     S.push_back(b->Sh[s]);
     keep.push_back(h);
   }
-  const int nxt = 1 - b->cur;
+  const int nxt = 1 - b->cur, znxt = 1 - b->zcur;
+  // the counts of the moved keys, for the next sort (the whole array: cells
+  // beyond the new total may hold counts of removed scenarios, which a later
+  // scenario's cells would otherwise inherit)
+  BCK(cudaMemsetAsync(b->count, 0, sizeof(int) * size_t(b->N_cap + 4), b->stream));
   if (!mv.empty()) {
     BCK(cudaMemcpyAsync(b->mblk, mv.data(), sizeof(int4) * mv.size(),
                         cudaMemcpyHostToDevice, b->stream));
@@ -548,11 +606,14 @@ int dampm_batch_compact(dampm_batch* b) {
     else
       launch_b_move<double>(int(mv.size()), b->stream, b->p64[nxt], b->p64[b->cur],
                             b->mblk);
+    const int* key = b->precision == DAMPM_FP32 ? b->p32[nxt].key : b->p64[nxt].key;
+    int* slot = b->precision == DAMPM_FP32 ? b->p32[nxt].slot : b->p64[nxt].slot;
+    k_count_n<<<grid_blocks(P, 256), 256, 0, b->stream>>>(key, b->count, slot, int(P));
   }
   if (!nm.empty()) {
     BCK(cudaMemcpyAsync(b->nmove, nm.data(), sizeof(int4) * nm.size(),
                         cudaMemcpyHostToDevice, b->stream));
-    k_b_move_nodes<<<int(nm.size()), kG2PThreads, 0, b->stream>>>(b->Z[nxt], b->Z[b->cur],
+    k_b_move_nodes<<<int(nm.size()), kG2PThreads, 0, b->stream>>>(b->Z[znxt], b->Z[b->zcur],
                                                                   b->nmove);
   }
   for (size_t s = 0; s < S.size(); ++s) b->Sh[s] = S[s];
@@ -561,6 +622,7 @@ int dampm_batch_compact(dampm_batch* b) {
                         b->stream));
   BCK(cudaGetLastError());
   b->cur = nxt;
+  b->zcur = znxt;
   b->scns = keep;
   b->P_tot = P;
   b->N_tot = N;
@@ -582,17 +644,20 @@ int dampm_batch_step(dampm_batch* b, int nsteps) {
   }
   // nsteps passes as one CUDA graph: captured after any change of layout or
   // pass count, replayed otherwise (the launches' sizes and pointers depend
-  // only on the layout; every other change lives in device memory)
-  if (b->graph_dirty || b->graph_passes != nsteps || !b->graph) {
-    if (b->graph) {
-      cudaGraphExecDestroy(b->graph);
-      b->graph = nullptr;
+  // only on the layout and on the half the passes start from; every other
+  // change lives in device memory)
+  const int h = b->cur;
+  if (b->graph_dirty[h] || b->graph_passes[h] != nsteps || !b->graph[h]) {
+    if (b->graph[h]) {
+      cudaGraphExecDestroy(b->graph[h]);
+      b->graph[h] = nullptr;
     }
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const long long l0 = b->launches;
     int rc = DAMPM_OK;
     for (int k = 0; k < nsteps && rc == DAMPM_OK; ++k) rc = enqueue_pass(b);
     b->launches = l0;
+    b->cur = h;  // nothing ran yet
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) {
@@ -600,13 +665,17 @@ int dampm_batch_step(dampm_batch* b, int nsteps) {
       return rc;
     }
     if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
-    const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+    const cudaError_t ei = cudaGraphInstantiate(&b->graph[h], g, 0);
     cudaGraphDestroy(g);
-    if (ei != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
-    b->graph_passes = nsteps;
-    b->graph_dirty = false;
+    if (ei != cudaSuccess) {
+      b->graph[h] = nullptr;
+      return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
+    }
+    b->graph_passes[h] = nsteps;
+    b->graph_dirty[h] = false;
   }
-  BCK(cudaGraphLaunch(b->graph, b->stream));
+  BCK(cudaGraphLaunch(b->graph[h], b->stream));
+  if (nsteps & 1) b->cur = 1 - h;
   b->launches += (long long)kPassLaunches * nsteps;
   return DAMPM_OK;
 }
@@ -616,7 +685,7 @@ int dampm_batch_tune(dampm_batch* b, int units_per_cta, int col_weight, int use_
   if (units_per_cta > 0) b->units_per_cta = units_per_cta;
   if (col_weight > 0) b->col_weight = col_weight;
   if (use_graphs >= 0) b->use_graphs = use_graphs;
-  b->graph_dirty = true;
+  b->graph_dirty[0] = b->graph_dirty[1] = true;
   return DAMPM_OK;
 }
 
@@ -626,7 +695,8 @@ int dampm_batch_sync(dampm_batch* b) {
   if (rc) return rc;
   for (size_t s = 0; s < b->scns.size(); ++s)
     if (b->scns[s].d.live && b->Sh[s].status)
-      return bfail(b, DAMPM_ERR_DEVICE, "device status word set");
+      return bfail(b, DAMPM_ERR_DEVICE,
+                   "a scenario's state diverged (non-finite or negative) and was stopped");
   return DAMPM_OK;
 }
 
@@ -681,10 +751,10 @@ int dampm_batch_states(dampm_batch* b, int cap, int* handles, int* running, int*
     const Scalars& S = b->Sh[s];
     const Phys& P = h.d.P;
     handles[n] = h.handle;
-    running[n] = (S.status == 0) && (P.fixed ? (S.it < P.NSTEPS) : (S.t < P.T));
+    // a scenario stopped by its status word reports -1; the others go on
+    running[n] = S.status ? -1 : (P.fixed ? (S.it < P.NSTEPS) : (S.t < P.T)) ? 1 : 0;
     its[n] = S.it;
     ts[n] = S.t;
-    if (S.status) return bfail(b, DAMPM_ERR_DEVICE, "device status word set");
     ++n;
   }
   *count = n;

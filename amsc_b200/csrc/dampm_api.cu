@@ -27,11 +27,15 @@ struct dampm_ctx {
   bool own_stream = false;
   long long cap = 0;
   int nn = 0, nc = 0;
-  Particles p{};
+  // p: the particles as the last pass left them (sorted by the cell of the
+  // last binning); q: the other buffer of the moving fields, which the next
+  // G2P (or a reordering) writes; the two are exchanged after each.
+  Particles p{}, q{};
   Nodes nodes{};
   double *Z = nullptr, *dZdx = nullptr, *dZdy = nullptr;
-  int *count = nullptr, *start = nullptr, *slot = nullptr, *perm = nullptr,
-      *tile_sum = nullptr;
+  int *count = nullptr, *start = nullptr, *perm = nullptr, *tile_sum = nullptr;
+  int* skey = nullptr;  // the cell of each sorted position
+  unsigned long long* sortbuf = nullptr;  // 2 x capacity: crowded cells' order
   int ntiles = 0;
   double* led_part = nullptr;
   int n_led = 0;
@@ -56,17 +60,23 @@ struct dampm_ctx {
   long long launches = 0;
   std::string err;
   std::vector<void*> allocs;
-  // CUDA graph of graph_passes passes (kGraphPasses identical ones, or one
-  // merge/split cycle from a given phase), valid while graph_key (the values
-  // the captured launches took by value, the cycle and its phase) is
-  // unchanged
+  // CUDA graphs of `passes` passes (kGraphPasses identical ones, or one
+  // merge/split cycle from a given phase), each valid while its key (the
+  // values the captured launches took by value -- buffers included, so the
+  // parity of the particle buffers -- the cycle and its phase) is unchanged.
+  // Two are kept: a merge/split cycle of odd length leaves the buffers
+  // exchanged, so consecutive cycles alternate between two graphs.
   bool use_graphs = true;
-  cudaGraphExec_t graph = nullptr;
-  int graph_passes = 0, graph_phase = 0;
-  long long graph_launches = 0;
-  unsigned char graph_key[sizeof(Particles) + sizeof(Nodes) + sizeof(Geom) + sizeof(Phys) +
-                          sizeof(long long) + sizeof(int) + sizeof(dampm_ms_params) +
-                          3 * sizeof(int)] = {};
+  static constexpr int kKeyBytes = 2 * sizeof(Particles) + sizeof(Nodes) + sizeof(Geom) +
+                                   sizeof(Phys) + sizeof(long long) + sizeof(int) +
+                                   sizeof(dampm_ms_params) + 3 * sizeof(int);
+  struct GraphSlot {
+    cudaGraphExec_t exec = nullptr;
+    int passes = 0, phase = 0;
+    long long launches = 0, used = 0;
+    unsigned char key[kKeyBytes] = {};
+  } graphs[2];
+  long long graph_clock = 0;
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -124,6 +134,29 @@ void ev_mark(dampm_ctx* ctx, int cls) {
   ctx->evused++;
 }
 
+// q shares p's fields that the step does not move
+void share_fixed(dampm_ctx* ctx) {
+  Particles& p = ctx->p;
+  Particles& q = ctx->q;
+  q.label = p.label;
+  q.level = p.level;
+  q.xp = p.xp;
+  q.yp = p.yp;
+  q.Ap = p.Ap;
+  q.Fbx = p.Fbx;
+  q.Fby = p.Fby;
+  q.apx = p.apx;
+  q.apy = p.apy;
+  q.Zp = p.Zp;
+  q.hpZ = p.hpZ;
+  q.dZxp = p.dZxp;
+  q.dZyp = p.dZyp;
+  q.Fpx = p.Fpx;
+  q.Fpy = p.Fpy;
+  q.Frx = p.Frx;
+  q.Fry = p.Fry;
+}
+
 int alloc_record(dampm_ctx* ctx) {
   if (ctx->record_alloc) return DAMPM_OK;
   const long long cap = ctx->cap;
@@ -144,39 +177,52 @@ int alloc_record(dampm_ctx* ctx) {
     if (rc) return rc;
     CK(cudaMemsetAsync(*q, 0, ctx->nn * sizeof(double), ctx->stream));
   }
+  share_fixed(ctx);
   ctx->record_alloc = true;
   return DAMPM_OK;
 }
 
 int alloc_particles(dampm_ctx* ctx, long long cap) {
   ctx->cap = cap;
+  for (Particles* pp : {&ctx->p, &ctx->q}) {
+    MovingRefs<double> m = moving_refs(*pp);
+    for (double** f : m.r) {
+      int rc = dalloc(ctx, f, cap);
+      if (rc) return rc;
+      CK(cudaMemsetAsync(*f, 0, cap * sizeof(double), ctx->stream));
+    }
+    for (int** f : m.i) {
+      int rc = dalloc(ctx, f, cap);
+      if (rc) return rc;
+      CK(cudaMemsetAsync(*f, 0, cap * sizeof(int), ctx->stream));
+    }
+    for (double2** f : m.v) {
+      int rc = dalloc(ctx, f, cap);
+      if (rc) return rc;
+      CK(cudaMemsetAsync(*f, 0, cap * sizeof(double2), ctx->stream));
+    }
+  }
   Particles& p = ctx->p;
-  double** f[] = {&p.x,     &p.y,      &p.vpx,    &p.vpy,    &p.hp,
-                  &p.F11,   &p.F12,    &p.F22,    &p.Mp,     &p.Vp,
-                  &p.H,     &p.Ap,     &p.Fbx,    &p.Fby,    &p.vpx_dx,
-                  &p.vpx_dy, &p.vpy_dx, &p.vpy_dy, &p.xp,     &p.yp};
+  double** f[] = {&p.Ap, &p.Fbx, &p.Fby, &p.xp, &p.yp};
   for (double** q : f) {
     int rc = dalloc(ctx, q, cap);
     if (rc) return rc;
     CK(cudaMemsetAsync(*q, 0, cap * sizeof(double), ctx->stream));
   }
-  double2** f2[] = {&p.mp, &p.qf, &p.xe, &p.qg};
-  for (double2** q : f2) {
-    int rc = dalloc(ctx, q, cap);
-    if (rc) return rc;
-    CK(cudaMemsetAsync(*q, 0, cap * sizeof(double2), ctx->stream));
-  }
-  int** fi[] = {&p.label, &p.level, &p.key, &ctx->slot, &ctx->perm};
+  int** fi[] = {&p.label, &p.level, &ctx->perm, &ctx->skey};
   for (int** q : fi) {
     int rc = dalloc(ctx, q, cap);
     if (rc) return rc;
   }
   {
-    int rc = dalloc(ctx, &ctx->cbig, size_t(cap / 256 + 4));
+    int rc = dalloc(ctx, &ctx->sortbuf, size_t(2 * cap));
+    if (rc) return rc;
+    rc = dalloc(ctx, &ctx->cbig, size_t(cap / 256 + 4));
     if (rc) return rc;
     rc = dalloc(ctx, &ctx->cmid, size_t(cap / 17 + 4));
     if (rc) return rc;
   }
+  share_fixed(ctx);
   int rc = ms_alloc(ctx->msb, cap, ctx->nc, [&](void** q, size_t bytes) {
     return dalloc(ctx, reinterpret_cast<unsigned char**>(q), bytes);
   });
@@ -185,28 +231,36 @@ int alloc_particles(dampm_ctx* ctx, long long cap) {
   return DAMPM_OK;
 }
 
-// Enqueues the binning of the current particles (SORT).
+// Enqueues the binning of the current particles (SORT), whose slots and
+// counts are in hand (from G2P, or from k_count after an upload, a state
+// upload or a merge/split).
 void enqueue_sort(dampm_ctx* ctx) {
   const int gp = grid_for(ctx->cap, 256);
-  k_count<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->count, ctx->slot, ctx->S);
-  k_scan_tiles<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(ctx->count, ctx->nc,
-                                                              ctx->tile_sum, ctx->S);
-  k_scan_tile_sums<<<1, kScanThreads, 0, ctx->stream>>>(ctx->tile_sum, ctx->ntiles,
-                                                        ctx->S);
-  k_list_reset<<<1, 1, 0, ctx->stream>>>(ctx->clist_n, ctx->S);
+  k_scan_sums<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(ctx->count, ctx->nc,
+                                                             ctx->tile_sum, ctx->clist_n,
+                                                             ctx->S, 1);
   k_scan_apply<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(
-      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S);
-  k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->slot, ctx->start,
-                                         ctx->perm, ctx->S);
+      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S, 1);
+  k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->p.slot, ctx->start, ctx->perm,
+                                         ctx->skey, ctx->S);
   k_segment_order<<<148 * 4, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,
-                                                   ctx->clist_n, ctx->perm, ctx->cmid,
-                                                   ctx->S);
+                                                   ctx->clist_n, ctx->perm, ctx->p.idx,
+                                                   ctx->cmid, ctx->S);
   k_segment_order_mid<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->cmid,
-                                                       ctx->clist_n, ctx->perm, ctx->cbig,
-                                                       ctx->S);
+                                                       ctx->clist_n, ctx->perm, ctx->p.idx,
+                                                       ctx->cbig, ctx->S);
   k_segment_order_big<<<148, 1024, 0, ctx->stream>>>(ctx->start, ctx->cbig, ctx->clist_n,
-                                                     ctx->perm, ctx->slot, ctx->S);
-  ctx->launches += 9;
+                                                     ctx->perm, ctx->p.idx, ctx->sortbuf,
+                                                     ctx->cap, ctx->S);
+  ctx->launches += 6;
+}
+
+// The particles into reference order (merge/split works in it): p -> q, then
+// the buffers are exchanged.
+void enqueue_unsort(dampm_ctx* ctx) {
+  launch_unsort<double>(grid_for(ctx->cap, 256), ctx->stream, ctx->p, ctx->q, ctx->S);
+  swap_moving(ctx->p, ctx->q);
+  ctx->launches += 1;
 }
 
 int enqueue_pass(dampm_ctx* ctx) {
@@ -222,13 +276,15 @@ int enqueue_pass(dampm_ctx* ctx) {
   k_step_begin<<<1, 1, 0, ctx->stream>>>(ctx->S, ctx->G, ctx->P);
   ctx->launches += 1;
   if (ms_due) {
+    enqueue_unsort(ctx);
     enqueue_sort(ctx);
     ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc,
                                 ctx->G, ctx->P, ctx->Z, ctx->ms, ctx->S, ctx->cap,
                                 ctx->stream, /*use_step_dt=*/1, 0.0);
-    k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(
-        ctx->p.x, ctx->p.y, ctx->p.key, ctx->G, ctx->S);
-    ctx->launches += 1;
+    k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
+    k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
+                                                             ctx->p.slot, ctx->S);
+    ctx->launches += 2;
   }
   ev_mark(ctx, 0);
   enqueue_sort(ctx);
@@ -254,17 +310,18 @@ int enqueue_pass(dampm_ctx* ctx) {
   k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S,
                                                ctx->ledger_log);
   ev_mark(ctx, 2);
-  launch_g2p(grid_for(ctx->cap, kG2PThreads), ctx->stream, ctx->p, ctx->nodes, ctx->Z,
-             ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0,
+  launch_g2p(grid_for(ctx->cap, kG2PThreads), ctx->stream, ctx->p, ctx->q, ctx->perm,
+             ctx->skey, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->count, ctx->record ? 1 : 0,
              (grad_next || ctx->record) ? 1 : 0);
   if (ctx->record) {
-    k_hv<<<grid_for(ctx->nn, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->perm, ctx->start,
+    k_hv<<<grid_for(ctx->nn, 256), 256, 0, ctx->stream>>>(ctx->q, ctx->start,
                                                            ctx->nodes.HV, ctx->G, ctx->S);
     ctx->launches += 1;
   }
   ev_mark(ctx, 3);
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->S);
   ctx->launches += 4;
+  swap_moving(ctx->p, ctx->q);
   ctx->it_host = it_next;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(e));
@@ -308,6 +365,7 @@ void graph_key_of(const dampm_ctx* ctx, int passes, int phase, unsigned char* k)
     o += n;
   };
   put(&ctx->p, sizeof(Particles));
+  put(&ctx->q, sizeof(Particles));
   put(&ctx->nodes, sizeof(Nodes));
   put(&ctx->G, sizeof(Geom));
   put(&ctx->P, sizeof(Phys));
@@ -318,35 +376,54 @@ void graph_key_of(const dampm_ctx* ctx, int passes, int phase, unsigned char* k)
   put(cyc, sizeof(cyc));
 }
 
+void drop_graphs(dampm_ctx* ctx) {
+  for (auto& g : ctx->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = dampm_ctx::GraphSlot{};
+  }
+}
+
 // A stream that cannot be captured (or a graph that cannot be built): the
 // context launches plainly from then on.
 int graphs_off(dampm_ctx* ctx) {
   cudaGetLastError();  // the capture's error is not the step's
   ctx->use_graphs = false;
-  ctx->graph = nullptr;
+  drop_graphs(ctx);
   return DAMPM_OK;
 }
 
-// (Re)captures `passes` passes from the current pass unless the graph in
-// hand was captured with the same buffers, parameters, cycle and phase.
-int ensure_graph(dampm_ctx* ctx, int passes, int phase) {
-  unsigned char key[sizeof(ctx->graph_key)];
+// The graph of `passes` passes from the current pass, captured unless one in
+// hand was captured with the same buffers, parameters, cycle and phase
+// (*out = null when graphs were turned off).
+int ensure_graph(dampm_ctx* ctx, int passes, int phase, dampm_ctx::GraphSlot** out) {
+  *out = nullptr;
+  unsigned char key[dampm_ctx::kKeyBytes];
   graph_key_of(ctx, passes, phase, key);
-  if (ctx->graph && std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) return DAMPM_OK;
-  if (ctx->graph) {
-    cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-  }
+  for (auto& g : ctx->graphs)
+    if (g.exec && std::memcmp(key, g.key, sizeof(key)) == 0) {
+      g.used = ++ctx->graph_clock;
+      *out = &g;
+      return DAMPM_OK;
+    }
+  dampm_ctx::GraphSlot* slot = &ctx->graphs[0];
+  for (auto& g : ctx->graphs)
+    if (!g.exec || g.used < slot->used) slot = &g;  // an empty slot, else the oldest
+  if (slot->exec) cudaGraphExecDestroy(slot->exec);
+  *slot = dampm_ctx::GraphSlot{};
   const long long it0 = ctx->it_host, l0 = ctx->launches;
+  const Particles p0 = ctx->p, q0 = ctx->q;
   if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return graphs_off(ctx);
   int rc = DAMPM_OK;
   for (int k = 0; k < passes && rc == DAMPM_OK; ++k) rc = enqueue_pass(ctx);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-  ctx->graph_launches = ctx->launches - l0;
+  const long long captured = ctx->launches - l0;
+  // nothing ran: the host's view of the passes and buffers goes back
   ctx->it_host = it0;
   ctx->launches = l0;
+  ctx->p = p0;
+  ctx->q = q0;
   if (rc) {
     if (g) cudaGraphDestroy(g);
     return rc;
@@ -355,26 +432,78 @@ int ensure_graph(dampm_ctx* ctx, int passes, int phase) {
     if (g) cudaGraphDestroy(g);
     return graphs_off(ctx);
   }
-  const cudaError_t ei = cudaGraphInstantiate(&ctx->graph, g, 0);
+  const cudaError_t ei = cudaGraphInstantiate(&slot->exec, g, 0);
   cudaGraphDestroy(g);
-  if (ei != cudaSuccess) return graphs_off(ctx);
-  std::memcpy(ctx->graph_key, key, sizeof(key));
-  ctx->graph_passes = passes;
-  ctx->graph_phase = phase;
+  if (ei != cudaSuccess) {
+    slot->exec = nullptr;
+    return graphs_off(ctx);
+  }
+  std::memcpy(slot->key, key, sizeof(key));
+  slot->passes = passes;
+  slot->phase = phase;
+  slot->launches = captured;
+  slot->used = ++ctx->graph_clock;
+  *out = slot;
   return DAMPM_OK;
 }
 
-int sync_status(dampm_ctx* ctx) {
+// The buffers after `passes` passes replayed from a graph: each pass
+// exchanges them once, a merge/split pass once more.
+void advance_buffers(dampm_ctx* ctx, int passes) {
+  int swaps = passes;
+  if (ms_cadence(ctx)) {
+    const int L = ctx->ms.call_interval;
+    for (long long it = ctx->it_host + 1; it <= ctx->it_host + passes; ++it)
+      if (it % L == 0) ++swaps;
+  }
+  if (swaps & 1) swap_moving(ctx->p, ctx->q);
+}
+
+// Reads the device scalars.  strict: a set status bit is returned as an
+// error (the calls that report the status word); the data-out calls pass
+// false so that a diverged state can still be inspected.
+// The next sort scans every cell (after new particles or a new count).
+void full_scan_next(const dampm_ctx* ctx, Scalars& s) {
+  s.krange[0] = 0x7fffffff;
+  s.krange[1] = -1;
+  s.knext[0] = 0;
+  s.knext[1] = ctx->nc - 1;
+}
+
+int sync_status(dampm_ctx* ctx, bool strict = true) {
   CK(cudaMemcpyAsync(ctx->Sh, ctx->S, sizeof(Scalars), cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (!strict) return DAMPM_OK;
   if (ctx->Sh->status & kStatusCapacity)
     return fail(ctx, DAMPM_ERR_CAPACITY, "particle capacity exceeded by merge/split");
+  if (ctx->Sh->status & kStatusNonFinite)
+    return fail(ctx, DAMPM_ERR_DEVICE,
+                "non-finite or negative particle state: the run diverged and was stopped");
   if (ctx->Sh->status)
     return fail(ctx, DAMPM_ERR_DEVICE, "device status word set");
   return DAMPM_OK;
 }
 
+
+// out[idx[j]] = a[j]: a field of the sorted slots into reference order
+__global__ void k_to_ref(const double* __restrict__ a, const int* __restrict__ idx,
+                         double* __restrict__ out, const Scalars* S) {
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x)
+    out[idx[j]] = a[j];
+}
+
+// one half of a pair field into reference order
+__global__ void k_pair_to_ref(const double2* __restrict__ a, int half,
+                              const int* __restrict__ idx, double* __restrict__ out,
+                              const Scalars* S) {
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x) {
+    const double2 v = a[j];
+    out[idx[j]] = half ? v.y : v.x;
+  }
+}
 
 __global__ void k_int_to_double(const int* a, double* b, const Scalars* S) {
   const int np = S->np;
@@ -384,7 +513,8 @@ __global__ void k_int_to_double(const int* a, double* b, const Scalars* S) {
 }
 
 // Ap, mom, Fb as the reference stores them at the end of a step
-// (main/optim_par.cpp:600-626), from the persistent state.
+// (main/optim_par.cpp:600-626), from the persistent state, into reference
+// order.
 __global__ void k_derived(Particles p, Phys P, const Scalars* S, int which,
                           double* out) {
   const int np = S->np;
@@ -400,7 +530,7 @@ __global__ void k_derived(Particles p, Phys P, const Scalars* S, int which,
       voellmy(P, p.vpx[i], p.vpy[i], hp, fx, fy);
       v = (which == 3) ? fx : fy;
     }
-    out[i] = v;
+    out[p.idx[i]] = v;
   }
 }
 
@@ -429,7 +559,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   if (ms) {
     ctx->ms = *ms;
   } else {  // main/mpm_data.h:102-112
-    ctx->ms = dampm_ms_params{0.9, 0.30, 0.0, 1e30, 0.05, 0.01, -2, 2, 2, 10, 1e9};
+    ctx->ms = dampm_ms_params{0.9, 0.30, 0.0, 1e30, 0.05, 0.01, -2, 2, 2, 10, 1e9, 0.0};
   }
   ctx->precision = precision;
   ctx->G = make_geom(*grid);
@@ -498,7 +628,7 @@ int dampm_ctx_destroy(dampm_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* q : ctx->allocs) cudaFree(q);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
-  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  drop_graphs(ctx);
   if (ctx->Sh) cudaFreeHost(ctx->Sh);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -553,13 +683,18 @@ int dampm_upload_particles(dampm_ctx* ctx, long long np, const double* x,
   Scalars s0{};
   s0.fresh = 1;
   s0.np = int(np);
+  full_scan_next(ctx, s0);
   *ctx->Sh = s0;
   CK(cudaMemcpyAsync(ctx->S, ctx->Sh, sizeof(Scalars), cudaMemcpyHostToDevice,
                      ctx->stream));
+  CK(cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));  // Sh is reused below
   if (np > 0) {
+    // the slots hold the particles in DATA order (idx = slot)
     launch_init_particles<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z,
                                   ctx->dZdx, ctx->dZdy, ctx->G, ctx->P, ctx->S, int(np), 0);
+    k_count_n<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.key, ctx->count, p.slot,
+                                                           int(np));
     launch_prep<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z, ctx->G, ctx->P,
                         ctx->S, 0);
     CK(cudaGetLastError());
@@ -593,27 +728,29 @@ int dampm_step(dampm_ctx* ctx, int nsteps) {
   if (len > 0) {
     bool aligned = true;
     if (ms_cadence(ctx)) {
-      // a graph of this cycle in hand: plain passes up to its phase
-      if (ctx->graph && ctx->graph_passes == len) {
-        unsigned char key[sizeof(ctx->graph_key)];
-        graph_key_of(ctx, len, ctx->graph_phase, key);
-        if (std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) phase = ctx->graph_phase;
-      }
+      // graphs of this cycle in hand: plain passes up to their phase
+      for (const auto& g : ctx->graphs)
+        if (g.exec && g.passes == len) phase = g.phase;
       for (; s < nsteps && int(ctx->it_host % len) != phase; ++s) {
         int rc = enqueue_pass(ctx);
         if (rc) return rc;
       }
       aligned = int(ctx->it_host % len) == phase;
     }
-    if (aligned) {
-      // captured on the first eligible call, whatever its length
-      int rc = ensure_graph(ctx, len, phase);
+    // captured on the first eligible call, whatever its length (a short call
+    // captures the graph for the calls to come and runs plainly)
+    bool first = true;
+    while (aligned && (first || s + len <= nsteps)) {
+      first = false;
+      dampm_ctx::GraphSlot* g = nullptr;
+      int rc = ensure_graph(ctx, len, phase, &g);
       if (rc) return rc;
-      for (; ctx->graph && s + len <= nsteps; s += len) {
-        CK(cudaGraphLaunch(ctx->graph, ctx->stream));
-        ctx->it_host += len;
-        ctx->launches += ctx->graph_launches;
-      }
+      if (!g || s + len > nsteps) break;
+      CK(cudaGraphLaunch(g->exec, ctx->stream));
+      advance_buffers(ctx, len);
+      ctx->it_host += len;
+      ctx->launches += g->launches;
+      s += len;
     }
   }
   for (; s < nsteps; ++s) {
@@ -661,13 +798,14 @@ int dampm_run(dampm_ctx* ctx, long long max_steps, int chunk,
 int dampm_status(dampm_ctx* ctx, int* it, double* t, double* dt_last,
                  long long* np) {
   if (!ctx) return DAMPM_ERR_ARG;
-  int rc = sync_status(ctx);
+  int rc = sync_status(ctx, false);
   if (rc) return rc;
   if (it) *it = ctx->Sh->it;
   if (t) *t = ctx->Sh->t;
   if (dt_last) *dt_last = ctx->Sh->dt;
   if (np) *np = ctx->Sh->np;
-  return DAMPM_OK;
+  // the loop state is filled in either way; a set status bit is reported
+  return ctx->Sh->status ? sync_status(ctx) : DAMPM_OK;
 }
 
 int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
@@ -683,11 +821,13 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
   CK(cudaMemcpyAsync(&S->active, &ctx->Sh->active, sizeof(int),
                      cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  enqueue_unsort(ctx);
   enqueue_sort(ctx);
   ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
              ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt);
-  k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.x, ctx->p.y,
-                                                           ctx->p.key, ctx->G, ctx->S);
+  k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
+  k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
+                                                           ctx->p.slot, ctx->S);
   CK(cudaGetLastError());
   rc = sync_status(ctx);
   if (rc) return rc;
@@ -703,70 +843,73 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
 int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
   if (!ctx || !field || !out) return DAMPM_ERR_ARG;
   if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "no particles");
-  int rc = sync_status(ctx);
+  int rc = sync_status(ctx, false);
   if (rc) return rc;
   const int np = ctx->Sh->np;
   const bool fresh = ctx->Sh->fresh != 0;
   const std::string f(field);
   Particles& p = ctx->p;
-  const double* src = nullptr;
-  const int* isrc = nullptr;
+  const double* sorted = nullptr;  // a field of the sorted slots
+  const double* ref = nullptr;     // a field already in reference order
+  const int* iref = nullptr;       // an integer field in reference order
   int derived = -1;
   int pair_half = -1;  // mom_px / mom_py: one half of the momentum pair
-  if (f == "x") src = p.x;
-  else if (f == "y") src = p.y;
-  else if (f == "Mp") src = p.Mp;
-  else if (f == "Vp") src = p.Vp;
-  else if (f == "H") src = p.H;
-  else if (f == "hp") src = p.hp;
-  else if (f == "vpx" || f == "vpxL") src = p.vpx;
-  else if (f == "vpy" || f == "vpyL") src = p.vpy;
-  else if (f == "F_11") src = p.F11;
-  else if (f == "F_12" || f == "F_21") src = p.F12;
-  else if (f == "F_22") src = p.F22;
-  else if (f == "xp") src = p.xp;
-  else if (f == "yp") src = p.yp;
-  else if (f == "vpx_dx") src = p.vpx_dx;
-  else if (f == "vpx_dy") src = p.vpx_dy;
-  else if (f == "vpy_dx") src = p.vpy_dx;
-  else if (f == "vpy_dy") src = p.vpy_dy;
-  else if (f == "label") isrc = p.label;
-  else if (f == "level") isrc = p.level;
-  else if (f == "Ap") { if (fresh) src = p.Ap; else derived = 0; }
+  if (f == "x") sorted = p.x;
+  else if (f == "y") sorted = p.y;
+  else if (f == "Mp") sorted = p.Mp;
+  else if (f == "Vp") sorted = p.Vp;
+  else if (f == "H") sorted = p.H;
+  else if (f == "hp") sorted = p.hp;
+  else if (f == "vpx" || f == "vpxL") sorted = p.vpx;
+  else if (f == "vpy" || f == "vpyL") sorted = p.vpy;
+  else if (f == "F_11") sorted = p.F11;
+  else if (f == "F_12" || f == "F_21") sorted = p.F12;
+  else if (f == "F_22") sorted = p.F22;
+  else if (f == "xp") ref = p.xp;
+  else if (f == "yp") ref = p.yp;
+  else if (f == "vpx_dx") sorted = p.vpx_dx;
+  else if (f == "vpx_dy") sorted = p.vpx_dy;
+  else if (f == "vpy_dx") sorted = p.vpy_dx;
+  else if (f == "vpy_dy") sorted = p.vpy_dy;
+  else if (f == "label") iref = p.label;
+  else if (f == "level") iref = p.level;
+  // fresh values sit in reference-ordered slots (idx = slot)
+  else if (f == "Ap") { if (fresh) sorted = p.Ap; else derived = 0; }
   else if (f == "mom_px" || f == "mom_py") pair_half = f == "mom_px" ? 0 : 1;
-  else if (f == "Fb_x") { if (fresh) src = p.Fbx; else derived = 3; }
-  else if (f == "Fb_y") { if (fresh) src = p.Fby; else derived = 4; }
+  else if (f == "Fb_x") { if (fresh) sorted = p.Fbx; else derived = 3; }
+  else if (f == "Fb_y") { if (fresh) sorted = p.Fby; else derived = 4; }
   else if (ctx->record_alloc) {
-    if (f == "apx") src = p.apx;
-    else if (f == "apy") src = p.apy;
-    else if (f == "Zp") src = p.Zp;
-    else if (f == "hpZ") src = p.hpZ;
-    else if (f == "dZxp") src = p.dZxp;
-    else if (f == "dZyp") src = p.dZyp;
-    else if (f == "Fpx") src = p.Fpx;
-    else if (f == "Fpy") src = p.Fpy;
-    else if (f == "Fric_px") src = p.Frx;
-    else if (f == "Fric_py") src = p.Fry;
+    if (f == "apx") sorted = p.apx;
+    else if (f == "apy") sorted = p.apy;
+    else if (f == "Zp") sorted = p.Zp;
+    else if (f == "hpZ") sorted = p.hpZ;
+    else if (f == "dZxp") sorted = p.dZxp;
+    else if (f == "dZyp") sorted = p.dZyp;
+    else if (f == "Fpx") sorted = p.Fpx;
+    else if (f == "Fpy") sorted = p.Fpy;
+    else if (f == "Fric_px") sorted = p.Frx;
+    else if (f == "Fric_py") sorted = p.Fry;
   }
-  if (!src && !isrc && derived < 0 && pair_half < 0)
+  if (!sorted && !ref && !iref && derived < 0 && pair_half < 0)
     return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown particle field " + f);
   if (np == 0) return DAMPM_OK;
-  if (pair_half >= 0) {
-    CK(download_pair_half(out, p.mp, pair_half, np, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    return DAMPM_OK;
-  }
-  if (isrc || derived >= 0) {
-    // reuse the merge/split scratch as a staging buffer
-    double* tmp = ctx->msb.stage;
-    if (isrc)
-      k_int_to_double<<<grid_for(np, 256), 256, 0, ctx->stream>>>(isrc, tmp, ctx->S);
-    else
-      k_derived<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->P, ctx->S,
-                                                            derived, tmp);
-    CK(cudaGetLastError());
+  double* tmp = ctx->msb.stage;  // the merge/split scratch as a staging buffer
+  const int gp = grid_for(np, 256);
+  const double* src = ref;
+  if (sorted) {
+    k_to_ref<<<gp, 256, 0, ctx->stream>>>(sorted, p.idx, tmp, ctx->S);
+    src = tmp;
+  } else if (pair_half >= 0) {
+    k_pair_to_ref<<<gp, 256, 0, ctx->stream>>>(p.mp, pair_half, p.idx, tmp, ctx->S);
+    src = tmp;
+  } else if (iref) {
+    k_int_to_double<<<gp, 256, 0, ctx->stream>>>(iref, tmp, ctx->S);
+    src = tmp;
+  } else if (derived >= 0) {
+    k_derived<<<gp, 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, derived, tmp);
     src = tmp;
   }
+  CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, src, sizeof(double) * np, cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -829,7 +972,7 @@ int dampm_ledger_history(dampm_ctx* ctx, long long first_it, int n, double* out)
 
 int dampm_ledgers(dampm_ctx* ctx, double out[9]) {
   if (!ctx || !out) return DAMPM_ERR_ARG;
-  int rc = sync_status(ctx);
+  int rc = sync_status(ctx, false);
   if (rc) return rc;
   std::memcpy(out, ctx->Sh->ledger, sizeof(double) * 9);
   return DAMPM_OK;
@@ -856,14 +999,19 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
     CK(cudaMemcpyAsync(p.Fbx, Fb_x, b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(p.Fby, Fb_y, b, cudaMemcpyHostToDevice, ctx->stream));
   }
-  int rc = sync_status(ctx);
+  int rc = sync_status(ctx, false);
   if (rc) return rc;
   ctx->Sh->np = int(np);
   ctx->Sh->fresh = fresh ? 1 : 0;
+  ctx->Sh->status = 0;  // a new state: an earlier divergence no longer applies
   ctx->Sh->red_cur[0] = ctx->Sh->red_cur[1] = ctx->Sh->red_cur[2] = 0ull;
+  full_scan_next(ctx, *ctx->Sh);
   CK(cudaMemcpyAsync(ctx->S, ctx->Sh, sizeof(Scalars), cudaMemcpyHostToDevice,
                      ctx->stream));
-  k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.x, p.y, p.key, ctx->G, ctx->S);
+  // the slots now hold the particles in reference order
+  CK(cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream));
+  k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->G, ctx->S);
+  k_count_n<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.key, ctx->count, p.slot, int(np));
   k_reduce_state<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->S);
   launch_prep<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z, ctx->G, ctx->P,
                       ctx->S, fresh ? 0 : 1);
@@ -873,16 +1021,23 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
 
 int dampm_get_state(dampm_ctx* ctx, double* const* fields) {
   if (!ctx || !fields) return DAMPM_ERR_ARG;
-  int rc = sync_status(ctx);
+  int rc = sync_status(ctx, false);
   if (rc) return rc;
   Particles& p = ctx->p;
   const double* src[11] = {p.x, p.y, p.vpx, p.vpy, p.hp, p.F11, p.F12, p.F22,
                            p.Mp, p.Vp, p.H};
-  const size_t b = sizeof(double) * ctx->Sh->np;
-  for (int k = 0; k < 11; ++k) {
+  const int np = ctx->Sh->np;
+  const size_t b = sizeof(double) * np;
+  for (int k = 0; k < 11; ++k)
     if (!fields[k]) return DAMPM_ERR_ARG;
-    CK(cudaMemcpyAsync(fields[k], src[k], b, cudaMemcpyDeviceToHost, ctx->stream));
-  }
+  if (np == 0) return DAMPM_OK;
+  // into reference order in the merge/split scratch, then one copy each
+  for (int k = 0; k < 11; ++k)
+    k_to_ref<<<grid_for(np, 256), 256, 0, ctx->stream>>>(src[k], p.idx, ctx->msb.sd[k],
+                                                         ctx->S);
+  CK(cudaGetLastError());
+  for (int k = 0; k < 11; ++k)
+    CK(cudaMemcpyAsync(fields[k], ctx->msb.sd[k], b, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return DAMPM_OK;
 }

@@ -40,6 +40,10 @@ struct Scalars {
   int np_next;  // particle count after a merge/split emit
   unsigned long long red_cur[3];   // ordered keys of max|vpx|, max|vpy|, max hp
   unsigned long long red_next[3];  // ... produced by this step's G2P
+  // cell-key ranges for the counting sort's scan: krange = the keys the cell
+  // starts describe, knext = the keys G2P produced since (lo > hi: none)
+  int krange[2];
+  int knext[2];
   double ledger[9];
   long long ms_counts[4];
 };
@@ -193,6 +197,39 @@ __device__ __forceinline__ void bingham_stress(const Phys& P, R vpx, R vpy, R hp
   F11 = R(P.BING * double(sig_xx) - pres);
   F12 = R(P.BING * double(sig_xy));
   F22 = R(P.BING * double(sig_yy) - pres);
+}
+
+// The rheology of the FP32 form is evaluated in FP64: the plug switch of
+// the Bingham stress (the root ZZ and tau_y/sqrt(II)) and the Voellmy
+// friction act on small differences of the strain rates and velocities,
+// which FP32 arithmetic would round away.  Inputs and results stay R.
+template <class R>
+__device__ __forceinline__ void rheology_stress(const Phys& P, R vpx, R vpy, R hp, R H,
+                                                R vpx_dx, R vpy_dy, R vpx_dy, R vpy_dx,
+                                                R& F11, R& F12, R& F22) {
+  if constexpr (sizeof(R) == 4) {
+    double f11, f12, f22;
+    bingham_stress<double>(P, vpx, vpy, hp, H, vpx_dx, vpy_dy, vpx_dy, vpy_dx, f11, f12,
+                           f22);
+    F11 = R(f11);
+    F12 = R(f12);
+    F22 = R(f22);
+  } else {
+    bingham_stress<R>(P, vpx, vpy, hp, H, vpx_dx, vpy_dy, vpx_dy, vpy_dx, F11, F12, F22);
+  }
+}
+
+template <class R>
+__device__ __forceinline__ void rheology_friction(const Phys& P, R vx, R vy, R h, R& fbx,
+                                                  R& fby) {
+  if constexpr (sizeof(R) == 4) {
+    double fx, fy;
+    voellmy<double>(P, vx, vy, h, fx, fy);
+    fbx = R(fx);
+    fby = R(fy);
+  } else {
+    voellmy<R>(P, vx, vy, h, fbx, fby);
+  }
 }
 
 }  // namespace dampm

@@ -1,6 +1,7 @@
 // dampm_kernels.h -- device buffers and kernel entry points of the step.
 #pragma once
 #include <cstddef>
+#include <utility>
 
 #include "dampm_device.cuh"
 
@@ -48,13 +49,21 @@ struct Vec2T<float> {
 template <class R>
 using V2 = typename Vec2T<R>::type;
 
-// Particle SoA in reference index order; R = double is the FP64 path,
-// R = float the FP32 form (batches).
+// Particle SoA.  The moving fields are kept in cell-sorted order -- by
+// (cell of the last binning, reference index) -- in two buffers: each step's
+// G2P reads one through the sort permutation and writes the other in the new
+// sorted order, so P2G and G2P stream contiguous runs of a cell column
+// instead of gathering across the whole set.  `idx` is each slot's index in
+// the reference's particle order (DATA order, then the compacted order
+// merge/split produces); data going in and out of the library is in that
+// order.  R = double is the FP64 path, R = float the FP32 form (batches).
 template <class R>
 struct ParticlesT {
-  // persistent state
+  // ---- moving (double-buffered, sorted order) ----
   R *x, *y, *vpx, *vpy, *hp, *F11, *F12, *F22, *Mp, *Vp, *H;
-  int *label, *level, *key;
+  // key: cell of the next binning; idx: reference index; slot: rank among
+  // the particles of its cell from the counting sort's atomics
+  int *key, *idx, *slot;
   // the record the next P2G transfers, written by G2P (or by k_prep after an
   // upload, a state upload or a merge/split), as pairs that P2G gathers
   // with one copy each:
@@ -65,15 +74,42 @@ struct ParticlesT {
   //   qg = gravity force -g*Vp*rho*grad(Z)*(1 - H/hp) there
   //        (main/optim_par.cpp:387,447-454).
   V2<R> *mp, *qf, *xe, *qg;
-  // Ap and Fb as stored at upload / merge/split (valid while Scalars::fresh
-  // is set; otherwise they are derived from the state)
-  R *Ap, *Fbx, *Fby;
-  // velocity gradients (merge/split input, outputs)
+  // velocity gradients (merge/split input, outputs); null in batches
   R *vpx_dx, *vpx_dy, *vpy_dx, *vpy_dy;
-  // output-only fields (allocated when outputs are recorded)
-  R *apx, *apy, *Zp, *hpZ, *dZxp, *dZyp, *Fpx, *Fpy, *Frx, *Fry;
+  // ---- reference order (not moved by the step) ----
+  int *label, *level;
   R *xp, *yp;
+  // Ap and Fb as stored at upload / merge/split: valid while Scalars::fresh
+  // is set, when the slots are in reference order (otherwise they are
+  // derived from the state)
+  R *Ap, *Fbx, *Fby;
+  // ---- output-only fields of a recorded step (G2P's sorted order) ----
+  R *apx, *apy, *Zp, *hpZ, *dZxp, *dZyp, *Fpx, *Fpy, *Frx, *Fry;
 };
+
+// Pointers to the moving fields of p, in a fixed order.
+constexpr int kMovingR = 15, kMovingI = 3, kMovingV = 4;
+template <class R>
+struct MovingRefs {
+  R** r[kMovingR];
+  int** i[kMovingI];
+  V2<R>** v[kMovingV];
+};
+template <class R>
+inline MovingRefs<R> moving_refs(ParticlesT<R>& p) {
+  return MovingRefs<R>{{&p.x, &p.y, &p.vpx, &p.vpy, &p.hp, &p.F11, &p.F12, &p.F22, &p.Mp,
+                        &p.Vp, &p.H, &p.vpx_dx, &p.vpx_dy, &p.vpy_dx, &p.vpy_dy},
+                       {&p.key, &p.idx, &p.slot},
+                       {&p.mp, &p.qf, &p.xe, &p.qg}};
+}
+// exchanges the moving buffers of a and b (the other pointers are shared)
+template <class R>
+inline void swap_moving(ParticlesT<R>& a, ParticlesT<R>& b) {
+  MovingRefs<R> ra = moving_refs(a), rb = moving_refs(b);
+  for (int k = 0; k < kMovingR; ++k) std::swap(*ra.r[k], *rb.r[k]);
+  for (int k = 0; k < kMovingI; ++k) std::swap(*ra.i[k], *rb.i[k]);
+  for (int k = 0; k < kMovingV; ++k) std::swap(*ra.v[k], *rb.v[k]);
+}
 using Particles = ParticlesT<double>;
 
 // Nodal fields, quadgrid node order.
@@ -94,29 +130,34 @@ template <class R>
 void launch_init_particles(int grid, int block, cudaStream_t st, ParticlesT<R> p,
                            const double* Z, const double* dZdx, const double* dZdy,
                            Geom G, Phys P, Scalars* S, int np, int key_off);
-__global__ void k_keys(const double* x, const double* y, int* key, Geom G,
-                       const Scalars* S);
+// cell keys of the current positions, idx = slot (reference order); the
+// next sort scans every cell
+__global__ void k_keys(Particles p, Geom G, Scalars* S);
 __global__ void k_reduce_state(Particles p, Scalars* S);
 template <class R>
 void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const double* Z,
                  Geom G, Phys P, const Scalars* S, int derive);
+// counting sort: slots and counts (after an upload, a state upload or a
+// merge/split; a step's G2P counts the keys it makes), the scan of the
+// counts over the key range (ranged != 0; else over all n), the scatter into
+// perm, and the order by reference index inside each cell
 __global__ void k_count(const int* key, int* count, int* slot,
                         const Scalars* S);
-__global__ void k_scan_tiles(const int* count, int n, int* tile_sum,
-                             const Scalars* S);
-__global__ void k_scan_tile_sums(int* tile_sum, int ntiles, const Scalars* S);
+__global__ void k_count_n(const int* key, int* count, int* slot, int n);
+__global__ void k_scan_sums(const int* count, int n, int* tile_sum, int* list_n,
+                            const Scalars* S, int ranged);
 __global__ void k_scan_apply(int* count, int n, const int* tile_sum,
                              int* start, int* list, int* list_n,
-                             const Scalars* S);
-__global__ void k_list_reset(int* list_n, const Scalars* S);
+                             const Scalars* S, int ranged);
 __global__ void k_scatter(const int* key, const int* slot, const int* start,
-                          int* perm, const Scalars* S);
+                          int* perm, int* skey, Scalars* S);
 __global__ void k_segment_order(const int* start, const int* list, int* list_n,
-                                int* perm, int* mid, const Scalars* S);
+                                int* perm, const int* idx, int* mid, const Scalars* S);
 __global__ void k_segment_order_mid(const int* start, const int* mid, int* list_n,
-                                    int* perm, int* big, const Scalars* S);
+                                    int* perm, const int* idx, int* big, const Scalars* S);
 __global__ void k_segment_order_big(const int* start, const int* big,
-                                    const int* list_n, int* perm, int* tmp,
+                                    const int* list_n, int* perm, const int* idx,
+                                    unsigned long long* tmp, long long cap,
                                     const Scalars* S);
 __global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
                              int target_units, int seg, int* ustart,
@@ -134,9 +175,16 @@ int setup_p2g();
 constexpr int kLedgerLog = 1024;  // rows of the per-step ledger log
 __global__ void k_ledger_final(const double* led_part, const int* ucount,
                                Scalars* S, double* log);
-// G2P of the single-scenario step (k_g2p_t specialised for the two flags)
-void launch_g2p(int grid, cudaStream_t st, Particles p, Nodes nodes, const double* Z,
-                Geom G, Phys P, Scalars* S, int record, int want_grad);
+// G2P of the single-scenario step (k_g2p_t specialised for the two flags):
+// reads `cur` through perm, writes `nxt` in this step's sorted order and
+// counts the next binning's keys
+void launch_g2p(int grid, cudaStream_t st, Particles cur, Particles nxt, const int* perm,
+                const int* skey, Nodes nodes, const double* Z, Geom G, Phys P, Scalars* S,
+                int* count, int record, int want_grad);
+// the particles of `src` into reference order in `dst` (slot idx[j])
+template <class R>
+void launch_unsort(int grid, cudaStream_t st, ParticlesT<R> src, ParticlesT<R> dst,
+                   const Scalars* S);
 
 // ---- batches of independent scenarios --------------------------------------
 // One scenario of a batch: its geometry, physics and place in the packed
@@ -174,9 +222,9 @@ __global__ void k_b_ledger(const double* led_part, const int2* scn_units,
                            const Scn* scn, Scalars* S, int nscn,
                            const Scalars* Sg);
 template <class R>
-void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const V2<R>* vvL,
-                  const double* Z, const Scn* scn, Scalars* S,
-                  const int2* gblk, const Scalars* Sg);
+void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> cur, ParticlesT<R> nxt,
+                  const int* perm, const int* skey, const V2<R>* vvL, const double* Z,
+                  const Scn* scn, Scalars* S, const int2* gblk, Scalars* Sg, int* count);
 template <class R>
 void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> src,
                    const int4* mblk);
@@ -185,8 +233,8 @@ __global__ void k_to_f32(const double* a, float* b, long long n);
 __global__ void k_to_f64(const float* a, double* b, long long n);
 __global__ void k_b_move_nodes(double* dst, const double* src, const int4* nblk);
 
-__global__ void k_hv(const Particles p, const int* perm, const int* cstart,
-                     double* HV, Geom G, const Scalars* S);
+__global__ void k_hv(const Particles p, const int* cstart, double* HV, Geom G,
+                     const Scalars* S);
 
 size_t p2g_smem_bytes();  // FP64 P2G staging (the single-scenario path)
 

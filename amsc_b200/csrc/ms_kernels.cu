@@ -28,6 +28,7 @@ struct MsCfg {
   double alpha, beta, split_hp_min, shear_split, hp_min, max_dv;
   int min_level, max_level, min_ppc;
   long long max_ops;  // (int)data.ms_max_ops, main/gpu_offload.cpp:317
+  double pair_gate2;  // squared pair-distance limit; 0: none
   double dt_host;
   int use_step_dt;
 };
@@ -124,7 +125,8 @@ __global__ void k_ms_split_cap(const int* perm, const int* rank, int* act,
 // kept after the undo loop.
 __device__ long long pair_cell(int b, int e, const int* perm, int* act,
                                int* partner, int* paired, const Particles& p,
-                               double max_dv2, int min_ppc, long long budget) {
+                               double max_dv2, double gate2, int min_ppc,
+                               long long budget) {
   long long n = 0;
   for (int j = b; j < e; ++j) paired[j] = 0;
   for (int ji = b; ji < e && n < budget; ++ji) {
@@ -141,7 +143,7 @@ __device__ long long pair_cell(int b, int e, const int* perm, int* act,
       const double d2 = dx * dx + dy * dy;
       const double dvx = u1 - p.vpx[i2];
       const double dvy = v1 - p.vpy[i2];
-      if (d2 < best && (dvx * dvx + dvy * dvy) < max_dv2) {
+      if (d2 < best && (dvx * dvx + dvy * dvy) < max_dv2 && (gate2 == 0.0 || d2 < gate2)) {
         best = d2;
         bj = jj;
       }
@@ -223,8 +225,8 @@ __global__ void k_ms_pair_parallel(const int* start, int ncells,
        cell += gridDim.x * blockDim.x) {
     const int b = start[cell], e = start[cell + 1];
     if (e - b < 1) continue;
-    local += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.min_ppc,
-                       0x7fffffffffffffffLL);
+    local += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.pair_gate2,
+                       c.min_ppc, 0x7fffffffffffffffLL);
   }
   if (local) atomicAdd((unsigned long long*)&S->ms_counts[1], (unsigned long long)local);
 }
@@ -241,8 +243,8 @@ __global__ void k_ms_pair_serial(const int* start, int ncells, const int* perm,
   for (int cell = 0; cell < ncells; ++cell) {
     const int b = start[cell], e = start[cell + 1];
     if (e - b < 1) continue;
-    n_merge += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.min_ppc,
-                         c.max_ops - n_merge);
+    n_merge += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.pair_gate2,
+                         c.min_ppc, c.max_ops - n_merge);
   }
   S->ms_counts[1] = n_merge;
 }
@@ -410,10 +412,9 @@ int grid_for(long long n, int threads) {
 // exclusive scan of a[0..n) -> out[0..n] (a is zeroed), n = cap
 int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
                  const Scalars* S, cudaStream_t st) {
-  k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, S);
-  k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(tile_sum, ntiles, S);
-  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, nullptr, nullptr, S);
-  return 3;
+  k_scan_sums<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, nullptr, S, 0);
+  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, nullptr, nullptr, S, 0);
+  return 2;
 }
 
 }  // namespace
@@ -433,6 +434,11 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   c.max_level = cfg.max_level;
   c.min_ppc = cfg.min_particles_per_cell;
   c.max_ops = (long long)(int)cfg.max_ops;
+  {
+    const double min_h = (G.hy < G.hx) ? G.hy : G.hx;
+    const double r = cfg.pair_dist * min_h;
+    c.pair_gate2 = cfg.pair_dist > 0.0 ? r * r : 0.0;
+  }
   c.dt_host = dt;
   c.use_step_dt = use_step_dt;
   int n = 0;

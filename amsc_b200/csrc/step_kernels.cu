@@ -87,6 +87,7 @@ __global__ void k_init_particles(ParticlesT<R> p, const double* __restrict__ Z,
     const double x = p.x[i], y = p.y[i];
     const int r = cell_row(y, G.hy, G.nrows), c = cell_col(x, G.hx, G.ncols);
     p.key[i] = r + c * G.nrows + key_off;
+    p.idx[i] = i;
     p.label[i] = i;
     p.level[i] = 0;
     double xi, eta;
@@ -132,17 +133,21 @@ __global__ void k_init_particles(ParticlesT<R> p, const double* __restrict__ Z,
   }
 }
 
-// Recomputes the cell key of every particle (after a merge/split emit or a
-// state upload).
-__global__ void k_keys(const double* __restrict__ x,
-                       const double* __restrict__ y, int* __restrict__ key,
-                       Geom G, const Scalars* S) {
+// Recomputes the cell key of every particle, with the slots in reference
+// order (idx = slot), after a merge/split emit or a state upload; the next
+// sort scans every cell.
+__global__ void k_keys(Particles p, Geom G, Scalars* S) {
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
-    const int r = cell_row(y[i], G.hy, G.nrows);
-    const int c = cell_col(x[i], G.hx, G.ncols);
-    key[i] = r + c * G.nrows;
+    const int r = cell_row(p.y[i], G.hy, G.nrows);
+    const int c = cell_col(p.x[i], G.hx, G.ncols);
+    p.key[i] = r + c * G.nrows;
+    p.idx[i] = i;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->knext[0] = 0;
+    S->knext[1] = G.nrows * G.ncols - 1;
   }
 }
 
@@ -214,7 +219,7 @@ __global__ void k_prep(ParticlesT<R> p, const double* __restrict__ Z, Geom G,
     R Ap, fbx, fby;
     if (derive) {
       Ap = hp > R(1.e-2) ? p.Vp[i] / hp : R(0);
-      voellmy<R>(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
+      rheology_friction<R>(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
       p.mp[i] = V2<R>{p.vpx[i] * p.Mp[i], p.vpy[i] * p.Mp[i]};
     } else {
       Ap = p.Ap[i];
@@ -255,12 +260,16 @@ __global__ void k_count(const int* __restrict__ key, int* __restrict__ count,
   }
 }
 
-// Exclusive scan of count[0..n) into start[0..n] in two passes over tiles of
-// kScanTile = 4 x kScanThreads items (each thread one int4): tile totals,
-// then per tile a block scan plus the scanned total of the preceding tiles.
-// count is zeroed on the way (ready for the next step).  When `list` is
-// given, cells holding two or more particles are appended to it (the cells
-// whose order k_segment_order has to establish).
+// Exclusive scan of count[0..n) into start[0..n], restricted to the tiles of
+// kScanTile = 4 x kScanThreads cells (each thread one int4) that meet the key
+// range [L, H] = krange U knext: the keys the starts describe and the keys
+// G2P produced since.  Outside that range no cell's count changed and every
+// start is either 0 (below every key) or np (above), as before, so the old
+// values stand.  k_scan_sums writes the tile totals; k_scan_apply adds, per
+// tile, the totals of the preceding tiles in the range to a block scan.
+// count is zeroed on the way (ready for the next step's atomics).  When
+// `list` is given, cells holding two or more particles are appended to it
+// (the cells whose order k_segment_order has to establish).
 __device__ __forceinline__ int block_incl_scan(int v, int* wsum) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int incl = v;
@@ -285,6 +294,17 @@ __device__ __forceinline__ int block_incl_scan(int v, int* wsum) {
   return incl + (w > 0 ? wsum[w - 1] : 0);
 }
 
+__device__ __forceinline__ int block_sum(int v, int* wsum) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += wsum[w];
+  __syncthreads();
+  return t;
+}
+
 __device__ __forceinline__ int4 load_count4(const int* count, int i0, int n) {
   if (i0 + 3 < n && (i0 & 3) == 0) return *reinterpret_cast<const int4*>(count + i0);
   int4 c;
@@ -295,55 +315,61 @@ __device__ __forceinline__ int4 load_count4(const int* count, int i0, int n) {
   return c;
 }
 
-__global__ void __launch_bounds__(kScanThreads)
-    k_scan_tiles(const int* __restrict__ count, int n, int* __restrict__ tile_sum,
-                 const Scalars* S) {
-  if (!S->active) return;
-  __shared__ int wsum[32];
-  const int i0 = blockIdx.x * kScanTile + threadIdx.x * 4;
-  const int4 c = load_count4(count, i0, n);
-  int v = c.x + c.y + c.z + c.w;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int t = (threadIdx.x < (blockDim.x >> 5)) ? wsum[threadIdx.x] : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (threadIdx.x == 0) tile_sum[blockIdx.x] = t;
+// tiles [t0, t1] meet the scan range (t0 > t1: none); ranged == 0: all
+__device__ __forceinline__ void scan_tiles_of(const Scalars* S, int n, int ranged, int& t0,
+                                              int& t1) {
+  if (!ranged) {
+    t0 = 0;
+    t1 = (n - 1) / kScanTile;
+    return;
   }
+  int L = min(S->krange[0], S->knext[0]);
+  int H = max(S->krange[1], S->knext[1]);
+  L = max(L, 0);
+  H = min(H, n - 1);
+  if (H < L) {
+    t0 = 1;
+    t1 = 0;
+    return;
+  }
+  t0 = L / kScanTile;
+  t1 = H / kScanTile;
 }
 
-// single block: exclusive scan of the tile sums in place; total at [ntiles]
 __global__ void __launch_bounds__(kScanThreads)
-    k_scan_tile_sums(int* __restrict__ tile_sum, int ntiles, const Scalars* S) {
+    k_scan_sums(const int* __restrict__ count, int n, int* __restrict__ tile_sum,
+                int* __restrict__ list_n, const Scalars* S, int ranged) {
   if (!S->active) return;
+  if (list_n && blockIdx.x == 0 && threadIdx.x < 3) list_n[threadIdx.x] = 0;
+  int t0, t1;
+  scan_tiles_of(S, n, ranged, t0, t1);
+  const int t = blockIdx.x;
+  if (t < t0 || t > t1) return;  // block-uniform
   __shared__ int wsum[32];
-  int carry = 0;
-  for (int base = 0; base < ntiles; base += blockDim.x) {
-    const int i = base + threadIdx.x;
-    const int v = (i < ntiles) ? tile_sum[i] : 0;
-    const int incl = block_incl_scan(v, wsum);
-    if (i < ntiles) tile_sum[i] = carry + incl - v;
-    const int total = wsum[(blockDim.x >> 5) - 1];
-    __syncthreads();
-    carry += total;
-  }
-  if (threadIdx.x == 0) tile_sum[ntiles] = carry;
+  const int4 c = load_count4(count, t * kScanTile + threadIdx.x * 4, n);
+  const int tot = block_sum(c.x + c.y + c.z + c.w, wsum);
+  if (threadIdx.x == 0) tile_sum[t] = tot;
 }
 
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_apply(int* __restrict__ count, int n, const int* __restrict__ tile_sum,
                  int* __restrict__ start, int* __restrict__ list,
-                 int* __restrict__ list_n, const Scalars* S) {
+                 int* __restrict__ list_n, const Scalars* S, int ranged) {
   if (!S->active) return;
+  int t0, t1;
+  scan_tiles_of(S, n, ranged, t0, t1);
+  const int t = blockIdx.x;
+  if (t < t0 || t > t1) return;  // block-uniform
   __shared__ int wsum[32];
-  const int i0 = blockIdx.x * kScanTile + threadIdx.x * 4;
+  // particles in the range's tiles before this one
+  int pre = 0;
+  for (int q = t0 + threadIdx.x; q < t; q += blockDim.x) pre += tile_sum[q];
+  pre = block_sum(pre, wsum);
+  const int i0 = t * kScanTile + threadIdx.x * 4;
   const int4 c = load_count4(count, i0, n);
   const int v = c.x + c.y + c.z + c.w;
   const int incl = block_incl_scan(v, wsum);
-  const int e0 = tile_sum[blockIdx.x] + incl - v;
+  const int e0 = pre + incl - v;
   int4 o;
   o.x = e0;
   o.y = e0 + c.x;
@@ -367,64 +393,78 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
     for (int k = 0; k < 4; ++k) mine += cv[k] >= 2 ? 1 : 0;
     const int lane = threadIdx.x & 31;
-    int incl = mine;
+    int incl2 = mine;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
+    for (int o2 = 1; o2 < 32; o2 <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl2, o2);
+      if (lane >= o2) incl2 += u;
     }
-    const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+    const int wtot = __shfl_sync(0xffffffffu, incl2, 31);
     int base = 0;
     if (lane == 31 && wtot > 0) base = atomicAdd(list_n, wtot);
     base = __shfl_sync(0xffffffffu, base, 31);
-    int q = base + incl - mine;
+    int q = base + incl2 - mine;
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       if (cv[k] >= 2) list[q++] = i0 + k;
   }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[n] = tile_sum[gridDim.x];
+  // start[n]: the total (with a key range: every particle, unchanged by a
+  // step; written whenever the range reaches the last tile)
+  if (t == (n - 1) / kScanTile && threadIdx.x == blockDim.x - 1) start[n] = pre + incl;
 }
 
+// perm[start[key] + slot] = the storage slot, and skey there the key (the
+// cell of each sorted position, which G2P reads without waiting for perm);
+// block 0 then rolls the key ranges over: the starts now describe knext,
+// and the next G2P starts an empty knext.
 __global__ void k_scatter(const int* __restrict__ key,
                           const int* __restrict__ slot,
                           const int* __restrict__ start, int* __restrict__ perm,
-                          const Scalars* S) {
+                          int* __restrict__ skey, Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
-       i += gridDim.x * blockDim.x)
-    perm[start[key[i]] + slot[i]] = i;
-}
-
-// list_n[0]: cells with two or more particles; list_n[1]: crowded cells
-// handed on to k_segment_order_big; list_n[2]: cells of more than
-// kThreadSort particles handed on to k_segment_order_mid
-__global__ void k_list_reset(int* list_n, const Scalars* S) {
-  if (threadIdx.x == 0 && blockIdx.x == 0 && S->active) {
-    list_n[0] = 0;
-    list_n[1] = 0;
-    list_n[2] = 0;
+       i += gridDim.x * blockDim.x) {
+    const int k = key[i];
+    const int pos = start[k] + slot[i];
+    perm[pos] = i;
+    skey[pos] = k;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->krange[0] = S->knext[0];
+    S->krange[1] = S->knext[1];
+    S->knext[0] = 0x7fffffff;
+    S->knext[1] = -1;
   }
 }
 
-// Orders each listed cell's segment by ascending particle index (the atomics
-// of k_count hand out slots in arbitrary order).  k_segment_order: each lane
-// sorts a cell of up to kThreadSort particles in registers (a bitonic
-// network over static indices) and hands larger cells on to `mid`.
-// k_segment_order_mid, one warp per cell: a register bitonic sort across the
-// lanes for up to 32 particles, a rank sort for up to 32 * kRankPer (each
-// lane holds kRankPer indices and counts, over all the cell's indices
-// broadcast lane by lane, those below each of its own; particle indices are
-// unique, so the ranks are a permutation of [0, m)); larger cells go on to
-// `big` for k_segment_order_big.
+// Orders each listed cell's segment of perm (storage slots) by the
+// particles' reference index idx[slot] (the atomics of the count hand out
+// slots in arbitrary order).  A segment entry is handled as the 64-bit
+// value idx << 32 | slot, so sorting those values orders by reference index
+// (unique) and carries the slot along.  k_segment_order: each lane sorts a
+// cell of up to kThreadSort particles in registers (a bitonic network over
+// static indices) and hands larger cells on to `mid`.  k_segment_order_mid,
+// one warp per cell: a register bitonic sort across the lanes for up to 32
+// particles, a rank sort for up to 32 * kRankPer (each lane holds kRankPer
+// values and counts, over all the cell's values broadcast lane by lane,
+// those below each of its own; the values are unique, so the ranks are a
+// permutation of [0, m)); larger cells go on to `big` for
+// k_segment_order_big.
 constexpr int kThreadSort = 16;
 constexpr int kRankPer = 8;
-constexpr int kBigRun = 8192;
+constexpr int kBigRun = 4096;
+constexpr unsigned long long kNoEntry = ~0ull;
 
-__device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m) {
-  int v[kThreadSort];
+__device__ __forceinline__ unsigned long long seg_entry(const int* __restrict__ idx, int s) {
+  return ((unsigned long long)(unsigned)idx[s] << 32) | (unsigned)s;
+}
+
+__device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m,
+                                                    const int* __restrict__ idx) {
+  unsigned long long v[kThreadSort];
 #pragma unroll
-  for (int k = 0; k < kThreadSort; ++k) v[k] = k < m ? seg[k] : 0x7fffffff;
+  for (int k = 0; k < kThreadSort; ++k) v[k] = k < m ? seg_entry(idx, seg[k]) : kNoEntry;
 #pragma unroll
   for (int k = 2; k <= kThreadSort; k <<= 1) {
 #pragma unroll
@@ -433,49 +473,53 @@ __device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m
       for (int i = 0; i < kThreadSort; ++i) {
         const int l = i ^ j;
         if (l > i) {
-          const int a = v[i], b = v[l];
+          const unsigned long long a = v[i], b = v[l];
           const bool up = (i & k) == 0;
-          v[i] = up ? min(a, b) : max(a, b);
-          v[l] = up ? max(a, b) : min(a, b);
+          const bool sw = up ? (a > b) : (a < b);
+          v[i] = sw ? b : a;
+          v[l] = sw ? a : b;
         }
       }
     }
   }
 #pragma unroll
   for (int k = 0; k < kThreadSort; ++k)
-    if (k < m) seg[k] = v[k];
+    if (k < m) seg[k] = int(unsigned(v[k]));
 }
 
 __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b, int m,
-                                                  int c, int lane, int* __restrict__ big,
+                                                  int c, int lane,
+                                                  const int* __restrict__ idx,
+                                                  int* __restrict__ big,
                                                   int* __restrict__ list_n) {
   if (m <= 32) {
-    int v = (lane < m) ? perm[b + lane] : 0x7fffffff;
+    unsigned long long v = (lane < m) ? seg_entry(idx, perm[b + lane]) : kNoEntry;
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
       for (int j = k >> 1; j > 0; j >>= 1) {
-        const int o = __shfl_xor_sync(0xffffffffu, v, j);
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, j);
         const bool up = ((lane & k) == 0);
         const bool lower = ((lane & j) == 0);
         // keep the min in the lower lane of an ascending pair
         v = (lower == up) ? min(v, o) : max(v, o);
       }
     }
-    if (lane < m) perm[b + lane] = v;
+    if (lane < m) perm[b + lane] = int(unsigned(v));
   } else if (m <= 32 * kRankPer) {
-    int v[kRankPer], rank[kRankPer];
+    unsigned long long v[kRankPer];
+    int rank[kRankPer];
 #pragma unroll
     for (int t = 0; t < kRankPer; ++t) {
       const int q = lane + 32 * t;
-      v[t] = (q < m) ? perm[b + q] : 0x7fffffff;
+      v[t] = (q < m) ? seg_entry(idx, perm[b + q]) : kNoEntry;
       rank[t] = 0;
     }
 #pragma unroll
     for (int t2 = 0; t2 < kRankPer; ++t2) {
       if (32 * t2 >= m) break;  // warp-uniform
       for (int src = 0; src < 32; ++src) {
-        const int o = __shfl_sync(0xffffffffu, v[t2], src);
+        const unsigned long long o = __shfl_sync(0xffffffffu, v[t2], src);
 #pragma unroll
         for (int t = 0; t < kRankPer; ++t) rank[t] += (o < v[t]) ? 1 : 0;
       }
@@ -483,7 +527,7 @@ __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b,
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < kRankPer; ++t)
-      if (lane + 32 * t < m) perm[b + rank[t]] = v[t];
+      if (lane + 32 * t < m) perm[b + rank[t]] = int(unsigned(v[t]));
   } else if (lane == 0) {
     big[atomicAdd(&list_n[1], 1)] = c;
   }
@@ -493,8 +537,8 @@ __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b,
 __global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict__ start,
                                 const int* __restrict__ list,
                                 int* __restrict__ list_n,
-                                int* __restrict__ perm, int* __restrict__ mid,
-                                const Scalars* S) {
+                                int* __restrict__ perm, const int* __restrict__ idx,
+                                int* __restrict__ mid, const Scalars* S) {
   if (!S->active) return;
   const int lane = threadIdx.x & 31;
   const int nl = list_n[0];
@@ -508,7 +552,7 @@ __global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict_
       m = start[c + 1] - b;
     }
     if (m <= kThreadSort) {
-      if (m >= 2) thread_sort_segment(perm + b, m);
+      if (m >= 2) thread_sort_segment(perm + b, m, idx);
     }
     // larger cells: one atomic per warp
     const unsigned larger = __ballot_sync(0xffffffffu, m > kThreadSort);
@@ -521,11 +565,11 @@ __global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict_
   }
 }
 
-__global__ void __launch_bounds__(256, 8) k_segment_order_mid(const int* __restrict__ start,
+__global__ void __launch_bounds__(256, 4) k_segment_order_mid(const int* __restrict__ start,
                                     const int* __restrict__ mid,
                                     int* __restrict__ list_n,
-                                    int* __restrict__ perm, int* __restrict__ big,
-                                    const Scalars* S) {
+                                    int* __restrict__ perm, const int* __restrict__ idx,
+                                    int* __restrict__ big, const Scalars* S) {
   if (!S->active) return;
   const int lane = threadIdx.x & 31;
   const int nm = list_n[2];
@@ -533,22 +577,24 @@ __global__ void __launch_bounds__(256, 8) k_segment_order_mid(const int* __restr
        w += (gridDim.x * blockDim.x) >> 5) {
     const int c = mid[w];
     const int b = start[c];
-    warp_sort_segment(perm, b, start[c + 1] - b, c, lane, big, list_n);
+    warp_sort_segment(perm, b, start[c + 1] - b, c, lane, idx, big, list_n);
   }
 }
 
 // Crowded cells (more than 32 * kRankPer particles), one block of 1024
-// threads each: runs of up to kBigRun indices are sorted by a bitonic network
-// in shared memory; longer cells then merge the sorted runs pairwise (each
-// output position finds its split by a binary search along the merge path),
-// ping-ponging between perm and tmp (the sort's slot array, free once the
-// scatter has run).
+// threads each: the cell's entries (idx << 32 | slot) go to tmp[b, b+m);
+// runs of up to kBigRun are sorted by a bitonic network in shared memory;
+// longer cells then merge the sorted runs pairwise (each output position
+// finds its split by a binary search along the merge path), ping-ponging
+// between tmp[b, b+m) and tmp[cap + b, cap + b + m); the slots go back to
+// perm.
 __global__ void __launch_bounds__(1024)
     k_segment_order_big(const int* __restrict__ start, const int* __restrict__ big,
                         const int* __restrict__ list_n, int* __restrict__ perm,
-                        int* __restrict__ tmp, const Scalars* S) {
+                        const int* __restrict__ idx, unsigned long long* __restrict__ tmp,
+                        long long cap, const Scalars* S) {
   if (!S->active) return;
-  __shared__ int sv[kBigRun];
+  __shared__ unsigned long long sv[kBigRun];
   const int nb = list_n[1];
   for (int q = blockIdx.x; q < nb; q += gridDim.x) {
     const int c = big[q];
@@ -558,14 +604,14 @@ __global__ void __launch_bounds__(1024)
       int P = 1;
       while (P < len) P <<= 1;
       for (int i = threadIdx.x; i < P; i += blockDim.x)
-        sv[i] = (i < len) ? perm[b + r0 + i] : 0x7fffffff;
+        sv[i] = (i < len) ? seg_entry(idx, perm[b + r0 + i]) : kNoEntry;
       __syncthreads();
       for (int k = 2; k <= P; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
           for (int i = threadIdx.x; i < P; i += blockDim.x) {
             const int ixj = i ^ j;
             if (ixj > i) {
-              const int a = sv[i], d = sv[ixj];
+              const unsigned long long a = sv[i], d = sv[ixj];
               if ((a > d) == ((i & k) == 0)) {
                 sv[i] = d;
                 sv[ixj] = a;
@@ -575,17 +621,17 @@ __global__ void __launch_bounds__(1024)
           __syncthreads();
         }
       }
-      for (int i = threadIdx.x; i < len; i += blockDim.x) perm[b + r0 + i] = sv[i];
+      for (int i = threadIdx.x; i < len; i += blockDim.x) tmp[b + r0 + i] = sv[i];
       __syncthreads();
     }
-    int* src = perm + b;
-    int* dst = tmp + b;
+    unsigned long long* src = tmp + b;
+    unsigned long long* dst = tmp + cap + b;
     for (int w = kBigRun; w < m; w <<= 1) {
       for (int k = threadIdx.x; k < m; k += blockDim.x) {
         const int lo = (k / (2 * w)) * (2 * w);
         const int la = min(w, m - lo), lb = max(0, min(w, m - lo - la));
-        const int* A = src + lo;
-        const int* B = A + la;
+        const unsigned long long* A = src + lo;
+        const unsigned long long* B = A + la;
         const int kk = k - lo;
         int i0 = max(0, kk - lb), i1 = min(kk, la);
         while (i0 < i1) {
@@ -596,13 +642,11 @@ __global__ void __launch_bounds__(1024)
         dst[k] = (j >= lb || (i0 < la && A[i0] < B[j])) ? A[i0] : B[j];
       }
       __syncthreads();
-      int* t = src;
+      unsigned long long* t = src;
       src = dst;
       dst = t;
     }
-    if (src != perm + b) {
-      for (int i = threadIdx.x; i < m; i += blockDim.x) perm[b + i] = src[i];
-    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) perm[b + i] = int(unsigned(src[i]));
     __syncthreads();
   }
 }
@@ -1334,21 +1378,25 @@ __global__ void k_ledger_final(const double* __restrict__ led_part,
 // cell of the step start, height update, Bingham stress, next cell key and
 // the CFL max-reductions (main/optim_par.cpp:532-651).
 // ---------------------------------------------------------------------------
-// One particle of G2P (the body of k_g2p and of the batched G2P).  key_off
-// is added to the cell key (the scenario's first cell in a batch).
+// One particle of G2P (the body of k_g2p and of the batched G2P): the
+// particle in slot `s` of the step-start buffer `src`, binned to cell `key`,
+// written to slot `j` of `dst` (its position in this step's sorted order).
+// key_off is the scenario's first cell in a batch (its cell keys are offset
+// by it); the new key is returned in `nkey`.
 template <class R>
 __device__ __forceinline__ void g2p_particle(
-    const ParticlesT<R>& p, int i, const NodesT<R>& nodes, const double* __restrict__ Z,
-    const Geom& G, const Phys& P, const ShapeT<R>& sh, double dtd, int record,
-    int want_grad, int key_off, unsigned long long& m0, unsigned long long& m1,
-    unsigned long long& m2) {
+    const ParticlesT<R>& src, int s, int key_in, const ParticlesT<R>& dst, int j,
+    const NodesT<R>& nodes, const double* __restrict__ Z, const Geom& G, const Phys& P,
+    const ShapeT<R>& sh, double dtd, int record, int want_grad, int key_off,
+    unsigned long long& m0, unsigned long long& m1, unsigned long long& m2, int& bad,
+    int& nkey) {
   const int nrows = G.nrows, ncols = G.ncols;
   const double hx = G.hx, hy = G.hy;
   const R ihx = sh.ihx, mihx = sh.mihx;
   const R ihy = sh.ihy, mihy = sh.mihy;
   const R eps = R(1e-10);
   const R dt = R(dtd);
-  const int key = p.key[i] - key_off;
+  const int key = key_in - key_off;
   const int r = key % nrows, c = key / nrows;
   int nd[4];
   R vxn[4], vyn[4];
@@ -1359,7 +1407,7 @@ __device__ __forceinline__ void g2p_particle(
     vxn[k] = v.x;
     vyn[k] = v.y;
   }
-  R x = p.x[i], y = p.y[i];
+  R x = src.x[s], y = src.y[s];
   R xi, eta;
   local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
   R vxL = R(0), vyL = R(0);
@@ -1384,15 +1432,15 @@ __device__ __forceinline__ void g2p_particle(
       dzx += double(shg_x(eta, k, ihx, mihx)) * zn;
       dzy += double(shg_y(xi, k, ihy, mihy)) * zn;
     }
-    p.apx[i] = ax;
-    p.apy[i] = ay;
-    p.dZxp[i] = R(dzx);
-    p.dZyp[i] = R(dzy);
-    const V2<R> qg = p.qg[i], qf = p.qf[i];
-    p.Fpx[i] = qg.x;
-    p.Fpy[i] = qg.y;
-    p.Frx[i] = qf.x;
-    p.Fry[i] = qf.y;
+    dst.apx[j] = ax;
+    dst.apy[j] = ay;
+    dst.dZxp[j] = R(dzx);
+    dst.dZyp[j] = R(dzy);
+    const V2<R> qg = src.qg[s], qf = src.qf[s];
+    dst.Fpx[j] = qg.x;
+    dst.Fpy[j] = qg.y;
+    dst.Frx[j] = qf.x;
+    dst.Fry[j] = qf.y;
   }
   const R vpx = vxL, vpy = vyL;
   x = x + dt * vpx;
@@ -1415,55 +1463,136 @@ __device__ __forceinline__ void g2p_particle(
   }
   // height from the strain rate (main/optim_par.cpp:595-599)
   const R div = vxdx + vydy;
-  R hp = p.hp[i];
+  R hp = src.hp[s];
   hp = hp / (R(1) + dt * div);
   hp = hp < R(1e-2) ? R(1e-2) : hp;
   R F11, F12, F22;
-  const R H = p.H[i];
-  bingham_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
-  p.x[i] = x;
-  p.y[i] = y;
-  p.vpx[i] = vpx;
-  p.vpy[i] = vpy;
-  p.hp[i] = hp;
-  p.F11[i] = F11;
-  p.F12[i] = F12;
-  p.F22[i] = F22;
+  const R H = src.H[s];
+  const R Mp = src.Mp[s], Vp = src.Vp[s];
+  rheology_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
+  dst.x[j] = x;
+  dst.y[j] = y;
+  dst.vpx[j] = vpx;
+  dst.vpy[j] = vpy;
+  dst.hp[j] = hp;
+  dst.F11[j] = F11;
+  dst.F12[j] = F12;
+  dst.F22[j] = F22;
+  dst.Mp[j] = Mp;
+  dst.Vp[j] = Vp;
+  dst.H[j] = H;
+  dst.idx[j] = src.idx[s];
   const int nr = cell_row(double(y), hy, nrows), ncl = cell_col(double(x), hx, ncols);
-  p.key[i] = nr + ncl * nrows + key_off;
+  nkey = nr + ncl * nrows + key_off;
+  dst.key[j] = nkey;
   if (want_grad) {
-    p.vpx_dx[i] = vxdx;
-    p.vpx_dy[i] = vxdy;
-    p.vpy_dx[i] = vydx;
-    p.vpy_dy[i] = vydy;
+    dst.vpx_dx[j] = vxdx;
+    dst.vpx_dy[j] = vxdy;
+    dst.vpy_dx[j] = vydx;
+    dst.vpy_dy[j] = vydy;
   }
   // the record of the next P2G: what the reference stores at the end of
   // the step (main/optim_par.cpp:600-626: momentum, Ap, basal friction) and
   // the local coordinates and gravity force in the cell of the next
   // binning (:387,447-454)
   {
-    const R Mp = p.Mp[i], Vp = p.Vp[i];
-    p.mp[i] = V2<R>{vpx * Mp, vpy * Mp};
+    dst.mp[j] = V2<R>{vpx * Mp, vpy * Mp};
     const R Ap = hp > R(1.e-2) ? Vp / hp : R(0);
     R fbx, fby;
-    voellmy(P, vpx, vpy, hp, fbx, fby);
-    p.qf[i] = V2<R>{Ap * fbx, Ap * fby};
+    rheology_friction(P, vpx, vpy, hp, fbx, fby);
+    dst.qf[j] = V2<R>{Ap * fbx, Ap * fby};
     R qxi, qeta, qgx, qgy;
     next_record(G, P, Z, x, y, hp, H, Vp, qxi, qeta, qgx, qgy);
-    p.xe[i] = V2<R>{qxi, qeta};
-    p.qg[i] = V2<R>{qgx, qgy};
+    dst.xe[j] = V2<R>{qxi, qeta};
+    dst.qg[j] = V2<R>{qgx, qgy};
   }
   if (record) {
     // g2p Z -> Zp at the new position, old cell (main/optim_par.cpp:642)
     double zp = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) zp += double(shp(xi, eta, k)) * Z[nd[k]];
-    p.Zp[i] = R(zp);
-    p.hpZ[i] = R(double(hp) + zp);
+    dst.Zp[j] = R(zp);
+    dst.hpZ[j] = R(double(hp) + zp);
   }
   m0 = max(m0, ordered_key(double(fabs(vpx))));
   m1 = max(m1, ordered_key(double(fabs(vpy))));
   m2 = max(m2, ordered_key(double(hp)));
+  // a diverged particle (NaN/inf anywhere in the state a step carries, or a
+  // negative depth) stops its scenario through the status word
+  bad |= !(isfinite(x) && isfinite(y) && isfinite(vpx) && isfinite(vpy) &&
+           isfinite(hp) && hp >= R(0));
+}
+
+// Copies the moving fields of slot s of src to slot j of dst (a particle
+// that does not step in this pass, or the reordering into reference order).
+template <class R>
+__device__ __forceinline__ void copy_moving(const ParticlesT<R>& src, int s,
+                                            const ParticlesT<R>& dst, int j) {
+  dst.x[j] = src.x[s];
+  dst.y[j] = src.y[s];
+  dst.vpx[j] = src.vpx[s];
+  dst.vpy[j] = src.vpy[s];
+  dst.hp[j] = src.hp[s];
+  dst.F11[j] = src.F11[s];
+  dst.F12[j] = src.F12[s];
+  dst.F22[j] = src.F22[s];
+  dst.Mp[j] = src.Mp[s];
+  dst.Vp[j] = src.Vp[s];
+  dst.H[j] = src.H[s];
+  dst.key[j] = src.key[s];
+  dst.idx[j] = src.idx[s];
+  dst.slot[j] = src.slot[s];
+  dst.mp[j] = src.mp[s];
+  dst.qf[j] = src.qf[s];
+  dst.xe[j] = src.xe[s];
+  dst.qg[j] = src.qg[s];
+  if (src.vpx_dx) {
+    dst.vpx_dx[j] = src.vpx_dx[s];
+    dst.vpx_dy[j] = src.vpx_dy[s];
+    dst.vpy_dx[j] = src.vpy_dx[s];
+    dst.vpy_dy[j] = src.vpy_dy[s];
+  }
+}
+
+// Raises kStatusNonFinite in S when any thread of the block saw a diverged
+// particle (all threads of the block call it).
+__device__ __forceinline__ void flag_non_finite(int bad, Scalars* S) {
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&S->status, kStatusNonFinite);
+}
+
+// The counting sort's first step for the next binning, done where the keys
+// are made: particle j of a warp takes slot[j] among its cell's particles,
+// one atomic per cell and warp (the lanes that share a cell take
+// consecutive slots).  All 32 lanes call it; ok == false lanes take part
+// without a particle.
+__device__ __forceinline__ void count_key(int k, bool ok, int* __restrict__ count,
+                                          int* __restrict__ slot_out) {
+  const int lane = threadIdx.x & 31;
+  const int kk = ok ? k : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, kk);
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (ok && lane == leader) base = atomicAdd(&count[kk], __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (ok) *slot_out = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+// Block min/max of the new keys into knext (the scan range of the next
+// sort); all threads of the block call it.
+__device__ __forceinline__ void key_range(int kmin, int kmax, int* sred, Scalars* S) {
+  for (int o = 16; o > 0; o >>= 1) {
+    kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+    kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&sred[0], kmin);
+    atomicMax(&sred[1], kmax);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && sred[1] >= 0) {
+    atomicMin(&S->knext[0], sred[0]);
+    atomicMax(&S->knext[1], sred[1]);
+  }
 }
 
 // Block reduction of the CFL maxima into one scenario's next-step slots.
@@ -1491,34 +1620,73 @@ __device__ __forceinline__ void cfl_block_max(unsigned long long m0,
 }
 
 // kRecord / kGrad: the output fields and the velocity gradients are
-// written (compiled out of the plain step)
+// written (compiled out of the plain step).  Thread j takes the particle
+// at position j of this step's sorted order: slot perm[j] of `cur`, written
+// to slot j of `nxt`.  A pass whose loop condition failed copies `cur` to
+// `nxt` unchanged (the host exchanges the buffers after every pass).
 template <bool kRecord, bool kGrad>
 __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
-    k_g2p_t(Particles p, Nodes nodes, const double* __restrict__ Z, Geom G,
-            Phys P, Scalars* S) {
-  if (!S->active) return;
-  __shared__ unsigned long long red[3];
-  if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
-  __syncthreads();
+    k_g2p_t(Particles cur, Particles nxt, const int* __restrict__ perm,
+            const int* __restrict__ skey, Nodes nodes, const double* __restrict__ Z, Geom G,
+            Phys P, Scalars* S, int* __restrict__ count) {
   const int np = S->np;
+  const int stride = gridDim.x * blockDim.x;
+  if (!S->active) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += stride)
+      copy_moving(cur, j, nxt, j);
+    return;
+  }
+  __shared__ unsigned long long red[3];
+  __shared__ int kred[2];
+  if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
+  if (threadIdx.x == 0) {
+    kred[0] = 0x7fffffff;
+    kred[1] = -1;
+  }
+  __syncthreads();
   const double dt = S->dt;
   const Shape sh{1.0 / G.hx, -1.0 / G.hx, 1.0 / G.hy, -1.0 / G.hy};
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
-       i += gridDim.x * blockDim.x)
-    g2p_particle(p, i, nodes, Z, G, P, sh, dt, kRecord ? 1 : 0, kGrad ? 1 : 0, 0, m0, m1,
-                 m2);
+  int bad = 0, kmin = 0x7fffffff, kmax = -1;
+  const int lane = threadIdx.x & 31;
+  for (int j0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); j0 < np; j0 += stride) {
+    const int j = j0 + lane;
+    const bool ok = j < np;
+    int nkey = -1;
+    if (ok) {
+      g2p_particle(cur, perm[j], skey[j], nxt, j, nodes, Z, G, P, sh, dt, kRecord ? 1 : 0,
+                   kGrad ? 1 : 0, 0, m0, m1, m2, bad, nkey);
+      kmin = min(kmin, nkey);
+      kmax = max(kmax, nkey);
+    }
+    count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
+  }
   cfl_block_max(m0, m1, m2, red, S);
+  key_range(kmin, kmax, kred, S);
+  flag_non_finite(bad, S);
 }
 
-void launch_g2p(int grid, cudaStream_t st, Particles p, Nodes nodes, const double* Z,
-                Geom G, Phys P, Scalars* S, int record, int want_grad) {
+void launch_g2p(int grid, cudaStream_t st, Particles cur, Particles nxt, const int* perm,
+                const int* skey, Nodes nodes, const double* Z, Geom G, Phys P, Scalars* S,
+                int* count, int record, int want_grad) {
   if (record)
-    k_g2p_t<true, true><<<grid, kG2PThreads, 0, st>>>(p, nodes, Z, G, P, S);
+    k_g2p_t<true, true><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, nodes, Z, G, P,
+                                                       S, count);
   else if (want_grad)
-    k_g2p_t<false, true><<<grid, kG2PThreads, 0, st>>>(p, nodes, Z, G, P, S);
+    k_g2p_t<false, true><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, nodes, Z, G, P,
+                                                        S, count);
   else
-    k_g2p_t<false, false><<<grid, kG2PThreads, 0, st>>>(p, nodes, Z, G, P, S);
+    k_g2p_t<false, false><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, nodes, Z, G,
+                                                         P, S, count);
+}
+
+// Storage into reference order: the particle in slot j of src goes to slot
+// idx[j] of dst (merge/split works in reference order).
+template <class R>
+__global__ void k_unsort(ParticlesT<R> src, ParticlesT<R> dst, const Scalars* S) {
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x)
+    copy_moving(src, j, dst, src.idx[j]);
 }
 
 size_t p2g_smem_bytes() { return sizeof(P2GSmemT<double>); }
@@ -1675,32 +1843,63 @@ __global__ void k_b_ledger(const double* __restrict__ led_part,
   ledger_reduce(led_part, scn_units[s].x, scn_units[s].y, &S[s]);
 }
 
-// gblk[b] = {scenario, its first particle handled by block b}
+// gblk[b] = {scenario, its first particle handled by block b}.  A
+// scenario's particles are positions [p_off, p_off + np) of the sorted order
+// (its cell keys lie between those of the scenarios before and after it).
+// Thread j takes position j: slot perm[j] of `cur`, written to slot j of
+// `nxt`; a scenario that does not step in this pass (finished, stopped or
+// removed) is copied through in sorted order and counted for the next sort;
+// a pass in which no scenario steps copies `cur` to `nxt` unchanged.
 template <class R>
 __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
-    k_b_g2p(ParticlesT<R> p, const V2<R>* __restrict__ vvL, const double* __restrict__ Z,
+    k_b_g2p(ParticlesT<R> cur, ParticlesT<R> nxt, const int* __restrict__ perm,
+            const int* __restrict__ skey, const V2<R>* __restrict__ vvL,
+            const double* __restrict__ Z,
             const Scn* __restrict__ scn, Scalars* S, const int2* __restrict__ gblk,
-            const Scalars* Sg) {
-  if (!Sg->active) return;
+            Scalars* Sg, int* __restrict__ count) {
   const int2 e = gblk[blockIdx.x];
   const int s = e.x;
-  if (!S[s].active) return;  // block-uniform
+  const int p_off = scn[s].p_off, np = scn[s].np;
+  const int li = e.y + threadIdx.x;
+  const int j = p_off + li;
+  const bool ok = li < np;
+  if (!Sg->active) {
+    if (ok) copy_moving(cur, j, nxt, j);
+    return;
+  }
   __shared__ unsigned long long red[3];
+  __shared__ int kred[2];
   if (threadIdx.x < 3) red[threadIdx.x] = 0ull;
+  if (threadIdx.x == 0) {
+    kred[0] = 0x7fffffff;
+    kred[1] = -1;
+  }
   __syncthreads();
+  int nkey = -1;
+  if (!S[s].active) {  // block-uniform
+    if (ok) {
+      copy_moving(cur, perm[j], nxt, j);
+      nkey = nxt.key[j];
+    }
+    count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
+    key_range(ok ? nkey : 0x7fffffff, ok ? nkey : -1, kred, Sg);
+    return;
+  }
   const Geom G = scn[s].G;
   const Phys P = scn[s].P;
-  const int p_off = scn[s].p_off, np = scn[s].np;
   const int n_off = scn[s].n_off, c_off = scn[s].c_off;
   NodesT<R> nd{};
   nd.vvL = const_cast<V2<R>*>(vvL) + n_off;
   const ShapeT<R> sh{R(1) / R(G.hx), -R(1) / R(G.hx), R(1) / R(G.hy), -R(1) / R(G.hy)};
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
-  const int li = e.y + threadIdx.x;
-  if (li < np)
-    g2p_particle(p, p_off + li, nd, Z + n_off, G, P, sh, S[s].dt, 0, 0, c_off, m0,
-                 m1, m2);
+  int bad = 0;
+  if (ok)
+    g2p_particle(cur, perm[j], skey[j], nxt, j, nd, Z + n_off, G, P, sh, S[s].dt, 0, 0,
+                 c_off, m0, m1, m2, bad, nkey);
+  count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
   cfl_block_max(m0, m1, m2, red, &S[s]);
+  key_range(ok ? nkey : 0x7fffffff, ok ? nkey : -1, kred, Sg);
+  flag_non_finite(bad, &S[s]);
 }
 
 // Compaction of a batch into the other half of its double buffer:
@@ -1711,19 +1910,20 @@ __global__ void k_b_move(ParticlesT<R> dst, ParticlesT<R> src, const int4* __res
   const int4 m = mblk[blockIdx.x];
   if ((int)threadIdx.x >= m.z) return;
   const int i = m.y + threadIdx.x, o = m.x + threadIdx.x;
-  R* const* df[] = {&dst.x,  &dst.y,  &dst.vpx, &dst.vpy, &dst.hp, &dst.F11, &dst.F12,
-                    &dst.F22, &dst.Mp, &dst.Vp, &dst.H, &dst.Ap, &dst.Fbx, &dst.Fby};
-  R* const* sf[] = {&src.x,  &src.y,  &src.vpx, &src.vpy, &src.hp, &src.F11, &src.F12,
-                    &src.F22, &src.Mp, &src.Vp, &src.H, &src.Ap, &src.Fbx, &src.Fby};
-#pragma unroll
-  for (int f = 0; f < 14; ++f) (*df[f])[o] = (*sf[f])[i];
-  V2<R>* const* dv[] = {&dst.mp, &dst.qf, &dst.xe, &dst.qg};
-  V2<R>* const* sv[] = {&src.mp, &src.qf, &src.xe, &src.qg};
-#pragma unroll
-  for (int f = 0; f < 4; ++f) (*dv[f])[o] = (*sv[f])[i];
-  dst.label[o] = src.label[i];
-  dst.level[o] = src.level[i];
+  copy_moving(src, i, dst, o);
   dst.key[o] = src.key[i] + m.w;
+}
+
+// Slots and counts of the keys [0, n) (after an upload or a compaction).
+__global__ void k_count_n(const int* __restrict__ key, int* __restrict__ count,
+                          int* __restrict__ slot, int n) {
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
+    const int i = i0 + lane;
+    const bool ok = i < n;
+    count_key(ok ? key[i] : -1, ok, count, slot + (ok ? i : 0));
+  }
 }
 
 // nblk[b] = {destination first node, source first node, count <= 256, 0}
@@ -1735,14 +1935,15 @@ __global__ void k_b_move_nodes(double* __restrict__ dst, const double* __restric
 
 // HV: p2g of the updated depth hp at the updated positions, each particle
 // still in the cell it was binned to at the start of the step
-// (main/optim_par.cpp:650, after the vars were zeroed at :362-364).  One
-// thread per node walks its four cells in id order -- (r-1,c-1) local 3,
-// (r,c-1) local 2, (r-1,c) local 1, (r,c) local 0 -- and each cell's
-// particles in index order (this step's perm), the quadgrid cell-sweep order.
-// Output-only: launched when outputs are recorded.
-__global__ void k_hv(const Particles p, const int* __restrict__ perm,
-                     const int* __restrict__ cstart, double* __restrict__ HV,
-                     Geom G, const Scalars* S) {
+// (main/optim_par.cpp:650, after the vars were zeroed at :362-364).  `p` is
+// the buffer this step's G2P wrote, in this step's sorted order, so the
+// particles of a cell are the slots [cstart[cell], cstart[cell+1]) in
+// reference index order.  One thread per node walks its four cells in id
+// order -- (r-1,c-1) local 3, (r,c-1) local 2, (r-1,c) local 1, (r,c) local
+// 0 -- the quadgrid cell-sweep order.  Output-only: launched when outputs
+// are recorded.
+__global__ void k_hv(const Particles p, const int* __restrict__ cstart,
+                     double* __restrict__ HV, Geom G, const Scalars* S) {
   if (!S->active) return;
   const int nrows = G.nrows, ncols = G.ncols;
   const int nn = (nrows + 1) * (ncols + 1);
@@ -1761,10 +1962,9 @@ __global__ void k_hv(const Particles p, const int* __restrict__ perm,
       if (cr < 0 || cr >= nrows || cc < 0 || cc >= ncols) continue;
       const int cell = cr + cc * nrows;
       for (int j = cstart[cell]; j < cstart[cell + 1]; ++j) {
-        const int i = perm[j];
         double xi, eta;
-        local_xy_g(p.x[i], p.y[i], cc, cr, G, ihx, ihy, xi, eta);
-        acc += shp(xi, eta, inode) * p.hp[i];
+        local_xy_g(p.x[j], p.y[j], cc, cr, G, ihx, ihy, xi, eta);
+        acc += shp(xi, eta, inode) * p.hp[j];
       }
     }
     HV[n] = acc;
@@ -1809,10 +2009,17 @@ int setup_b_p2g() {
 }
 
 template <class R>
-void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> p, const V2<R>* vvL,
-                  const double* Z, const Scn* scn, Scalars* S,
-                  const int2* gblk, const Scalars* Sg) {
-  k_b_g2p<R><<<grid, kG2PThreads, 0, st>>>(p, vvL, Z, scn, S, gblk, Sg);
+void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> cur, ParticlesT<R> nxt,
+                  const int* perm, const int* skey, const V2<R>* vvL, const double* Z,
+                  const Scn* scn, Scalars* S, const int2* gblk, Scalars* Sg, int* count) {
+  k_b_g2p<R><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, vvL, Z, scn, S, gblk, Sg,
+                                           count);
+}
+
+template <class R>
+void launch_unsort(int grid, cudaStream_t st, ParticlesT<R> src, ParticlesT<R> dst,
+                   const Scalars* S) {
+  k_unsort<R><<<grid, 256, 0, st>>>(src, dst, S);
 }
 
 template <class R>
@@ -1831,9 +2038,11 @@ void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> s
                                 const int*, V2<R>*, double*, const Scn*, Scalars*,    \
                                 const int4*, const int*, const Scalars*);             \
   template int setup_b_p2g<R>();                                                      \
-  template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, const V2<R>*,       \
-                                const double*, const Scn*, Scalars*, const int2*,     \
-                                const Scalars*);                                      \
+  template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,      \
+                                const int*, const int*, const V2<R>*, const double*,  \
+                                const Scn*, Scalars*, const int2*, Scalars*, int*);   \
+  template void launch_unsort<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,     \
+                                 const Scalars*);                                     \
   template void launch_b_move<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,     \
                                  const int4*);
 DAMPM_INSTANTIATE(double)

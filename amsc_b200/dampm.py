@@ -48,7 +48,7 @@ class dampm_ms_params(C.Structure):
                 ("shear_split", C.c_double), ("hp_min", C.c_double), ("max_dv", C.c_double),
                 ("min_level", C.c_int), ("max_level", C.c_int),
                 ("min_particles_per_cell", C.c_int), ("call_interval", C.c_int),
-                ("max_ops", C.c_double)]
+                ("max_ops", C.c_double), ("pair_dist", C.c_double)]
 
 
 class DampmError(RuntimeError):
@@ -152,7 +152,7 @@ def make_structs(d: DATA):
                         float(s["ms_hp_min"]), float(s["ms_max_dv"]),
                         int(s["ms_min_level"]), int(s["ms_max_level"]),
                         int(s["ms_min_particles_per_cell"]), int(s["ms_call_interval"]),
-                        float(s["ms_max_ops"]))
+                        float(s["ms_max_ops"]), float(s.get("ms_pair_dist", 0.0)))
     return g, p, m
 
 
@@ -231,18 +231,32 @@ class Solver:
     def sync(self):
         self._check(self.lib.dampm_sync(self.h))
 
-    def status(self) -> Dict[str, float]:
+    def _status(self):
         it = C.c_int()
         t = C.c_double()
         dt = C.c_double()
         n = C.c_longlong()
-        self._check(self.lib.dampm_status(self.h, C.byref(it), C.byref(t), C.byref(dt),
-                                          C.byref(n)))
-        return {"it": it.value, "t": t.value, "dt": dt.value, "np": int(n.value)}
+        rc = self.lib.dampm_status(self.h, C.byref(it), C.byref(t), C.byref(dt), C.byref(n))
+        return rc, {"it": it.value, "t": t.value, "dt": dt.value, "np": int(n.value)}
+
+    def status(self) -> Dict[str, float]:
+        """Loop state; raises when the device status word is set (the run
+        diverged or merge/split ran out of capacity)."""
+        rc, st = self._status()
+        self._check(rc)
+        return st
+
+    @property
+    def failed(self) -> bool:
+        """True once the device status word stopped the run."""
+        return self._status()[0] == -5
 
     @property
     def num_particles(self) -> int:
-        return self.status()["np"]
+        rc, st = self._status()
+        if rc not in (0, -5):  # a diverged run still has its particles
+            self._check(rc)
+        return st["np"]
 
     def merge_split(self, dt: float):
         counts = (C.c_longlong * 4)()

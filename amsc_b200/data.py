@@ -34,6 +34,9 @@ OPTIONAL_DEFAULTS = {
     "ms_shear_split": 1e30, "ms_hp_min": 0.05, "ms_max_dv": 0.01,
     "ms_min_level": -2, "ms_max_level": 2, "ms_min_particles_per_cell": 2,
     "ms_call_interval": 10, "ms_max_ops": 1e9,
+    # no counterpart in the reference (which ignores the key): merge only
+    # pairs closer than ms_pair_dist * min(hx, hy); 0 = no limit
+    "ms_pair_dist": 0.0,
 }
 _INT_KEYS = {"Nex", "Ney", "BC_FLAG", "MERGE_SPLIT_ON", "NSTEPS", "ms_min_level",
              "ms_max_level", "ms_min_particles_per_cell", "ms_call_interval"}

@@ -63,7 +63,7 @@ def _base_scalars(**kw) -> dict:
         "ms_alpha": 0.9, "ms_beta": 0.30, "ms_split_hp_min": 0.0,
         "ms_shear_split": 1e30, "ms_hp_min": 0.05, "ms_max_dv": 0.01,
         "ms_min_level": -2, "ms_max_level": 2, "ms_min_particles_per_cell": 2,
-        "ms_call_interval": 10, "ms_max_ops": 1e9,
+        "ms_call_interval": 10, "ms_max_ops": 1e9, "ms_pair_dist": 0.0,
     }
     s.update(kw)
     return s
@@ -290,7 +290,8 @@ def mudflow(N: int = 2048, h: float = 0.5, seed: int = DEFAULT_SEED,
                        BC_FLAG=1, MERGE_SPLIT_ON=1 if merge_split else 0, eq_level=0.0,
                        DT_FIXED=0.0, NSTEPS=nsteps,
                        ms_alpha=math.sqrt(2.0 * A0) / h, ms_beta=math.sqrt(0.5 * A0) / h,
-                       ms_min_level=-2, ms_max_level=2, ms_call_interval=10)
+                       ms_min_level=-2, ms_max_level=2, ms_call_interval=10,
+                       ms_pair_dist=0.25 if merge_split else 0.0)
     return DATA(arrays, sc)
 
 

@@ -172,6 +172,8 @@ def cpu_baseline_port(d, seconds: float = 15.0):
 
 
 REF_MAX_STEPS = 30
+LATE_IT = 1000  # the `late` window of the mudflow line starts here
+LATE_STEPS = 20
 
 
 def run_reference(args, world, rank):
@@ -233,14 +235,59 @@ def run_reference(args, world, rank):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": np_, "grid": "2048x2048",
-                       "precision": "fp64"},
+            "config": mudflow_config(np_, None, 1, args.merge_split,
+                                     dt_mode=("fixed dt 0.0145 s, the workload's first CFL "
+                                              "step: the reference's adaptive first step "
+                                              "reads an uninitialised dt "
+                                              "(main/optim_par.cpp:284,303)")
+                                     if kind == "reference" else "adaptive CFL 0.4",
+                                     launch="host program, one core" if kind == "reference"
+                                     else "host program, OpenMP"),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def mudflow_config(np_, np_end, world, merge_split, dt_mode="adaptive CFL 0.4",
+                   launch="CUDA graphs of 16 passes"):
+    """The config object of the mudflow lines (this library's and the
+    reference arm's carry the same keys)."""
+    return {"workload": WORKLOAD + (", merge/split every 10 steps" if merge_split else ""),
+            "particles": np_, "particles_end": np_end, "grid": "2048x2048",
+            "precision": "fp64", "parallelism": f"replicas{world}",
+            "l2": "state 354 MB > 126 MB L2, no flush", "launch": launch,
+            "dt": dt_mode, "seed": 12345}
+
+
+def cpu_baseline_scenarios(ds, passes, seconds: float = 15.0):
+    """The CPU restatement (OpenMP, all host cores) on a bounded sample of the
+    same scenarios, one at a time: each sampled scenario runs some of its
+    passes and its time is scaled to `passes` (passes per scenario, a list
+    or one count).  Returns scenarios/s."""
+    from oracle.oracle import Oracle
+    threads = os.cpu_count() or 1
+    per = passes if isinstance(passes, (list, tuple)) else [passes] * len(ds)
+    t_used, t_est, m = 0.0, 0.0, 0
+    for d, n in zip(ds, per):
+        if m and t_used > seconds:
+            break
+        o = Oracle(d, threads=threads)
+        k = 0
+        t0 = time.perf_counter()
+        while k < n and (k < 2 or time.perf_counter() - t0 < seconds / 4):
+            o.run(1)
+            k += 1
+        el = time.perf_counter() - t0
+        o.close()
+        t_used += el
+        t_est += el / k * n
+        m += 1
+    return {"value": m / t_est, "unit": "scenarios/s", "cores": threads, "kind": "port",
+            "sample": f"{m} scenarios one at a time, each timed over up to its first passes "
+                      f"and scaled to its full run; {t_used:.1f} s of CPU time"}
 
 
 def run_ensemble(args, world, rank, local):
@@ -343,7 +390,8 @@ def run_ensemble(args, world, rank, local):
                     "note": "per ensemble: upload of every scenario, all passes, final hp back"},
             "gpu_launches": int(launches),
             "clocks": clocks,
-            "cpu_baseline": None,
+            "cpu_baseline": (cpu_baseline_scenarios(ds, K) if world == 1 and
+                             not args.no_cpu_baseline else None),
             "checksum_hp": float(sum(float(o.sum()) for o in outs)),
         }
         print(json.dumps(line), flush=True)
@@ -386,6 +434,10 @@ def run_mudflow_fp32(args, world, rank, local):
     per_pass = 180.0 * d.np
     achieved = per_pass / (el_ms / args.steps * 1e-3) / 1e9
     b.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(d)
+        cpu["sample"] += " (the FP64 restatement: the reference has no FP32 form)"
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -401,7 +453,7 @@ def run_mudflow_fp32(args, world, rank, local):
                          "frac": achieved / peak, "traffic": None,
                          "algorithmic_bytes_per_launch": per_pass},
             "e2e": None, "gpu_launches": int(launches), "clocks": clocks,
-            "cpu_baseline": None, "state": {"it": q["it"], "t": q["t"], "dt": q["dt"]},
+            "cpu_baseline": cpu, "state": {"it": q["it"], "t": q["t"], "dt": q["dt"]},
         }), flush=True)
     _barrier(world)
     return 0
@@ -459,6 +511,21 @@ def run_serving(args, world, rank, local):
     plain = m / (time.perf_counter() - tp) if m else None
     h2d = sum(8 * (10 * r.data.np + r.data.nnodes) for r in reqs)
     d2h = sum(8 * 3 * r.data.np for r in reqs)
+    # time-to-result below and above capacity: the same requests at other
+    # arrival rates, through a fresh server each
+    sweep = []
+    for rate in ([float(x) for x in args.rates.split(",")] if args.rates else []):
+        arr_r = poisson_arrivals(n, rate, seed=777 + rank)
+        rr = [Request(k, reqs[k].data, float(arr_r[k])) for k in range(n)]
+        sv = Server(budget, max_scenarios=args.max_scenarios, tick=args.tick,
+                    stream=stream.cuda_stream, precision=args.precision,
+                    graphs=not args.no_graphs)
+        sv.run([Request(-1, warm, 0.0)])
+        sv.run(rr)
+        sv.close()
+        mk = max(r.finished for r in rr)
+        sweep.append({"rate_per_s": rate, "scenarios_per_s": n / mk,
+                      "latency": latency_summary(rr)})
     if rank == 0:
         line = {
             "metric": "serving scenarios/s", "value": value, "unit": "scenarios/s",
@@ -488,7 +555,10 @@ def run_serving(args, world, rank, local):
                     "note": "time-to-result runs from arrival to results on the host"},
             "gpu_launches": int(launches),
             "clocks": clocks,
-            "cpu_baseline": None,
+            "cpu_baseline": (cpu_baseline_scenarios([r.data for r in reqs[:m]],
+                                                    [r.passes for r in reqs[:m]])
+                             if world == 1 and not args.no_cpu_baseline and m else None),
+            "rate_sweep": sweep,
         }
         print(json.dumps(line), flush=True)
     _barrier(world)
@@ -505,6 +575,8 @@ def main():
                     choices=["mudflow", "ensemble", "serving"])
     ap.add_argument("--requests", type=int, default=300)
     ap.add_argument("--rate", type=float, default=100.0)
+    ap.add_argument("--rates", default="",
+                    help="serving workload: also run these arrival rates (comma list)")
     ap.add_argument("--t-end", type=float, default=60.0)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--max-scenarios", type=int, default=1024)
@@ -521,6 +593,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-late", dest="late", action="store_false",
+                    help="mudflow workload: skip the window at step 1000")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.steps is None:
@@ -584,16 +658,37 @@ def main():
     ms_per_step = el_ms / args.steps
     st = s.status()
 
-    # roofline of the dominant kernel, algorithmic bytes per launch:
-    # P2G reads each particle's 13-value f64 record (written by the previous
-    # G2P) and its sorted index: 108 B per particle, and writes vvxL, vvyL:
-    # 16 B per node touched.  G2P reads key, x, y, hp, H, Mp, Vp (52 B) and
-    # writes x, y, vpx, vpy, hp, F11, F12, F22, key and the 8-value next
-    # record (132 B): 184 B per particle, and gathers vvxL, vvyL, Z: 24 B per
-    # node touched.
-    # the per-kernel times: the same warm-up and K steps once more, from the
+    # the same rate later in the run: advance to step LATE_IT (the flow has
+    # spread and piled up), then time LATE_STEPS more
+    late = None
+    if not args.merge_split and args.late:
+        s.step(max(0, LATE_IT - st["it"]))
+        s.sync()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(ts)
+        s.step(LATE_STEPS)
+        l1.record(ts)
+        ts.synchronize()
+        lms = _allreduce(l0.elapsed_time(l1), world)
+        sl = s.status()
+        late = {"from_it": sl["it"] - LATE_STEPS, "steps": LATE_STEPS,
+                "ms_per_step": lms / LATE_STEPS,
+                "value": total_particles * LATE_STEPS / (lms * 1e-3), "unit": METRIC,
+                "t": sl["t"]}
+
+    # roofline of the dominant kernel.  `achieved` uses the algorithmic bytes
+    # of the scope table: P2G reads 11 f64 fields of each particle and its
+    # sorted index (92 B) and writes 5 f64 sums and reads Z per touched node
+    # (48 B); G2P reads x, y, hp, Mp, Vp, H and the index (52 B) and writes
+    # x, y, vpx, vpy, hp, F11, F12, F22 (64 B) per particle and reads vvxL,
+    # vvyL, Z per touched node (24 B).  `design_bytes_per_launch` is what
+    # this implementation moves: P2G gathers the 13-value f64 record and the
+    # slot (108 B) and writes vvxL, vvyL (16 B per node); G2P reads the slot,
+    # key, index and x, y, hp, H, Mp, Vp (60 B) and writes the 11 state
+    # fields, key, index, sort slot and the 8-value record (164 B).
+    # The per-kernel times: the same warm-up and K steps once more, from the
     # same initial state, with CUDA events between the kernel classes (those
-    # passes are launched one by one)
+    # passes are launched one by one).
     with Solver(d, merge_split=args.merge_split, stream=ts.cuda_stream) as sk:
         sk.step(args.warmup)
         sk.sync()
@@ -601,23 +696,26 @@ def main():
         sk.step(args.steps)
         sk.sync()
         tm = sk.timings(False)
-    x = s.download("x")
-    y = s.download("y")
+        x = sk.download("x")
+        y = sk.download("y")
+        np_now = sk.status()["np"]
     h = float(d.scalars["hx"])
     nrows = int(d.scalars["Ney"])
     kc = (np.clip(np.floor(y / h), 0, nrows - 1).astype(np.int64) +
           np.clip(np.floor(x / h), 0, int(d.scalars["Nex"]) - 1).astype(np.int64) * nrows)
     n_nodes = _touched_nodes(d, kc)
-    np_now = st["np"]
-    p2g_bytes = 108 * np_now + 16 * n_nodes
-    g2p_bytes = 184 * np_now + 24 * n_nodes
-    p2g_ms = tm[1] / args.steps
-    g2p_ms = tm[2] / args.steps
+    alg = {"p2g": 92 * np_now + 48 * n_nodes, "g2p": 116 * np_now + 24 * n_nodes}
+    design = {"p2g": 108 * np_now + 16 * n_nodes, "g2p": 224 * np_now + 24 * n_nodes}
+    kms = {"p2g": tm[1] / args.steps, "g2p": tm[2] / args.steps}
     peak, peak_kind = _peaks()
-    dom = "p2g" if p2g_ms >= g2p_ms else "g2p"
-    dom_bytes, dom_ms = (p2g_bytes, p2g_ms) if dom == "p2g" else (g2p_bytes, g2p_ms)
-    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    dom = "p2g" if kms["p2g"] >= kms["g2p"] else "g2p"
+    achieved = alg[dom] / (kms[dom] * 1e-3) / 1e9
     traffic = _traffic_profile().get(dom)
+    per_kernel = {k: {"algorithmic_bytes": alg[k], "design_bytes": design[k],
+                      "ms": kms[k], "achieved_gbs": alg[k] / (kms[k] * 1e-3) / 1e9,
+                      "frac": alg[k] / (kms[k] * 1e-3) / 1e9 / peak,
+                      "design_gbs": design[k] / (kms[k] * 1e-3) / 1e9}
+                  for k in ("p2g", "g2p")}
 
     # end to end through the C ABI with host buffers: per step the persistent
     # state goes host->device from pinned memory (dampm_set_state), the step
@@ -650,24 +748,23 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD + (", merge/split every 10 steps"
-                                               if args.merge_split else ""),
-                       "particles": np_, "particles_end": st["np"], "grid": "2048x2048",
-                       "precision": "fp64", "parallelism": f"replicas{world}",
-                       "l2": "state 354 MB > 126 MB L2, no flush",
-                       "launch": ("one by one (merge/split passes differ)" if args.merge_split
-                                  else "CUDA graphs of 16 passes"),
-                       "seed": 12345},
+            "config": mudflow_config(np_, st["np"], world, args.merge_split,
+                                     launch=("one pass at a time outside the merge/split "
+                                             "cycle graphs" if args.merge_split
+                                             else "CUDA graphs of 16 passes")),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic,
-                         "algorithmic_bytes_per_launch": dom_bytes,
-                         "kernel_ms": dom_ms,
+                         "algorithmic_bytes_per_launch": alg[dom],
+                         "design_bytes_per_launch": design[dom],
+                         "kernel_ms": kms[dom],
                          "kernel_ms_from": "the same warm-up and steps run again from the "
                                            "same state with CUDA events between kernel "
                                            "classes"},
-            "kernels_ms_per_step": {"sort": tm[0] / args.steps, "p2g": p2g_ms,
-                                    "g2p": g2p_ms, "other": tm[3] / args.steps},
+            "kernels": per_kernel,
+            "kernels_ms_per_step": {"sort": tm[0] / args.steps, "p2g": kms["p2g"],
+                                    "g2p": kms["g2p"], "other": tm[3] / args.steps},
+            "late": late,
             "e2e": {"value": e2e_value, "unit": METRIC,
                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
             "gpu_launches": int(launches),

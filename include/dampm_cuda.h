@@ -17,10 +17,13 @@
  * Conventions
  *   - Plain C types only; host pointers are host memory, never retained.
  *   - Every function returns 0 (DAMPM_OK) or a negative dampm_status code;
- *     dampm_last_error() gives a one-line message.  Device-side problems
- *     (non-finite depth, particle capacity exceeded) are reported through a
- *     device status word read by dampm_sync()/dampm_status(); kernels never
- *     trap.
+ *     dampm_last_error() gives a one-line message.  Device-side problems are
+ *     reported through a device status word, never by a trap: G2P sets it
+ *     when any particle's x, y, vpx, vpy or hp is NaN or infinite, or hp is
+ *     negative (DAMPM_ERR_DEVICE); merge/split sets it when the particle
+ *     capacity would be exceeded (DAMPM_ERR_CAPACITY).  A flagged run does
+ *     no further passes.  dampm_sync(), dampm_run() and dampm_status()
+ *     return the code; the data-out calls still copy the (diverged) state.
  *   - A context owns all of its device memory and is used from one host
  *     thread at a time.  Work is enqueued on the stream given at creation
  *     (NULL = a stream the context creates).
@@ -74,6 +77,12 @@ typedef struct {
   double alpha, beta, split_hp_min, shear_split, hp_min, max_dv;
   int min_level, max_level, min_particles_per_cell, call_interval;
   double max_ops;
+  /* Merge only pairs closer than pair_dist * min(hx, hy); 0 (what a
+   * positional initialiser of the fields above leaves) = no distance limit,
+   * the reference's pairing of the nearest co-moving candidate in the cell
+   * (main/merge_split_ops_cmes.h:192-210).  No counterpart in the reference:
+   * the benchmark's merge/split configuration asks for 0.25. */
+  double pair_dist;
 } dampm_ms_params;
 
 typedef struct dampm_ctx dampm_ctx;
@@ -133,7 +142,9 @@ int dampm_run(dampm_ctx* ctx, long long max_steps, int chunk,
 /* Waits for the stream and checks the device status word. */
 int dampm_sync(dampm_ctx* ctx);
 
-/* Loop state: iteration, time, last dt, particle count (synchronises). */
+/* Loop state: iteration, time, last dt, particle count (synchronises).  The
+ * outputs are filled in even when the status word is set, which is then
+ * returned as the error code. */
 int dampm_status(dampm_ctx* ctx, int* it, double* t, double* dt_last,
                  long long* np);
 
@@ -306,8 +317,10 @@ int dampm_batch_query(dampm_batch* b, int handle, int* it, double* t,
                       double* dt_last, int* running, long long* np);
 
 /* The loop state of every live scenario in one synchronising call: handle,
- * whether its loop condition still holds, iteration, time.  cap is the
- * length of the arrays; *count receives the live count. */
+ * running (1: its loop condition still holds; 0: finished; -1: stopped by
+ * its status word -- its state diverged, see the conventions above; the
+ * other scenarios are unaffected), iteration, time.  cap is the length of
+ * the arrays; *count receives the live count. */
 int dampm_batch_states(dampm_batch* b, int cap, int* handles, int* running,
                        int* its, double* ts, int* count);
 

@@ -61,6 +61,7 @@ typedef struct {
       ms_max_dv;
   int ms_min_level, ms_max_level, ms_min_particles_per_cell, ms_call_interval;
   double ms_max_ops;
+  double ms_pair_dist;  // pair-distance gate (0: none, the reference's pairing)
 } oracle_data;
 
 }  // extern "C"
@@ -478,6 +479,10 @@ void decide_actions(Oracle& o, double dt, std::vector<int>& act,
   const double* vpx = o.dprops.at("vpx").data();
   const double* vpy = o.dprops.at("vpy").data();
   const double max_dv2 = o.d.ms_max_dv * o.d.ms_max_dv;
+  // the optional pair-distance gate (no counterpart in the reference)
+  const double gmin_h = (o.d.hy < o.d.hx) ? o.d.hy : o.d.hx;
+  const double gr = o.d.ms_pair_dist * gmin_h;
+  const double gate2 = o.d.ms_pair_dist > 0.0 ? gr * gr : 0.0;
   long long n_split = 0, n_merge = 0;
   for (idx_t cell = 0; cell < o.ncells(); ++cell) {
     const idx_t b = o.cell_start[cell], e = o.cell_start[cell + 1];
@@ -506,7 +511,7 @@ void decide_actions(Oracle& o, double dt, std::vector<int>& act,
         const double d2 = dx * dx + dy * dy;
         const double dvx = vpx[i1] - vpx[i2];
         const double dvy = vpy[i1] - vpy[i2];
-        if (d2 < best && (dvx * dvx + dvy * dvy) < max_dv2) {
+        if (d2 < best && (dvx * dvx + dvy * dvy) < max_dv2 && (gate2 == 0.0 || d2 < gate2)) {
           best = d2;
           bj = j;
         }

@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 OPTIM_PAR = os.path.join(REF_DIR, "optim_par")
 MS_HARNESS = os.path.join(REF_DIR, "ms_harness")
+BINDING = os.path.join(REF_DIR, "b200_offload")
 
 
 def available() -> bool:
@@ -46,6 +47,9 @@ def build(ref_root: Optional[str] = None) -> bool:
     if ref_root is None:
         return available()
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
+    lib = os.path.join(os.path.dirname(HERE), "amsc_b200", "libdampm_cuda.so")
+    if os.path.exists(lib):  # the reference-side driver of the C ABI
+        subprocess.run(["make", "-s", "-C", HERE, "binding", f"REF={ref_root}"], check=True)
     return available()
 
 

@@ -48,3 +48,23 @@ def test_momentum_conserved_without_forcing():
     mx = (o.get("vpx") * o.get("Mp")).sum()
     mass = o.get("Mp").sum()
     assert abs(mx) / mass < 1e-12
+
+
+def test_pair_distance_gate():
+    """The optional merge gate (ms_pair_dist, no counterpart in the reference):
+    0 keeps the reference's pairing; a limit below every pair's distance
+    stops all merges; a wide limit merges as without one; merges never pair
+    particles farther apart than the limit."""
+    d = scenarios.bench_slab(1000, nsteps=20)
+    d.scalars.update({"ms_alpha": 0.5, "ms_beta": 0.5, "ms_max_dv": 1.0, "MERGE_SPLIT_ON": 1})
+    counts = {}
+    for gate in (0.0, 1e-9, 100.0, 0.2):
+        dd = d.copy()
+        dd.scalars["ms_pair_dist"] = gate
+        o = Oracle(dd, threads=2)
+        o.run(12)
+        counts[gate] = o.merge_split(1e-3)
+    assert counts[0.0][1] > 0
+    assert counts[1e-9][1] == 0
+    assert counts[100.0] == counts[0.0]
+    assert 0 <= counts[0.2][1] <= counts[0.0][1]
