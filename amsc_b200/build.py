@@ -15,8 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdampm_cuda.so")
-SOURCES = ["step_kernels.cu", "ms_kernels.cu", "dampm_api.cu", "cfl_noalloc.cu",
-           "batch_api.cu", "data_json.cpp"]
+SOURCES = ["step_kernels.cu", "ms_kernels.cu", "slab_kernels.cu", "dampm_api.cu",
+           "cfl_noalloc.cu", "batch_api.cu", "data_json.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

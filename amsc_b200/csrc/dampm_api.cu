@@ -3,6 +3,7 @@
 // Host orchestration of the sm_100a step: device buffers owned by the
 // context, all kernels enqueued on one stream, loop state kept on the device
 // (Scalars) so that dampm_step() never synchronises.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -77,6 +78,13 @@ struct dampm_ctx {
     unsigned char key[kKeyBytes] = {};
   } graphs[2];
   long long graph_clock = 0;
+  // slab mode (one scenario split over contexts by cell columns): the
+  // leaver list G2P fills, scratch for the route, the particle count
+  bool slab = false;
+  int* leave = nullptr;
+  int* sel = nullptr;        // slot lists (capacity)
+  int* selcount = nullptr;   // one counter
+  int2* moves = nullptr;     // hole fills (capacity)
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -263,15 +271,13 @@ void enqueue_unsort(dampm_ctx* ctx) {
   ctx->launches += 1;
 }
 
-int enqueue_pass(dampm_ctx* ctx) {
+// One pass of the loop body in two halves: step start, sort and P2G; then
+// G2P and step end (slab mode exchanges node columns between them).
+int enqueue_front(dampm_ctx* ctx) {
   const long long it_next = ctx->it_host + 1;
   const bool ms_due = ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 &&
                       ctx->ms.call_interval > 0 &&
                       (it_next % ctx->ms.call_interval) == 0;
-  // the pass after the merge/split call needs the gradients of this one
-  const bool grad_next = ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 &&
-                         ctx->ms.call_interval > 0 &&
-                         ((it_next + 1) % ctx->ms.call_interval) == 0;
   ev_mark(ctx, 3);
   k_step_begin<<<1, 1, 0, ctx->stream>>>(ctx->S, ctx->G, ctx->P);
   ctx->launches += 1;
@@ -309,9 +315,21 @@ int enqueue_pass(dampm_ctx* ctx) {
   ev_mark(ctx, 3);
   k_ledger_final<<<1, 1024, 0, ctx->stream>>>(ctx->led_part, ctx->ucount, ctx->S,
                                                ctx->ledger_log);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  return DAMPM_OK;
+}
+
+int enqueue_back(dampm_ctx* ctx) {
+  const long long it_next = ctx->it_host + 1;
+  // the pass after the merge/split call needs the gradients of this one
+  const bool grad_next = ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON != 0 &&
+                         ctx->ms.call_interval > 0 &&
+                         ((it_next + 1) % ctx->ms.call_interval) == 0;
   ev_mark(ctx, 2);
   launch_g2p(grid_for(ctx->cap, kG2PThreads), ctx->stream, ctx->p, ctx->q, ctx->perm,
-             ctx->skey, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->count, ctx->record ? 1 : 0,
+             ctx->skey, ctx->nodes, ctx->Z, ctx->G, ctx->P, ctx->S, ctx->count, ctx->leave,
+             ctx->record ? 1 : 0,
              (grad_next || ctx->record) ? 1 : 0);
   if (ctx->record) {
     k_hv<<<grid_for(ctx->nn, 256), 256, 0, ctx->stream>>>(ctx->q, ctx->start,
@@ -326,6 +344,11 @@ int enqueue_pass(dampm_ctx* ctx) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ctx, DAMPM_ERR_CUDA, cudaGetErrorString(e));
   return DAMPM_OK;
+}
+
+int enqueue_pass(dampm_ctx* ctx) {
+  int rc = enqueue_front(ctx);
+  return rc ? rc : enqueue_back(ctx);
 }
 
 // Passes can be replayed from a graph when they repeat: kGraphPasses alike
@@ -712,6 +735,7 @@ int dampm_enable_merge_split(dampm_ctx* ctx, int enable) {
 
 int dampm_record_outputs(dampm_ctx* ctx, int enable) {
   if (!ctx) return DAMPM_ERR_ARG;
+  if (ctx->slab && enable) return fail(ctx, DAMPM_ERR_STATE, "slab mode records no outputs");
   ctx->record = enable != 0;
   if (ctx->record && ctx->p.x) return alloc_record(ctx);
   return DAMPM_OK;
@@ -719,6 +743,7 @@ int dampm_record_outputs(dampm_ctx* ctx, int enable) {
 
 int dampm_step(dampm_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return DAMPM_ERR_ARG;
+  if (ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "slab mode: use the dampm_slab_* calls");
   if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
   ctx->launches = 0;
   ctx->evused = 0;
@@ -810,6 +835,7 @@ int dampm_status(dampm_ctx* ctx, int* it, double* t, double* dt_last,
 
 int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
   if (!ctx) return DAMPM_ERR_ARG;
+  if (ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "slab mode: use the dampm_slab_* calls");
   if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
   // bin with the current positions, then decide + emit (an always-active
   // pass: the loop condition does not apply to a standalone call)
@@ -842,6 +868,7 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
 
 int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
   if (!ctx || !field || !out) return DAMPM_ERR_ARG;
+  if (ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "slab mode: use the dampm_slab_* calls");
   if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "no particles");
   int rc = sync_status(ctx, false);
   if (rc) return rc;
@@ -982,6 +1009,7 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
                     const double* Ap, const double* mom_px,
                     const double* mom_py, const double* Fb_x,
                     const double* Fb_y) {
+  if (ctx && ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "slab mode: use the dampm_slab_* calls");
   if (!ctx || !fields || np < 0 || np > ctx->cap) return DAMPM_ERR_ARG;
   if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
   Particles& p = ctx->p;
@@ -1021,6 +1049,7 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
 
 int dampm_get_state(dampm_ctx* ctx, double* const* fields) {
   if (!ctx || !fields) return DAMPM_ERR_ARG;
+  if (ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "slab mode: use the dampm_slab_* calls");
   int rc = sync_status(ctx, false);
   if (rc) return rc;
   Particles& p = ctx->p;
@@ -1061,6 +1090,252 @@ int dampm_last_timings(dampm_ctx* ctx, int enable_events, double out[5]) {
     }
   }
   ctx->timing = enable_events != 0;
+  return DAMPM_OK;
+}
+
+// ---- one scenario over slabs of cell columns ------------------------------
+namespace {
+
+unsigned long long host_ordered_key(double v) {
+  unsigned long long b;
+  std::memcpy(&b, &v, sizeof b);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+double host_ordered_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  double v;
+  std::memcpy(&v, &b, sizeof v);
+  return v;
+}
+
+int slab_alloc(dampm_ctx* ctx) {
+  if (ctx->leave || !ctx->p.x) return DAMPM_OK;
+  int rc = dalloc(ctx, &ctx->leave, size_t(ctx->cap));
+  rc = rc ? rc : dalloc(ctx, &ctx->sel, size_t(ctx->cap));
+  rc = rc ? rc : dalloc(ctx, &ctx->selcount, 1);
+  rc = rc ? rc : dalloc(ctx, &ctx->moves, size_t(ctx->cap));
+  return rc;
+}
+
+int slab_ready(dampm_ctx* ctx) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (!ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "not in slab mode (dampm_slab_set)");
+  if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "upload particles first");
+  return slab_alloc(ctx);
+}
+
+}  // namespace
+
+int dampm_slab_record_doubles(void) { return kSlabRecord; }
+
+int dampm_slab_set(dampm_ctx* ctx, int col_lo, int col_hi) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (!(0 <= col_lo && col_lo < col_hi && col_hi <= ctx->grid.Nex))
+    return fail(ctx, DAMPM_ERR_ARG, "slab columns outside the grid");
+  if (ctx->record || (ctx->ms_enabled && ctx->params.MERGE_SPLIT_ON))
+    return fail(ctx, DAMPM_ERR_STATE, "slab mode runs without recorded outputs or merge/split");
+  ctx->slab = true;
+  ctx->use_graphs = false;
+  ctx->G.pc_lo = col_lo;
+  ctx->G.pc_hi = col_hi;
+  ctx->G.nc_lo = col_lo;
+  ctx->G.nc_hi = col_hi == ctx->grid.Nex ? col_hi : col_hi - 1;
+  return slab_alloc(ctx);
+}
+
+int dampm_slab_set_index(dampm_ctx* ctx, const int* idx) {
+  int rc = slab_ready(ctx);
+  if (rc) return rc;
+  if (!idx) return DAMPM_ERR_ARG;
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  const int np = ctx->Sh->np - ctx->Sh->nghost;
+  CK(cudaMemcpyAsync(ctx->p.idx, idx, sizeof(int) * np, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+int dampm_slab_pass(dampm_ctx* ctx, int phase) {
+  int rc = slab_ready(ctx);
+  if (rc) return rc;
+  ctx->launches = 0;
+  if (phase == 0) return enqueue_front(ctx);
+  if (phase == 1) return enqueue_back(ctx);
+  return DAMPM_ERR_ARG;
+}
+
+int dampm_slab_node_column(dampm_ctx* ctx, int col, double* buf, int set) {
+  if (!ctx || !buf || col < 0 || col > ctx->grid.Nex) return DAMPM_ERR_ARG;
+  const size_t n = size_t(ctx->grid.Ney + 1);
+  double2* c = ctx->nodes.vvL + (size_t)col * n;
+  if (set)
+    CK(cudaMemcpyAsync(c, buf, n * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
+  else
+    CK(cudaMemcpyAsync(buf, c, n * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+int dampm_slab_cfl(dampm_ctx* ctx, double maxima[3], int set) {
+  if (!ctx || !maxima) return DAMPM_ERR_ARG;
+  if (set) {
+    k_slab_set_red<<<1, 1, 0, ctx->stream>>>(ctx->S, host_ordered_key(maxima[0]),
+                                             host_ordered_key(maxima[1]),
+                                             host_ordered_key(maxima[2]));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DAMPM_OK;
+  }
+  int rc = sync_status(ctx, false);
+  if (rc) return rc;
+  for (int k = 0; k < 3; ++k) maxima[k] = host_ordered_value(ctx->Sh->red_cur[k]);
+  return DAMPM_OK;
+}
+
+int dampm_slab_route(dampm_ctx* ctx, double* left, double* right, long long cap,
+                     long long* n_left, long long* n_right) {
+  int rc = slab_ready(ctx);
+  if (rc) return rc;
+  if (!n_left || !n_right || cap < 0) return DAMPM_ERR_ARG;
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  const int np = ctx->Sh->np, L = ctx->Sh->nleave;
+  *n_left = *n_right = 0;
+  if (L == 0) return DAMPM_OK;
+  std::vector<int> slots(L), keys(L);
+  CK(cudaMemcpyAsync(slots.data(), ctx->leave, sizeof(int) * L, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  k_slab_keys<<<grid_for(L, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->leave, L, ctx->sel);
+  CK(cudaMemcpyAsync(keys.data(), ctx->sel, sizeof(int) * L, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // leavers by side, in slot order
+  std::vector<int> order(L);
+  for (int k = 0; k < L; ++k) order[k] = k;
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return slots[a] < slots[b]; });
+  std::vector<int> lefts, rights, sorted_slots;
+  for (int k : order) {
+    sorted_slots.push_back(slots[k]);
+    (keys[k] / ctx->grid.Ney < ctx->G.pc_lo ? lefts : rights).push_back(slots[k]);
+  }
+  if ((long long)lefts.size() > cap || (long long)rights.size() > cap)
+    return fail(ctx, DAMPM_ERR_CAPACITY, "route buffers smaller than the migrants");
+  if ((!left && !lefts.empty()) || (!right && !rights.empty()))
+    return fail(ctx, DAMPM_ERR_STATE, "particles left the slab on a side without a neighbour");
+  // pack the migrants, then fill the holes below the new count with the
+  // particles that stay above it
+  const int keep = np - L;
+  std::vector<int2> mv;
+  {
+    size_t h = 0;  // leavers below `keep`, in slot order, are the holes
+    size_t li = 0;
+    for (int src = keep; src < np; ++src) {
+      while (li < sorted_slots.size() && sorted_slots[li] < src) ++li;
+      if (li < sorted_slots.size() && sorted_slots[li] == src) continue;  // a leaver
+      while (h < sorted_slots.size() && sorted_slots[h] >= keep) ++h;
+      mv.push_back(make_int2(src, sorted_slots[h++]));
+    }
+  }
+  for (int side = 0; side < 2; ++side) {
+    const std::vector<int>& v = side ? rights : lefts;
+    if (v.empty()) continue;
+    CK(cudaMemcpyAsync(ctx->sel, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    k_slab_pack<<<grid_for(long(v.size()), 256), 256, 0, ctx->stream>>>(
+        ctx->p, ctx->sel, int(v.size()), side ? right : left);
+    CK(cudaStreamSynchronize(ctx->stream));  // sel is reused
+  }
+  if (!mv.empty()) {
+    CK(cudaMemcpyAsync(ctx->moves, mv.data(), sizeof(int2) * mv.size(),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    k_slab_move<<<grid_for(long(mv.size()), 256), 256, 0, ctx->stream>>>(ctx->p, ctx->moves,
+                                                                         int(mv.size()));
+  }
+  k_slab_scalars<<<1, 1, 0, ctx->stream>>>(ctx->S, keep, 0, ctx->nc);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n_left = (long long)lefts.size();
+  *n_right = (long long)rights.size();
+  return DAMPM_OK;
+}
+
+int dampm_slab_ghosts(dampm_ctx* ctx, double* buf, long long cap, long long* n) {
+  int rc = slab_ready(ctx);
+  if (rc) return rc;
+  if (!buf || !n) return DAMPM_ERR_ARG;
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  const int np = ctx->Sh->np - ctx->Sh->nghost;
+  CK(cudaMemsetAsync(ctx->selcount, 0, sizeof(int), ctx->stream));
+  k_slab_select<<<grid_for(np, 256), 256, 0, ctx->stream>>>(
+      ctx->p.key, np, ctx->G.pc_hi - 1, ctx->grid.Ney, ctx->sel, ctx->selcount);
+  int cnt = 0;
+  CK(cudaMemcpyAsync(&ctx->Sh->np_next, ctx->selcount, sizeof(int), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  cnt = ctx->Sh->np_next;
+  if (cnt > cap) return fail(ctx, DAMPM_ERR_CAPACITY, "ghost buffer smaller than the column");
+  if (cnt > 0)
+    k_slab_pack<<<grid_for(cnt, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->sel, cnt, buf);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n = cnt;
+  return DAMPM_OK;
+}
+
+int dampm_slab_import(dampm_ctx* ctx, const double* buf, long long n, int ghosts) {
+  int rc = slab_ready(ctx);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && !buf)) return DAMPM_ERR_ARG;
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  const long long base = ctx->Sh->np;
+  if (base + n > ctx->cap)
+    return fail(ctx, DAMPM_ERR_CAPACITY, "slab capacity below its particles and imports");
+  if (n > 0) {
+    k_slab_unpack<<<grid_for(n, 256), 256, 0, ctx->stream>>>(ctx->p, buf, int(n), int(base));
+    // ghosts: the left neighbour's last column; migrants: this slab's columns
+    const int lo = ghosts ? ctx->G.pc_lo - 1 : ctx->G.pc_lo;
+    const int hi = ghosts ? ctx->G.pc_lo : ctx->G.pc_hi;
+    k_slab_check<<<grid_for(n, 256), 256, 0, ctx->stream>>>(ctx->p.key + base, int(n), lo, hi,
+                                                            ctx->grid.Ney, ctx->S);
+    k_count_n<<<grid_for(n, 256), 256, 0, ctx->stream>>>(ctx->p.key + base, ctx->count,
+                                                         ctx->p.slot + base, int(n));
+  }
+  k_slab_scalars<<<1, 1, 0, ctx->stream>>>(ctx->S, int(base + n), ghosts ? int(n) : 0,
+                                           ctx->nc);
+  CK(cudaGetLastError());
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  if (ctx->Sh->status & kStatusSlab)
+    return fail(ctx, DAMPM_ERR_STATE, "a particle moved more than one slab in a step");
+  return DAMPM_OK;
+}
+
+int dampm_slab_download(dampm_ctx* ctx, const char* field, double* out, long long* idx) {
+  int rc = slab_ready(ctx);
+  if (rc) return rc;
+  if (!field || !out) return DAMPM_ERR_ARG;
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  const int np = ctx->Sh->np - ctx->Sh->nghost;
+  const std::string f(field);
+  Particles& p = ctx->p;
+  const double* src = f == "x" ? p.x : f == "y" ? p.y : f == "vpx" ? p.vpx
+                    : f == "vpy" ? p.vpy : f == "hp" ? p.hp : f == "F_11" ? p.F11
+                    : (f == "F_12" || f == "F_21") ? p.F12 : f == "F_22" ? p.F22
+                    : f == "Mp" ? p.Mp : f == "Vp" ? p.Vp : f == "H" ? p.H : nullptr;
+  if (!src) return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown slab field " + f);
+  if (np == 0) return DAMPM_OK;
+  CK(cudaMemcpyAsync(out, src, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
+  if (idx) {
+    std::vector<int> ix(np);
+    CK(cudaMemcpyAsync(ix.data(), p.idx, sizeof(int) * np, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < np; ++k) idx[k] = ix[k];
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
   return DAMPM_OK;
 }
 

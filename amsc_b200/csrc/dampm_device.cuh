@@ -18,6 +18,10 @@ struct Geom {
   double hx, hy;
   double Lx, Ly;  // Nex*hx, Ney*hy (main/optim_par.cpp:557-558)
   int hx_pow2, hy_pow2;  // h is a power of two: v/h == v*(1/h) exactly
+  // The part of the grid a slab owns (the whole grid outside slab mode):
+  // particles of cell columns [pc_lo, pc_hi), node columns [nc_lo, nc_hi]
+  // written by P2G.
+  int pc_lo, pc_hi, nc_lo, nc_hi;
 };
 
 // Scalars of struct DATA used inside the step (main/mpm_data.h:21-44).
@@ -38,6 +42,8 @@ struct Scalars {
   int status;   // error bits (kStatus*)
   int np;       // current particle count
   int np_next;  // particle count after a merge/split emit
+  int nghost;   // slab mode: copies of the neighbour's last column, sorted first
+  int nleave;   // slab mode: particles G2P moved out of the slab's columns
   unsigned long long red_cur[3];   // ordered keys of max|vpx|, max|vpy|, max hp
   unsigned long long red_next[3];  // ... produced by this step's G2P
   // cell-key ranges for the counting sort's scan: krange = the keys the cell
@@ -50,6 +56,7 @@ struct Scalars {
 
 constexpr int kStatusCapacity = 1;
 constexpr int kStatusNonFinite = 2;
+constexpr int kStatusSlab = 4;  // a particle arrived outside the slab's columns
 
 // --- order-preserving double <-> u64 map for atomicMax reductions --------
 __device__ __forceinline__ unsigned long long ordered_key(double v) {

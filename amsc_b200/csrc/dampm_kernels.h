@@ -180,7 +180,7 @@ __global__ void k_ledger_final(const double* led_part, const int* ucount,
 // counts the next binning's keys
 void launch_g2p(int grid, cudaStream_t st, Particles cur, Particles nxt, const int* perm,
                 const int* skey, Nodes nodes, const double* Z, Geom G, Phys P, Scalars* S,
-                int* count, int record, int want_grad);
+                int* count, int* leave, int record, int want_grad);
 // the particles of `src` into reference order in `dst` (slot idx[j])
 template <class R>
 void launch_unsort(int grid, cudaStream_t st, ParticlesT<R> src, ParticlesT<R> dst,
@@ -237,5 +237,19 @@ __global__ void k_hv(const Particles p, const int* cstart, double* HV, Geom G,
                      const Scalars* S);
 
 size_t p2g_smem_bytes();  // FP64 P2G staging (the single-scenario path)
+
+// ---- one scenario over slabs of cell columns (slab_kernels.cu) ---------------
+constexpr int kSlabRecord = 20;  // doubles per particle record that travels
+__global__ void k_slab_pack(Particles p, const int* slots, int n, double* buf);
+__global__ void k_slab_unpack(Particles p, const double* buf, int n, int base);
+__global__ void k_slab_select(const int* key, int n, int col, int nrows, int* slots,
+                              int* count);
+__global__ void k_slab_keys(const int* key, const int* slots, int n, int* out);
+__global__ void k_slab_check(const int* key, int n, int col_lo, int col_hi, int nrows,
+                             Scalars* S);
+__global__ void k_slab_move(Particles p, const int2* moves, int n);
+__global__ void k_slab_scalars(Scalars* S, int np, int ghosts_added, int ncells);
+__global__ void k_slab_set_red(Scalars* S, unsigned long long a, unsigned long long b,
+                               unsigned long long c);
 
 }  // namespace dampm

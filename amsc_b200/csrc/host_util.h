@@ -20,6 +20,10 @@ inline Geom make_geom(const dampm_grid& g) {
   int e;
   G.hx_pow2 = std::frexp(g.hx, &e) == 0.5 ? 1 : 0;
   G.hy_pow2 = std::frexp(g.hy, &e) == 0.5 ? 1 : 0;
+  G.pc_lo = 0;
+  G.pc_hi = g.Nex;
+  G.nc_lo = 0;
+  G.nc_hi = g.Nex;
   return G;
 }
 

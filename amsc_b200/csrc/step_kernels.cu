@@ -52,6 +52,10 @@ __device__ __forceinline__ void step_begin_one(Scalars* S, const Geom& G,
 }
 
 __device__ __forceinline__ void step_end_one(Scalars* S) {
+  // slab mode: the neighbour's column copies were read by P2G only; G2P
+  // wrote the slab's own particles
+  S->np -= S->nghost;
+  S->nghost = 0;
   if (!S->active) return;
   S->t += S->dt;
   S->fresh = 0;
@@ -784,6 +788,7 @@ __device__ __forceinline__ void nodal_update(
     R Mv, R momx, R momy, R FPx, R FPy, R Frx, R Fry, R Fix, R Fiy, int r, int nc,
     const Geom& G, const Phys& P, double dtd, const NodesT<R>& nodes, int record,
     double& ln0, double& ln1, double& ln2) {
+  if (nc < G.nc_lo || nc > G.nc_hi) return;  // a slab's neighbour writes this column
   const int nrows = G.nrows, ncols = G.ncols;
   const int n = r + nc * (nrows + 1);
   const R dt = R(dtd);
@@ -1207,7 +1212,8 @@ __device__ __forceinline__ void p2g_unit(
     load_perm(pf, perm, nxt);
     cp_async_wait_all();
     __syncthreads();  // batch `cur` is in shared memory
-    const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA;
+    const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA && cur.cc >= G.pc_lo &&
+                     cur.cc < G.pc_hi;
     const bool lead = cur.cc < cA;  // started chains only
     switch (grp) {
       case 0: chain_group<R, 0>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
@@ -1620,19 +1626,25 @@ __device__ __forceinline__ void cfl_block_max(unsigned long long m0,
 }
 
 // kRecord / kGrad: the output fields and the velocity gradients are
-// written (compiled out of the plain step).  Thread j takes the particle
-// at position j of this step's sorted order: slot perm[j] of `cur`, written
-// to slot j of `nxt`.  A pass whose loop condition failed copies `cur` to
-// `nxt` unchanged (the host exchanges the buffers after every pass).
+// written (compiled out of the plain step).  Thread t takes the particle
+// at position ng + t of this step's sorted order: slot perm[ng + t] of
+// `cur`, written to slot t of `nxt`.  ng = 0 outside slab mode; in slab
+// mode the first ng positions are the copies of the neighbour's last column
+// (they sort first), which only P2G reads, and a particle whose new cell
+// lies outside the slab's columns is listed in `leave` (and not counted:
+// it moves to the neighbour).  A pass whose loop condition failed copies
+// `cur` to `nxt` unchanged (the host exchanges the buffers after every
+// pass).
 template <bool kRecord, bool kGrad>
 __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
     k_g2p_t(Particles cur, Particles nxt, const int* __restrict__ perm,
             const int* __restrict__ skey, Nodes nodes, const double* __restrict__ Z, Geom G,
-            Phys P, Scalars* S, int* __restrict__ count) {
-  const int np = S->np;
+            Phys P, Scalars* S, int* __restrict__ count, int* __restrict__ leave) {
+  const int ng = S->nghost;
+  const int n = S->np - ng;  // the slab's own particles
   const int stride = gridDim.x * blockDim.x;
-  if (!S->active) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += stride)
+  if (!S->active) {  // (ghosts, imported last, sit in the slots after n)
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
       copy_moving(cur, j, nxt, j);
     return;
   }
@@ -1649,17 +1661,26 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   int bad = 0, kmin = 0x7fffffff, kmax = -1;
   const int lane = threadIdx.x & 31;
-  for (int j0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); j0 < np; j0 += stride) {
-    const int j = j0 + lane;
-    const bool ok = j < np;
+  for (int t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); t0 < n; t0 += stride) {
+    const int t = t0 + lane;
+    const bool ok = t < n;
     int nkey = -1;
+    bool stay = ok;
     if (ok) {
-      g2p_particle(cur, perm[j], skey[j], nxt, j, nodes, Z, G, P, sh, dt, kRecord ? 1 : 0,
+      const int j = ng + t;
+      g2p_particle(cur, perm[j], skey[j], nxt, t, nodes, Z, G, P, sh, dt, kRecord ? 1 : 0,
                    kGrad ? 1 : 0, 0, m0, m1, m2, bad, nkey);
       kmin = min(kmin, nkey);
       kmax = max(kmax, nkey);
+      if (leave) {
+        const int col = nkey / G.nrows;
+        if (col < G.pc_lo || col >= G.pc_hi) {
+          stay = false;
+          leave[atomicAdd(&S->nleave, 1)] = t;
+        }
+      }
     }
-    count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
+    count_key(nkey, stay, count, nxt.slot + (ok ? t : 0));
   }
   cfl_block_max(m0, m1, m2, red, S);
   key_range(kmin, kmax, kred, S);
@@ -1668,16 +1689,16 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
 
 void launch_g2p(int grid, cudaStream_t st, Particles cur, Particles nxt, const int* perm,
                 const int* skey, Nodes nodes, const double* Z, Geom G, Phys P, Scalars* S,
-                int* count, int record, int want_grad) {
+                int* count, int* leave, int record, int want_grad) {
   if (record)
     k_g2p_t<true, true><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, nodes, Z, G, P,
-                                                       S, count);
+                                                       S, count, leave);
   else if (want_grad)
     k_g2p_t<false, true><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, nodes, Z, G, P,
-                                                        S, count);
+                                                        S, count, leave);
   else
     k_g2p_t<false, false><<<grid, kG2PThreads, 0, st>>>(cur, nxt, perm, skey, nodes, Z, G,
-                                                         P, S, count);
+                                                         P, S, count, leave);
 }
 
 // Storage into reference order: the particle in slot j of src goes to slot

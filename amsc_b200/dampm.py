@@ -105,6 +105,17 @@ def _declare(lib):
                                          C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]),
         "dampm_batch_last_error": (C.c_char_p, [P]),
         "dampm_batch_tune": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
+        "dampm_slab_record_doubles": (C.c_int, []),
+        "dampm_slab_set": (C.c_int, [P, C.c_int, C.c_int]),
+        "dampm_slab_set_index": (C.c_int, [P, C.POINTER(C.c_int)]),
+        "dampm_slab_pass": (C.c_int, [P, C.c_int]),
+        "dampm_slab_node_column": (C.c_int, [P, C.c_int, P, C.c_int]),
+        "dampm_slab_cfl": (C.c_int, [P, _DP, C.c_int]),
+        "dampm_slab_route": (C.c_int, [P, P, P, C.c_longlong, C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_longlong)]),
+        "dampm_slab_ghosts": (C.c_int, [P, P, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "dampm_slab_import": (C.c_int, [P, P, C.c_longlong, C.c_int]),
+        "dampm_slab_download": (C.c_int, [P, C.c_char_p, _DP, C.POINTER(C.c_longlong)]),
         "dampm_json_read": (C.c_int, [C.c_char_p, C.POINTER(P)]),
         "dampm_json_size": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_longlong)]),
         "dampm_json_kind": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_int)]),

@@ -260,6 +260,51 @@ int dampm_cfl_dt_noalloc(const double* vpx, const double* vpy,
                          const double* hp, long long np, double g, double CFL,
                          double hx, double hy, double* out, void* cuda_stream);
 
+/* ---- One scenario over slabs of cell columns --------------------------------
+ * A scenario too large for one GPU (or one that should run on several)
+ * splits along x: each context in slab mode holds the whole grid's nodes
+ * and terrain and the particles of its cell columns [col_lo, col_hi).  The
+ * reference has no counterpart (one domain per process, main/optim_par.cpp
+ * :128-682, main/gpu_offload.cpp:258-271); with the exchanges below every
+ * particle's numbers equal the single-context run bit for bit.  A step is,
+ * for all slabs, in this order:
+ *   1. dampm_slab_ghosts on slab r, dampm_slab_import(.., ghosts=1) of the
+ *      result on slab r+1 (copies of slab r's last column, which P2G of
+ *      slab r+1 reads first);
+ *   2. dampm_slab_pass(ctx, 0): step start, sort, P2G;
+ *   3. dampm_slab_node_column(get) of column col_lo on slab r, (set) on slab
+ *      r-1 -- the (vvxL, vvyL) pairs G2P of slab r-1 interpolates;
+ *   4. dampm_slab_pass(ctx, 1): G2P, step end;
+ *   5. dampm_slab_route on every slab, dampm_slab_import(.., ghosts=0) of
+ *      its left / right output on slab r-1 / r+1 (particles that moved);
+ *   6. dampm_slab_cfl(get) on every slab, the element-wise maximum set on
+ *      every slab (the next CFL step).
+ * Buffers are device memory on the context's device holding particle
+ * records of dampm_slab_record_doubles() doubles.  A particle may move at
+ * most one slab per step (DAMPM_ERR_STATE otherwise).  Slab mode excludes
+ * merge/split, recorded outputs and CUDA graphs; dampm_step, dampm_download
+ * and the state calls return DAMPM_ERR_STATE in it. */
+int dampm_slab_record_doubles(void);
+/* After dampm_upload_particles of the slab's own particles (any order). */
+int dampm_slab_set(dampm_ctx* ctx, int col_lo, int col_hi);
+/* The reference index of each uploaded particle (np host ints). */
+int dampm_slab_set_index(dampm_ctx* ctx, const int* idx);
+int dampm_slab_ghosts(dampm_ctx* ctx, double* buf, long long cap, long long* n);
+int dampm_slab_import(dampm_ctx* ctx, const double* buf, long long n, int ghosts);
+int dampm_slab_pass(dampm_ctx* ctx, int phase);
+/* (Ney+1) pairs (vvxL, vvyL) of node column col: set != 0 writes them. */
+int dampm_slab_node_column(dampm_ctx* ctx, int col, double* buf, int set);
+/* Particles whose new cell is left of col_lo go to `left`, right of
+ * col_hi - 1 to `right` (NULL at the domain's edges); cap records each. */
+int dampm_slab_route(dampm_ctx* ctx, double* left, double* right, long long cap,
+                     long long* n_left, long long* n_right);
+/* {max |vpx|, max |vpy|, max hp} of the slab's last G2P (get), or the
+ * maxima over all slabs for the next step's CFL dt (set != 0). */
+int dampm_slab_cfl(dampm_ctx* ctx, double maxima[3], int set);
+/* One field of the slab's own particles in storage order, with their
+ * reference indices in idx (may be NULL).  Fields as dampm_get_state. */
+int dampm_slab_download(dampm_ctx* ctx, const char* field, double* out, long long* idx);
+
 /* ---- Batches of independent scenarios -------------------------------------
  * One set of device arrays holds many scenarios back to back, each with its
  * own grid, terrain, particles, physics and loop (fixed dt for NSTEPS passes,
