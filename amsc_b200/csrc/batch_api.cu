@@ -253,12 +253,13 @@ int enqueue_pass(dampm_batch* b) {
                                                b->Sg, 1);
   k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(b->count, ncell, b->tile_sum, b->start,
                                                 b->clist, b->clist_n, b->Sg, 1);
-  k_scatter<<<gp, 256, 0, st>>>(key, slot, b->start, b->perm, b->skey, b->Sg);
-  k_segment_order<<<148 * 4, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm, idx,
-                                            b->cmid, b->Sg);
-  k_segment_order_mid<<<148 * 8, 256, 0, st>>>(b->start, b->cmid, b->clist_n, b->perm, idx,
-                                                b->cbig, b->Sg);
-  k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm, idx,
+  k_scatter<<<gp, 256, 0, st>>>(key, slot, idx, b->start, b->perm, b->skey, b->sortbuf,
+                                b->Sg);
+  k_segment_order<<<148 * 4, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
+                                            b->sortbuf, b->cmid, b->Sg);
+  k_segment_order_mid<<<148 * 8, 256, 0, st>>>(b->start, b->cmid, b->clist_n, b->perm,
+                                                b->sortbuf, b->cbig, b->Sg);
+  k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
                                             b->sortbuf, b->P_cap, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
       b->start, b->scn, b->S, b->strip_scn, b->Sg, b->units_per_cta * b->p2g_grid,

@@ -249,17 +249,17 @@ void enqueue_sort(dampm_ctx* ctx) {
                                                              ctx->S, 1);
   k_scan_apply<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(
       ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S, 1);
-  k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->p.slot, ctx->start, ctx->perm,
-                                         ctx->skey, ctx->S);
+  k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->p.slot, ctx->p.idx, ctx->start,
+                                         ctx->perm, ctx->skey, ctx->sortbuf, ctx->S);
   k_segment_order<<<148 * 4, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,
-                                                   ctx->clist_n, ctx->perm, ctx->p.idx,
+                                                   ctx->clist_n, ctx->perm, ctx->sortbuf,
                                                    ctx->cmid, ctx->S);
   k_segment_order_mid<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->cmid,
-                                                       ctx->clist_n, ctx->perm, ctx->p.idx,
+                                                       ctx->clist_n, ctx->perm, ctx->sortbuf,
                                                        ctx->cbig, ctx->S);
   k_segment_order_big<<<148, 1024, 0, ctx->stream>>>(ctx->start, ctx->cbig, ctx->clist_n,
-                                                     ctx->perm, ctx->p.idx, ctx->sortbuf,
-                                                     ctx->cap, ctx->S);
+                                                     ctx->perm, ctx->sortbuf, ctx->cap,
+                                                     ctx->S);
   ctx->launches += 6;
 }
 

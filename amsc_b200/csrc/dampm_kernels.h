@@ -25,8 +25,14 @@ constexpr int kColWeight = DAMPM_COL_WEIGHT;
 constexpr int kPlanThreads = 1024;
 constexpr int kMaxStrips = 8192;  // strip offsets of the unit list in shared memory
 constexpr int kP2GThreads = 128;
-constexpr int kCap = 512;
-constexpr int kP2GMinBlocks = 4;
+#ifndef DAMPM_P2G_CAP
+#define DAMPM_P2G_CAP 512
+#endif
+#ifndef DAMPM_P2G_MIN_BLOCKS
+#define DAMPM_P2G_MIN_BLOCKS 4
+#endif
+constexpr int kCap = DAMPM_P2G_CAP;
+constexpr int kP2GMinBlocks = DAMPM_P2G_MIN_BLOCKS;
 constexpr int kG2PThreads = 256;
 #ifndef DAMPM_G2P_MIN_BLOCKS
 #define DAMPM_G2P_MIN_BLOCKS 4
@@ -149,16 +155,19 @@ __global__ void k_scan_sums(const int* count, int n, int* tile_sum, int* list_n,
 __global__ void k_scan_apply(int* count, int n, const int* tile_sum,
                              int* start, int* list, int* list_n,
                              const Scalars* S, int ranged);
-__global__ void k_scatter(const int* key, const int* slot, const int* start,
-                          int* perm, int* skey, Scalars* S);
+// pk: 2 x capacity entries; the scatter writes the first half, which the
+// per-cell ordering sorts (the crowded cells use both halves)
+__global__ void k_scatter(const int* key, const int* slot, const int* idx, const int* start,
+                          int* perm, int* skey, unsigned long long* pk, Scalars* S);
 __global__ void k_segment_order(const int* start, const int* list, int* list_n,
-                                int* perm, const int* idx, int* mid, const Scalars* S);
+                                int* perm, const unsigned long long* pk, int* mid,
+                                const Scalars* S);
 __global__ void k_segment_order_mid(const int* start, const int* mid, int* list_n,
-                                    int* perm, const int* idx, int* big, const Scalars* S);
-__global__ void k_segment_order_big(const int* start, const int* big,
-                                    const int* list_n, int* perm, const int* idx,
-                                    unsigned long long* tmp, long long cap,
+                                    int* perm, const unsigned long long* pk, int* big,
                                     const Scalars* S);
+__global__ void k_segment_order_big(const int* start, const int* big,
+                                    const int* list_n, int* perm, unsigned long long* pk,
+                                    long long cap, const Scalars* S);
 __global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
                              int target_units, int seg, int* ustart,
                              long long* upex, int2* plan, int* strip_n);

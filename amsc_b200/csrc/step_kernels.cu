@@ -417,14 +417,16 @@ __global__ void __launch_bounds__(kScanThreads)
   if (t == (n - 1) / kScanTile && threadIdx.x == blockDim.x - 1) start[n] = pre + incl;
 }
 
-// perm[start[key] + slot] = the storage slot, and skey there the key (the
-// cell of each sorted position, which G2P reads without waiting for perm);
-// block 0 then rolls the key ranges over: the starts now describe knext,
-// and the next G2P starts an empty knext.
+// perm[start[key] + slot] = the storage slot, skey there the key (the
+// cell of each sorted position, which G2P reads without waiting for perm)
+// and pk the entry idx << 32 | slot that the per-cell ordering sorts; block
+// 0 then rolls the key ranges over: the starts now describe knext, and the
+// next G2P starts an empty knext.
 __global__ void k_scatter(const int* __restrict__ key,
-                          const int* __restrict__ slot,
+                          const int* __restrict__ slot, const int* __restrict__ idx,
                           const int* __restrict__ start, int* __restrict__ perm,
-                          int* __restrict__ skey, Scalars* S) {
+                          int* __restrict__ skey, unsigned long long* __restrict__ pk,
+                          Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
@@ -433,6 +435,7 @@ __global__ void k_scatter(const int* __restrict__ key,
     const int pos = start[k] + slot[i];
     perm[pos] = i;
     skey[pos] = k;
+    pk[pos] = ((unsigned long long)(unsigned)idx[i] << 32) | (unsigned)i;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S->krange[0] = S->knext[0];
@@ -444,9 +447,10 @@ __global__ void k_scatter(const int* __restrict__ key,
 
 // Orders each listed cell's segment of perm (storage slots) by the
 // particles' reference index idx[slot] (the atomics of the count hand out
-// slots in arbitrary order).  A segment entry is handled as the 64-bit
-// value idx << 32 | slot, so sorting those values orders by reference index
-// (unique) and carries the slot along.  k_segment_order: each lane sorts a
+// slots in arbitrary order).  A segment entry is the 64-bit value
+// idx << 32 | slot that the scatter wrote to pk at the same position, so
+// sorting those values orders by reference index (unique) and carries the
+// slot along; a cell whose entries are already in order is left as it is.  k_segment_order: each lane sorts a
 // cell of up to kThreadSort particles in registers (a bitonic network over
 // static indices) and hands larger cells on to `mid`.  k_segment_order_mid,
 // one warp per cell: a register bitonic sort across the lanes for up to 32
@@ -460,15 +464,15 @@ constexpr int kRankPer = 8;
 constexpr int kBigRun = 4096;
 constexpr unsigned long long kNoEntry = ~0ull;
 
-__device__ __forceinline__ unsigned long long seg_entry(const int* __restrict__ idx, int s) {
-  return ((unsigned long long)(unsigned)idx[s] << 32) | (unsigned)s;
-}
-
 __device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m,
-                                                    const int* __restrict__ idx) {
+                                                    const unsigned long long* __restrict__ pk) {
   unsigned long long v[kThreadSort];
 #pragma unroll
-  for (int k = 0; k < kThreadSort; ++k) v[k] = k < m ? seg_entry(idx, seg[k]) : kNoEntry;
+  for (int k = 0; k < kThreadSort; ++k) v[k] = k < m ? pk[k] : kNoEntry;
+  bool in_order = true;
+#pragma unroll
+  for (int k = 1; k < kThreadSort; ++k) in_order &= (k >= m) || v[k - 1] < v[k];
+  if (in_order) return;  // perm already holds this order
 #pragma unroll
   for (int k = 2; k <= kThreadSort; k <<= 1) {
 #pragma unroll
@@ -493,11 +497,11 @@ __device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m
 
 __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b, int m,
                                                   int c, int lane,
-                                                  const int* __restrict__ idx,
+                                                  const unsigned long long* __restrict__ pk,
                                                   int* __restrict__ big,
                                                   int* __restrict__ list_n) {
   if (m <= 32) {
-    unsigned long long v = (lane < m) ? seg_entry(idx, perm[b + lane]) : kNoEntry;
+    unsigned long long v = (lane < m) ? pk[b + lane] : kNoEntry;
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
@@ -516,7 +520,7 @@ __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b,
 #pragma unroll
     for (int t = 0; t < kRankPer; ++t) {
       const int q = lane + 32 * t;
-      v[t] = (q < m) ? seg_entry(idx, perm[b + q]) : kNoEntry;
+      v[t] = (q < m) ? pk[b + q] : kNoEntry;
       rank[t] = 0;
     }
 #pragma unroll
@@ -541,7 +545,8 @@ __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b,
 __global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict__ start,
                                 const int* __restrict__ list,
                                 int* __restrict__ list_n,
-                                int* __restrict__ perm, const int* __restrict__ idx,
+                                int* __restrict__ perm,
+                                const unsigned long long* __restrict__ pk,
                                 int* __restrict__ mid, const Scalars* S) {
   if (!S->active) return;
   const int lane = threadIdx.x & 31;
@@ -556,7 +561,7 @@ __global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict_
       m = start[c + 1] - b;
     }
     if (m <= kThreadSort) {
-      if (m >= 2) thread_sort_segment(perm + b, m, idx);
+      if (m >= 2) thread_sort_segment(perm + b, m, pk + b);
     }
     // larger cells: one atomic per warp
     const unsigned larger = __ballot_sync(0xffffffffu, m > kThreadSort);
@@ -572,7 +577,8 @@ __global__ void __launch_bounds__(256, 4) k_segment_order(const int* __restrict_
 __global__ void __launch_bounds__(256, 4) k_segment_order_mid(const int* __restrict__ start,
                                     const int* __restrict__ mid,
                                     int* __restrict__ list_n,
-                                    int* __restrict__ perm, const int* __restrict__ idx,
+                                    int* __restrict__ perm,
+                                    const unsigned long long* __restrict__ pk,
                                     int* __restrict__ big, const Scalars* S) {
   if (!S->active) return;
   const int lane = threadIdx.x & 31;
@@ -581,22 +587,22 @@ __global__ void __launch_bounds__(256, 4) k_segment_order_mid(const int* __restr
        w += (gridDim.x * blockDim.x) >> 5) {
     const int c = mid[w];
     const int b = start[c];
-    warp_sort_segment(perm, b, start[c + 1] - b, c, lane, idx, big, list_n);
+    warp_sort_segment(perm, b, start[c + 1] - b, c, lane, pk, big, list_n);
   }
 }
 
 // Crowded cells (more than 32 * kRankPer particles), one block of 1024
-// threads each: the cell's entries (idx << 32 | slot) go to tmp[b, b+m);
-// runs of up to kBigRun are sorted by a bitonic network in shared memory;
-// longer cells then merge the sorted runs pairwise (each output position
-// finds its split by a binary search along the merge path), ping-ponging
-// between tmp[b, b+m) and tmp[cap + b, cap + b + m); the slots go back to
-// perm.
+// threads each: runs of up to kBigRun entries of tmp[b, b+m) (the pk the
+// scatter wrote) are sorted by a bitonic network in shared memory and
+// written back; longer cells then merge the sorted runs pairwise (each
+// output position finds its split by a binary search along the merge
+// path), ping-ponging between tmp[b, b+m) and tmp[cap + b, cap + b + m); the
+// slots go back to perm.
 __global__ void __launch_bounds__(1024)
     k_segment_order_big(const int* __restrict__ start, const int* __restrict__ big,
                         const int* __restrict__ list_n, int* __restrict__ perm,
-                        const int* __restrict__ idx, unsigned long long* __restrict__ tmp,
-                        long long cap, const Scalars* S) {
+                        unsigned long long* __restrict__ tmp, long long cap,
+                        const Scalars* S) {
   if (!S->active) return;
   __shared__ unsigned long long sv[kBigRun];
   const int nb = list_n[1];
@@ -608,7 +614,7 @@ __global__ void __launch_bounds__(1024)
       int P = 1;
       while (P < len) P <<= 1;
       for (int i = threadIdx.x; i < P; i += blockDim.x)
-        sv[i] = (i < len) ? seg_entry(idx, perm[b + r0 + i]) : kNoEntry;
+        sv[i] = (i < len) ? tmp[b + r0 + i] : kNoEntry;
       __syncthreads();
       for (int k = 2; k <= P; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
@@ -726,6 +732,9 @@ __device__ __forceinline__ void cp_async_commit() {
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() {  // all but the newest group
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
 struct Batch {
@@ -1384,14 +1393,26 @@ __global__ void k_ledger_final(const double* __restrict__ led_part,
 // cell of the step start, height update, Bingham stress, next cell key and
 // the CFL max-reductions (main/optim_par.cpp:532-651).
 // ---------------------------------------------------------------------------
+// The step-start values G2P reads of a particle.
+template <class R>
+struct G2PIn {
+  R x, y, hp, H, Mp, Vp;
+  int idx;
+};
+template <class R>
+__device__ __forceinline__ G2PIn<R> g2p_in(const ParticlesT<R>& src, int s) {
+  return G2PIn<R>{src.x[s], src.y[s], src.hp[s], src.H[s], src.Mp[s], src.Vp[s], src.idx[s]};
+}
+
 // One particle of G2P (the body of k_g2p and of the batched G2P): the
-// particle in slot `s` of the step-start buffer `src`, binned to cell `key`,
-// written to slot `j` of `dst` (its position in this step's sorted order).
-// key_off is the scenario's first cell in a batch (its cell keys are offset
-// by it); the new key is returned in `nkey`.
+// particle in slot `s` of the step-start buffer `src` -- its values `in` --
+// binned to cell `key`, written to slot `j` of `dst` (its position in this
+// step's sorted order).  key_off is the scenario's first cell in a batch (its
+// cell keys are offset by it); the new key is returned in `nkey`.
 template <class R>
 __device__ __forceinline__ void g2p_particle(
-    const ParticlesT<R>& src, int s, int key_in, const ParticlesT<R>& dst, int j,
+    const ParticlesT<R>& src, int s, const G2PIn<R>& in, int key_in,
+    const ParticlesT<R>& dst, int j,
     const NodesT<R>& nodes, const double* __restrict__ Z, const Geom& G, const Phys& P,
     const ShapeT<R>& sh, double dtd, int record, int want_grad, int key_off,
     unsigned long long& m0, unsigned long long& m1, unsigned long long& m2, int& bad,
@@ -1413,7 +1434,7 @@ __device__ __forceinline__ void g2p_particle(
     vxn[k] = v.x;
     vyn[k] = v.y;
   }
-  R x = src.x[s], y = src.y[s];
+  R x = in.x, y = in.y;
   R xi, eta;
   local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
   R vxL = R(0), vyL = R(0);
@@ -1469,12 +1490,12 @@ __device__ __forceinline__ void g2p_particle(
   }
   // height from the strain rate (main/optim_par.cpp:595-599)
   const R div = vxdx + vydy;
-  R hp = src.hp[s];
+  R hp = in.hp;
   hp = hp / (R(1) + dt * div);
   hp = hp < R(1e-2) ? R(1e-2) : hp;
   R F11, F12, F22;
-  const R H = src.H[s];
-  const R Mp = src.Mp[s], Vp = src.Vp[s];
+  const R H = in.H;
+  const R Mp = in.Mp, Vp = in.Vp;
   rheology_stress(P, vpx, vpy, hp, H, vxdx, vydy, vxdy, vydx, F11, F12, F22);
   dst.x[j] = x;
   dst.y[j] = y;
@@ -1487,7 +1508,7 @@ __device__ __forceinline__ void g2p_particle(
   dst.Mp[j] = Mp;
   dst.Vp[j] = Vp;
   dst.H[j] = H;
-  dst.idx[j] = src.idx[s];
+  dst.idx[j] = in.idx;
   const int nr = cell_row(double(y), hy, nrows), ncl = cell_col(double(x), hx, ncols);
   nkey = nr + ncl * nrows + key_off;
   dst.key[j] = nkey;
@@ -1661,15 +1682,45 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   int bad = 0, kmin = 0x7fffffff, kmax = -1;
   const int lane = threadIdx.x & 31;
-  for (int t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); t0 < n; t0 += stride) {
+  // Each thread copies the step-start values of its next particle into its
+  // own slots of shared memory (cp.async) while it works on the current
+  // one, so the gather through perm is in flight during the FP64 work.  A
+  // thread reads only what it copied itself: no block barrier is needed.
+  __shared__ double stv[2][6][kG2PThreads];
+  __shared__ int sti[2][kG2PThreads];
+  const int tid = threadIdx.x;
+  auto stage = [&](int buf, int t) {
+    const int s = perm[ng + t];
+    cp_async<8>(&stv[buf][0][tid], cur.x + s);
+    cp_async<8>(&stv[buf][1][tid], cur.y + s);
+    cp_async<8>(&stv[buf][2][tid], cur.hp + s);
+    cp_async<8>(&stv[buf][3][tid], cur.H + s);
+    cp_async<8>(&stv[buf][4][tid], cur.Mp + s);
+    cp_async<8>(&stv[buf][5][tid], cur.Vp + s);
+    cp_async<4>(&sti[buf][tid], cur.idx + s);
+    return s;
+  };
+  int t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  int s_cur = 0, buf = 0;
+  if (t0 + lane < n) s_cur = stage(0, t0 + lane);
+  cp_async_commit();
+  for (; t0 < n; t0 += stride, buf ^= 1) {
     const int t = t0 + lane;
     const bool ok = t < n;
+    const int tn = t + stride;
+    int s_next = 0;
+    if (tn < n) s_next = stage(buf ^ 1, tn);
+    cp_async_commit();
+    cp_async_wait_one();  // this particle's values are in stv[buf]
     int nkey = -1;
     bool stay = ok;
     if (ok) {
       const int j = ng + t;
-      g2p_particle(cur, perm[j], skey[j], nxt, t, nodes, Z, G, P, sh, dt, kRecord ? 1 : 0,
-                   kGrad ? 1 : 0, 0, m0, m1, m2, bad, nkey);
+      const G2PIn<double> in{stv[buf][0][tid], stv[buf][1][tid], stv[buf][2][tid],
+                             stv[buf][3][tid], stv[buf][4][tid], stv[buf][5][tid],
+                             sti[buf][tid]};
+      g2p_particle(cur, s_cur, in, skey[j], nxt, t, nodes, Z, G, P, sh, dt,
+                   kRecord ? 1 : 0, kGrad ? 1 : 0, 0, m0, m1, m2, bad, nkey);
       kmin = min(kmin, nkey);
       kmax = max(kmax, nkey);
       if (leave) {
@@ -1681,7 +1732,9 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
       }
     }
     count_key(nkey, stay, count, nxt.slot + (ok ? t : 0));
+    s_cur = s_next;
   }
+  cp_async_wait_all();
   cfl_block_max(m0, m1, m2, red, S);
   key_range(kmin, kmax, kred, S);
   flag_non_finite(bad, S);
@@ -1915,7 +1968,8 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   int bad = 0;
   if (ok)
-    g2p_particle(cur, perm[j], skey[j], nxt, j, nd, Z + n_off, G, P, sh, S[s].dt, 0, 0,
+    g2p_particle(cur, perm[j], g2p_in(cur, perm[j]), skey[j], nxt, j, nd, Z + n_off, G, P,
+                 sh, S[s].dt, 0, 0,
                  c_off, m0, m1, m2, bad, nkey);
   count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
   cfl_block_max(m0, m1, m2, red, &S[s]);
