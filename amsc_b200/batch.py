@@ -41,7 +41,7 @@ class Batch:
             raise DampmError(f"dampm_batch_create failed ({rc})")
         self.h = h
         self.np: Dict[int, int] = {}
-        self._tuning = (4, 192)  # the library's defaults
+        self._tuning = (2, 192)  # the library's defaults
 
     def _check(self, rc: int):
         if rc != 0:
@@ -119,7 +119,7 @@ class Batch:
         g = -1 if graphs is None else (1 if graphs else 0)
         self._check(self.lib.dampm_batch_tune(self.h, int(units_per_cta), int(col_weight), g))
 
-    def autotune(self, passes: int = 16, units=(2, 4, 8), weights=(64, 192, 512),
+    def autotune(self, passes: int = 16, units=(1, 2, 4, 8), weights=(64, 192, 512),
                  margin: float = 0.03) -> Dict:
         """Coordinate search over the unit plan (units per CTA, then column
         weight) from the current setting.  Each trial times `passes` passes

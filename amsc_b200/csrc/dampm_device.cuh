@@ -178,9 +178,17 @@ __device__ __forceinline__ void bingham_stress(const Phys& P, R vpx, R vpy, R hp
   const R mu = R(P.mu), tau_Y = R(P.tauy);
   const R ALF = hp > R(1.e-3) ? (R(6.) * mu * nrm) / ((hp + R(0.001)) * tau_Y) : R(0);
   const R B = -R(114.) / R(32.) - ALF;
-  const R Z1 = (-B + sqrt(B * B - R(4.) * A * C)) / (R(2.) * A);
-  const R Z2 = (-B - sqrt(B * B - R(4.) * A * C)) / (R(2.) * A);
-  const R ZZ = fabs(Z1 - R(.5)) <= R(.5) ? Z1 : Z2;
+  const R sq = sqrt(B * B - R(4.) * A * C);
+  const R Z2 = (-B - sq) / (R(2.) * A);
+  // The reference takes Z1 when |Z1 - 0.5| <= 0.5.  With B <= -3 (every
+  // ALF >= 0) Z1 = (-B + sq)/3 >= 1 rounds to at least 1.1875 whenever sq
+  // is a number (and is NaN otherwise), so Z2 is taken: Z1 is only
+  // evaluated where it can be chosen.  The result is the same in every case.
+  R ZZ = Z2;
+  if (!(B <= R(-3.))) {
+    const R Z1 = (-B + sq) / (R(2.) * A);
+    ZZ = fabs(Z1 - R(.5)) <= R(.5) ? Z1 : Z2;
+  }
   const R D_xx = vpx_dx;
   const R D_xy = R(0.5) * (vpx_dy + vpy_dx);
   const R D_yy = vpy_dy;
@@ -199,7 +207,8 @@ __device__ __forceinline__ void bingham_stress(const Phys& P, R vpx, R vpy, R hp
     sig_yy = k * D_yy;
   }
   const double hpd = hp, Hd = H;
-  const double h_corr = hpd > 1e-10 ? hpd - (Hd * Hd) / hpd : 0.0;
+  // (H*H)/hp is +0 when H == 0 (no still-water level): hp - 0 is hp
+  const double h_corr = hpd > 1e-10 ? (Hd == 0.0 ? hpd : hpd - (Hd * Hd) / hpd) : 0.0;
   const double pres = .5 * P.rho * P.g * h_corr;
   F11 = R(P.BING * double(sig_xx) - pres);
   F12 = R(P.BING * double(sig_xy));

@@ -14,7 +14,7 @@ namespace dampm {
 // particle records staged in shared memory kCap at a time.
 constexpr int kTR = 30;
 #ifndef DAMPM_UNITS_PER_CTA
-#define DAMPM_UNITS_PER_CTA 4
+#define DAMPM_UNITS_PER_CTA 2
 #endif
 #ifndef DAMPM_COL_WEIGHT
 #define DAMPM_COL_WEIGHT 192

@@ -208,7 +208,8 @@ __device__ __forceinline__ void next_record(const Geom& G, const Phys& P,
   }
   // gravity along the bed, well balanced (main/optim_par.cpp:447-454)
   const double hpd = hp, Hd = H, Vpd = Vp;
-  const double wb = hpd > 1e-10 ? 1.0 - (Hd / hpd) : 1.0;
+  // H/hp is +0 when H == 0 (no still-water level): 1 - 0 is 1
+  const double wb = (hpd > 1e-10 && Hd != 0.0) ? 1.0 - (Hd / hpd) : 1.0;
   gx = R(-P.g * Vpd * P.rho * dzx * wb);
   gy = R(-P.g * Vpd * P.rho * dzy * wb);
 }
@@ -732,9 +733,6 @@ __device__ __forceinline__ void cp_async_commit() {
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_one() {  // all but the newest group
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
 struct Batch {
@@ -1682,44 +1680,15 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   unsigned long long m0 = 0, m1 = 0, m2 = 0;
   int bad = 0, kmin = 0x7fffffff, kmax = -1;
   const int lane = threadIdx.x & 31;
-  // Each thread copies the step-start values of its next particle into its
-  // own slots of shared memory (cp.async) while it works on the current
-  // one, so the gather through perm is in flight during the FP64 work.  A
-  // thread reads only what it copied itself: no block barrier is needed.
-  __shared__ double stv[2][6][kG2PThreads];
-  __shared__ int sti[2][kG2PThreads];
-  const int tid = threadIdx.x;
-  auto stage = [&](int buf, int t) {
-    const int s = perm[ng + t];
-    cp_async<8>(&stv[buf][0][tid], cur.x + s);
-    cp_async<8>(&stv[buf][1][tid], cur.y + s);
-    cp_async<8>(&stv[buf][2][tid], cur.hp + s);
-    cp_async<8>(&stv[buf][3][tid], cur.H + s);
-    cp_async<8>(&stv[buf][4][tid], cur.Mp + s);
-    cp_async<8>(&stv[buf][5][tid], cur.Vp + s);
-    cp_async<4>(&sti[buf][tid], cur.idx + s);
-    return s;
-  };
-  int t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-  int s_cur = 0, buf = 0;
-  if (t0 + lane < n) s_cur = stage(0, t0 + lane);
-  cp_async_commit();
-  for (; t0 < n; t0 += stride, buf ^= 1) {
+  for (int t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); t0 < n; t0 += stride) {
     const int t = t0 + lane;
     const bool ok = t < n;
-    const int tn = t + stride;
-    int s_next = 0;
-    if (tn < n) s_next = stage(buf ^ 1, tn);
-    cp_async_commit();
-    cp_async_wait_one();  // this particle's values are in stv[buf]
     int nkey = -1;
     bool stay = ok;
     if (ok) {
       const int j = ng + t;
-      const G2PIn<double> in{stv[buf][0][tid], stv[buf][1][tid], stv[buf][2][tid],
-                             stv[buf][3][tid], stv[buf][4][tid], stv[buf][5][tid],
-                             sti[buf][tid]};
-      g2p_particle(cur, s_cur, in, skey[j], nxt, t, nodes, Z, G, P, sh, dt,
+      const int s = perm[j];
+      g2p_particle(cur, s, g2p_in(cur, s), skey[j], nxt, t, nodes, Z, G, P, sh, dt,
                    kRecord ? 1 : 0, kGrad ? 1 : 0, 0, m0, m1, m2, bad, nkey);
       kmin = min(kmin, nkey);
       kmax = max(kmax, nkey);
@@ -1732,9 +1701,7 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
       }
     }
     count_key(nkey, stay, count, nxt.slot + (ok ? t : 0));
-    s_cur = s_next;
   }
-  cp_async_wait_all();
   cfl_block_max(m0, m1, m2, red, S);
   key_range(kmin, kmax, kred, S);
   flag_non_finite(bad, S);

@@ -34,6 +34,8 @@ def test_slabs_equal_single_context(cuda_lib, case, nslabs, steps):
         for k in FIELDS:
             np.testing.assert_array_equal(run.gather(k), ref[k], err_msg=k)
         np.testing.assert_allclose(run.ledgers()[:6], led[:6], rtol=1e-12, atol=1e-9)
+        if case == "bench_slab":
+            return  # the fixed-dt slab moves too little to cross an edge in 40 steps
         # particles did cross the slab edges
         d2 = d.copy()
         d2.arrays["x"] = run.gather("x")
