@@ -85,6 +85,14 @@ struct dampm_ctx {
   int* sel = nullptr;        // slot lists (capacity)
   int* selcount = nullptr;   // one counter
   int2* moves = nullptr;     // hole fills (capacity)
+  // staged downloads (dampm_stage_download): fields gathered into reference
+  // order in `outbuf` on the step stream, copied to the host on `side`
+  cudaStream_t side = nullptr;
+  cudaEvent_t staged = nullptr;
+  double* outbuf = nullptr;
+  int outbuf_fields = 0;
+  long long outbuf_cap = 0;
+  bool side_pending = false;
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -535,7 +543,7 @@ __global__ void k_int_to_double(const int* a, double* b, const Scalars* S) {
     b[i] = double(a[i]);
 }
 
-// Ap, mom, Fb as the reference stores them at the end of a step
+// Ap (which 0) and Fb as the reference stores them at the end of a step
 // (main/optim_par.cpp:600-626), from the persistent state, into reference
 // order.
 __global__ void k_derived(Particles p, Phys P, const Scalars* S, int which,
@@ -545,16 +553,86 @@ __global__ void k_derived(Particles p, Phys P, const Scalars* S, int which,
        i += gridDim.x * blockDim.x) {
     const double hp = p.hp[i];
     double v = 0.0;
-    if (which == 0) v = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
-    else if (which == 1) v = p.vpx[i] * p.Mp[i];
-    else if (which == 2) v = p.vpy[i] * p.Mp[i];
+    if (which == 0) {
+      v = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
+    }
     else {
       double fx, fy;
       voellmy(P, p.vpx[i], p.vpy[i], hp, fx, fy);
-      v = (which == 3) ? fx : fy;
+      v = (which == 3) ? fx : fy;  // which 3, 4: Fb_x, Fb_y
     }
     out[p.idx[i]] = v;
   }
+}
+
+constexpr int kMaxStaged = 64;  // fields per dampm_stage_download call
+
+// Where a particle field comes from, as dampm_download names it.
+struct FieldSrc {
+  const double* sorted = nullptr;  // a field of the sorted slots
+  const double* ref = nullptr;     // a field already in reference order
+  const int* iref = nullptr;       // an integer field in reference order
+  int derived = -1;                // Ap / Fb formed from the state
+  int pair_half = -1;              // one half of the stored momentum pair
+};
+
+int resolve_field(dampm_ctx* ctx, const std::string& f, bool fresh, FieldSrc& r) {
+  Particles& p = ctx->p;
+  if (f == "x") r.sorted = p.x;
+  else if (f == "y") r.sorted = p.y;
+  else if (f == "Mp") r.sorted = p.Mp;
+  else if (f == "Vp") r.sorted = p.Vp;
+  else if (f == "H") r.sorted = p.H;
+  else if (f == "hp") r.sorted = p.hp;
+  else if (f == "vpx" || f == "vpxL") r.sorted = p.vpx;
+  else if (f == "vpy" || f == "vpyL") r.sorted = p.vpy;
+  else if (f == "F_11") r.sorted = p.F11;
+  else if (f == "F_12" || f == "F_21") r.sorted = p.F12;
+  else if (f == "F_22") r.sorted = p.F22;
+  else if (f == "xp") r.ref = p.xp;
+  else if (f == "yp") r.ref = p.yp;
+  else if (f == "vpx_dx") r.sorted = p.vpx_dx;
+  else if (f == "vpx_dy") r.sorted = p.vpx_dy;
+  else if (f == "vpy_dx") r.sorted = p.vpy_dx;
+  else if (f == "vpy_dy") r.sorted = p.vpy_dy;
+  else if (f == "label") r.iref = p.label;
+  else if (f == "level") r.iref = p.level;
+  // fresh values sit in reference-ordered slots (idx = slot)
+  else if (f == "Ap") { if (fresh) r.sorted = p.Ap; else r.derived = 0; }
+  else if (f == "mom_px" || f == "mom_py") r.pair_half = f == "mom_px" ? 0 : 1;
+  else if (f == "Fb_x") { if (fresh) r.sorted = p.Fbx; else r.derived = 3; }
+  else if (f == "Fb_y") { if (fresh) r.sorted = p.Fby; else r.derived = 4; }
+  else if (ctx->record_alloc) {
+    if (f == "apx") r.sorted = p.apx;
+    else if (f == "apy") r.sorted = p.apy;
+    else if (f == "Zp") r.sorted = p.Zp;
+    else if (f == "hpZ") r.sorted = p.hpZ;
+    else if (f == "dZxp") r.sorted = p.dZxp;
+    else if (f == "dZyp") r.sorted = p.dZyp;
+    else if (f == "Fpx") r.sorted = p.Fpx;
+    else if (f == "Fpy") r.sorted = p.Fpy;
+    else if (f == "Fric_px") r.sorted = p.Frx;
+    else if (f == "Fric_py") r.sorted = p.Fry;
+  }
+  if (!r.sorted && !r.ref && !r.iref && r.derived < 0 && r.pair_half < 0)
+    return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown particle field " + f);
+  return DAMPM_OK;
+}
+
+// The field into reference order at dst (np doubles), on the context stream.
+void enqueue_to_ref(dampm_ctx* ctx, const FieldSrc& r, double* dst, int np) {
+  Particles& p = ctx->p;
+  const int gp = grid_for(np, 256);
+  if (r.sorted)
+    k_to_ref<<<gp, 256, 0, ctx->stream>>>(r.sorted, p.idx, dst, ctx->S);
+  else if (r.pair_half >= 0)
+    k_pair_to_ref<<<gp, 256, 0, ctx->stream>>>(p.mp, r.pair_half, p.idx, dst, ctx->S);
+  else if (r.iref)
+    k_int_to_double<<<gp, 256, 0, ctx->stream>>>(r.iref, dst, ctx->S);
+  else if (r.derived >= 0)
+    k_derived<<<gp, 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, r.derived, dst);
+  else
+    cudaMemcpyAsync(dst, r.ref, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream);
 }
 
 }  // namespace
@@ -649,6 +727,11 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
 int dampm_ctx_destroy(dampm_ctx* ctx) {
   if (!ctx) return DAMPM_ERR_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->staged) cudaEventDestroy(ctx->staged);
   for (void* q : ctx->allocs) cudaFree(q);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   drop_graphs(ctx);
@@ -873,72 +956,14 @@ int dampm_download(dampm_ctx* ctx, const char* field, double* out) {
   int rc = sync_status(ctx, false);
   if (rc) return rc;
   const int np = ctx->Sh->np;
-  const bool fresh = ctx->Sh->fresh != 0;
-  const std::string f(field);
-  Particles& p = ctx->p;
-  const double* sorted = nullptr;  // a field of the sorted slots
-  const double* ref = nullptr;     // a field already in reference order
-  const int* iref = nullptr;       // an integer field in reference order
-  int derived = -1;
-  int pair_half = -1;  // mom_px / mom_py: one half of the momentum pair
-  if (f == "x") sorted = p.x;
-  else if (f == "y") sorted = p.y;
-  else if (f == "Mp") sorted = p.Mp;
-  else if (f == "Vp") sorted = p.Vp;
-  else if (f == "H") sorted = p.H;
-  else if (f == "hp") sorted = p.hp;
-  else if (f == "vpx" || f == "vpxL") sorted = p.vpx;
-  else if (f == "vpy" || f == "vpyL") sorted = p.vpy;
-  else if (f == "F_11") sorted = p.F11;
-  else if (f == "F_12" || f == "F_21") sorted = p.F12;
-  else if (f == "F_22") sorted = p.F22;
-  else if (f == "xp") ref = p.xp;
-  else if (f == "yp") ref = p.yp;
-  else if (f == "vpx_dx") sorted = p.vpx_dx;
-  else if (f == "vpx_dy") sorted = p.vpx_dy;
-  else if (f == "vpy_dx") sorted = p.vpy_dx;
-  else if (f == "vpy_dy") sorted = p.vpy_dy;
-  else if (f == "label") iref = p.label;
-  else if (f == "level") iref = p.level;
-  // fresh values sit in reference-ordered slots (idx = slot)
-  else if (f == "Ap") { if (fresh) sorted = p.Ap; else derived = 0; }
-  else if (f == "mom_px" || f == "mom_py") pair_half = f == "mom_px" ? 0 : 1;
-  else if (f == "Fb_x") { if (fresh) sorted = p.Fbx; else derived = 3; }
-  else if (f == "Fb_y") { if (fresh) sorted = p.Fby; else derived = 4; }
-  else if (ctx->record_alloc) {
-    if (f == "apx") sorted = p.apx;
-    else if (f == "apy") sorted = p.apy;
-    else if (f == "Zp") sorted = p.Zp;
-    else if (f == "hpZ") sorted = p.hpZ;
-    else if (f == "dZxp") sorted = p.dZxp;
-    else if (f == "dZyp") sorted = p.dZyp;
-    else if (f == "Fpx") sorted = p.Fpx;
-    else if (f == "Fpy") sorted = p.Fpy;
-    else if (f == "Fric_px") sorted = p.Frx;
-    else if (f == "Fric_py") sorted = p.Fry;
-  }
-  if (!sorted && !ref && !iref && derived < 0 && pair_half < 0)
-    return fail(ctx, DAMPM_ERR_UNKNOWN_FIELD, "unknown particle field " + f);
+  FieldSrc r;
+  rc = resolve_field(ctx, field, ctx->Sh->fresh != 0, r);
+  if (rc) return rc;
   if (np == 0) return DAMPM_OK;
   double* tmp = ctx->msb.stage;  // the merge/split scratch as a staging buffer
-  const int gp = grid_for(np, 256);
-  const double* src = ref;
-  if (sorted) {
-    k_to_ref<<<gp, 256, 0, ctx->stream>>>(sorted, p.idx, tmp, ctx->S);
-    src = tmp;
-  } else if (pair_half >= 0) {
-    k_pair_to_ref<<<gp, 256, 0, ctx->stream>>>(p.mp, pair_half, p.idx, tmp, ctx->S);
-    src = tmp;
-  } else if (iref) {
-    k_int_to_double<<<gp, 256, 0, ctx->stream>>>(iref, tmp, ctx->S);
-    src = tmp;
-  } else if (derived >= 0) {
-    k_derived<<<gp, 256, 0, ctx->stream>>>(p, ctx->P, ctx->S, derived, tmp);
-    src = tmp;
-  }
+  enqueue_to_ref(ctx, r, tmp, np);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(out, src, sizeof(double) * np, cudaMemcpyDeviceToHost,
-                     ctx->stream));
+  CK(cudaMemcpyAsync(out, tmp, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return DAMPM_OK;
 }
@@ -1336,6 +1361,66 @@ int dampm_slab_download(dampm_ctx* ctx, const char* field, double* out, long lon
     for (int k = 0; k < np; ++k) idx[k] = ix[k];
   }
   CK(cudaStreamSynchronize(ctx->stream));
+  return DAMPM_OK;
+}
+
+// ---- output without stalling the step loop ---------------------------------
+int dampm_staged_wait(dampm_ctx* ctx) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (ctx->side_pending) {
+    CK(cudaStreamSynchronize(ctx->side));
+    ctx->side_pending = false;
+  }
+  return DAMPM_OK;
+}
+
+int dampm_stage_download(dampm_ctx* ctx, int n, const char* const* fields,
+                         double* const* host_out, long long* np_out) {
+  if (!ctx || n < 0 || n > kMaxStaged || (n > 0 && (!fields || !host_out)))
+    return DAMPM_ERR_ARG;
+  if (ctx->slab) return fail(ctx, DAMPM_ERR_STATE, "slab mode: use the dampm_slab_* calls");
+  if (!ctx->particles_ok) return fail(ctx, DAMPM_ERR_STATE, "no particles");
+  int rc = dampm_staged_wait(ctx);  // the buffer of the last call is free again
+  if (rc) return rc;
+  rc = sync_status(ctx, false);
+  if (rc) return rc;
+  const int np = ctx->Sh->np;
+  const bool fresh = ctx->Sh->fresh != 0;
+  std::vector<FieldSrc> src(n);
+  for (int k = 0; k < n; ++k) {
+    if (!fields[k] || !host_out[k]) return DAMPM_ERR_ARG;
+    rc = resolve_field(ctx, fields[k], fresh, src[k]);
+    if (rc) return rc;
+  }
+  if (np_out) *np_out = np;
+  if (n == 0 || np == 0) return DAMPM_OK;
+  if (!ctx->side) {
+    CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming));
+  }
+  if (ctx->outbuf_fields < n || ctx->outbuf_cap != ctx->cap) {  // grows, then stays
+    if (ctx->outbuf) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      cudaFree(ctx->outbuf);
+      ctx->allocs.erase(std::remove(ctx->allocs.begin(), ctx->allocs.end(),
+                                    static_cast<void*>(ctx->outbuf)),
+                        ctx->allocs.end());
+      ctx->outbuf = nullptr;
+    }
+    rc = dalloc(ctx, &ctx->outbuf, size_t(n) * size_t(ctx->cap));
+    if (rc) return rc;
+    ctx->outbuf_fields = n;
+    ctx->outbuf_cap = ctx->cap;
+  }
+  for (int k = 0; k < n; ++k)
+    enqueue_to_ref(ctx, src[k], ctx->outbuf + size_t(k) * size_t(ctx->cap), np);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->staged, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->side, ctx->staged, 0));
+  for (int k = 0; k < n; ++k)
+    CK(cudaMemcpyAsync(host_out[k], ctx->outbuf + size_t(k) * size_t(ctx->cap),
+                       sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->side));
+  ctx->side_pending = true;
   return DAMPM_OK;
 }
 

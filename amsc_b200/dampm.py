@@ -105,6 +105,9 @@ def _declare(lib):
                                          C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]),
         "dampm_batch_last_error": (C.c_char_p, [P]),
         "dampm_batch_tune": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
+        "dampm_stage_download": (C.c_int, [P, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_DP),
+                                           C.POINTER(C.c_longlong)]),
+        "dampm_staged_wait": (C.c_int, [P]),
         "dampm_slab_record_doubles": (C.c_int, []),
         "dampm_slab_set": (C.c_int, [P, C.c_int, C.c_int]),
         "dampm_slab_set_index": (C.c_int, [P, C.POINTER(C.c_int)]),
@@ -138,6 +141,15 @@ def load_library(path: str = LIB_PATH):
             raise DampmError(f"{path} missing: build it with `python -m amsc_b200.build`")
         _lib = _declare(C.CDLL(path))
     return _lib
+
+
+def pinned_array(n: int) -> np.ndarray:
+    """A float64 array in page-locked host memory (device-to-host copies into
+    it run asynchronously); plain memory where no CUDA device is present."""
+    import torch
+    if torch.cuda.is_available():
+        return torch.empty(int(n), dtype=torch.float64, pin_memory=True).numpy()
+    return np.empty(int(n), dtype=np.float64)
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -281,6 +293,28 @@ class Solver:
             out = np.empty(n, dtype=np.float64)
         self._check(self.lib.dampm_download(self.h, name.encode(), _ptr(out)))
         return out
+
+    def stage_download(self, out: Dict[str, np.ndarray]) -> int:
+        """Starts copying the named particle fields into the given float64
+        arrays and returns at once; steps enqueued afterwards run meanwhile
+        when the arrays are page-locked (pinned_array).  Call staged_wait()
+        before reading them.  Returns the count of values each receives."""
+        names = list(out)
+        for k in names:
+            a = out[k]
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size < self.num_particles:
+                raise ValueError(f"{k}: needs a contiguous float64 array of >= np values")
+        self._staged = [out[k] for k in names]  # kept alive until the copies end
+        fields = (C.c_char_p * len(names))(*[k.encode() for k in names])
+        ptrs = (_DP * len(names))(*[_ptr(out[k]) for k in names])
+        n = C.c_longlong()
+        self._check(self.lib.dampm_stage_download(self.h, len(names), fields, ptrs,
+                                                  C.byref(n)))
+        return int(n.value)
+
+    def staged_wait(self):
+        self._check(self.lib.dampm_staged_wait(self.h))
+        self._staged = None
 
     def download_nodal(self, name: str) -> np.ndarray:
         out = np.empty(self.nn, dtype=np.float64)

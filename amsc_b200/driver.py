@@ -16,7 +16,11 @@ the C ABI and writes, as optim_par does:
 The steps between outputs run on the device without host synchronisation;
 output-only fields are materialised (dampm_record_outputs) only for the
 steps whose results are written, and the conservation rows come back from
-the device log in chunks.  The last line printed is
+the device log in chunks.  The particle fields of an output step are copied
+to page-locked buffers on a second stream while the next step runs
+(dampm_stage_download), and the files are formatted and written by a writer
+thread while the following steps run; two buffer sets alternate, so at most
+one output is being written while the next is copied.  The last line printed is
 ``PERF np=<n> counted_steps=<k> tot_s=<s>`` over the steps after the
 reference's 5 warm-up steps.
 """
@@ -26,24 +30,61 @@ import argparse
 import os
 import sys
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
 from . import outputs
 from .data import from_json
-from .dampm import Solver
+from .dampm import Solver, pinned_array
 
 _ZERO_VARS = ("div_v",)  # declared by optim_par, never computed
+
+
+_UNWRITTEN = ("F_ext_px", "F_ext_py")  # declared, never written by optim_par
 
 
 def particle_fields(s: Solver) -> dict:
     cols = {}
     for k in ("x", "y") + outputs.DPROPS + outputs.IPROPS:
-        if k in ("F_ext_px", "F_ext_py"):  # declared, never written by optim_par
+        if k in _UNWRITTEN:
             cols[k] = np.zeros(s.num_particles)
         else:
             cols[k] = s.download(k)
     return cols
+
+
+class _StagedParticles:
+    """Two sets of page-locked buffers for the particle fields of an output
+    step: one is copied into while the writer thread may still read the
+    other."""
+
+    NAMES = tuple(k for k in ("x", "y") + outputs.DPROPS + outputs.IPROPS if k not in _UNWRITTEN)
+
+    def __init__(self):
+        self.sets = [None, None]
+        self.busy = [None, None]  # the writer's future reading each set
+        self.turn = 0
+
+    def stage(self, s: Solver):
+        """Starts the copies of the particles as they are now; returns the
+        set index and the particle count."""
+        i = self.turn
+        self.turn ^= 1
+        if self.busy[i] is not None:
+            self.busy[i].result()
+            self.busy[i] = None
+        n = s.num_particles
+        if self.sets[i] is None or self.sets[i]["x"].size < n:
+            cap = max(n, 1)
+            self.sets[i] = {k: pinned_array(cap) for k in self.NAMES}
+        return i, s.stage_download(self.sets[i])
+
+    def columns(self, i: int, n: int) -> dict:
+        cols = {k: self.sets[i][k][:n] for k in self.NAMES}
+        for k in _UNWRITTEN:
+            cols[k] = np.zeros(n)
+        return cols
 
 
 def nodal_vars(s: Solver, nn: int) -> dict:
@@ -89,6 +130,9 @@ def run(data_path: str, outdir: str = ".", write: bool = True, max_steps: int = 
             outputs.write_vts(path("GRID_forZ.vts"), nrows, ncols, hx, hy, grid0)
             errf = open(path("conservation_errors.csv"), "w")
             outputs.write_errors_header(errf)
+            writer = ThreadPoolExecutor(max_workers=1)
+            staged = _StagedParticles()
+            pending = []
             logged, t0, warm_it = 0, None, 0
             st = s.status()
             while cond(st):
@@ -102,16 +146,25 @@ def run(data_path: str, outdir: str = ".", write: bool = True, max_steps: int = 
                     s.lib.dampm_record_outputs(s.h, 0)
                 st = s.status()
                 if cond(st) and st["it"] == nxt - 1:
-                    # step nxt begins: the particles as they are now
-                    outputs.write_particles_csv(path(f"nc_particles_{nxt}.csv"),
-                                                particle_fields(s))
+                    # step nxt begins: the particles as they are now, copied
+                    # while step nxt runs
+                    i, n = staged.stage(s)
                     s.lib.dampm_record_outputs(s.h, 1)
                     s.step(1)
                     s.lib.dampm_record_outputs(s.h, 0)
                     st = s.status()
+                    s.staged_wait()
+                    staged.busy[i] = writer.submit(outputs.write_particles_csv,
+                                                   path(f"nc_particles_{nxt}.csv"),
+                                                   staged.columns(i, n))
+                    pending.append(staged.busy[i])
                     if st["it"] == nxt:  # and its nodal vars once it has run
-                        outputs.write_vts(path(f"nc_grid_{nxt}.vts"), nrows, ncols, hx, hy,
-                                          nodal_vars(s, d.nnodes))
+                        pending.append(writer.submit(outputs.write_vts,
+                                                     path(f"nc_grid_{nxt}.vts"), nrows, ncols,
+                                                     hx, hy, nodal_vars(s, d.nnodes)))
+                    for f in [f for f in pending if f.done()]:
+                        f.result()  # a writer's exception surfaces here
+                    pending = [f for f in pending if not f.done()]
                 if st["it"] > logged:
                     rows = s.ledger_history(logged + 1, st["it"] - logged)
                     outputs.write_error_rows(errf, rows)
@@ -120,6 +173,9 @@ def run(data_path: str, outdir: str = ".", write: bool = True, max_steps: int = 
                     t0, warm_it = time.perf_counter(), st["it"]
                 if st["it"] == it:  # nothing ran: the loop has ended on the device
                     break
+            for f in pending:
+                f.result()  # a writer's exception surfaces here
+            writer.shutdown()
             errf.close()
             tot = time.perf_counter() - t0 if t0 is not None else 0.0
             it, np_ = st["it"], st["np"]

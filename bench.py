@@ -685,7 +685,8 @@ def main():
     # this implementation moves: P2G gathers the 13-value f64 record and the
     # slot (108 B) and writes vvxL, vvyL (16 B per node); G2P reads the slot,
     # key, index and x, y, hp, H, Mp, Vp (60 B) and writes the 11 state
-    # fields, key, index, sort slot and the 8-value record (164 B).
+    # fields, key, index, sort slot and the 8-value record (164 B), and reads
+    # vvxL, vvyL, Z (24 B per node).
     # The per-kernel times: the same warm-up and K steps once more, from the
     # same initial state, with CUDA events between the kernel classes (those
     # passes are launched one by one).

@@ -166,6 +166,19 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]);
  * `out` must hold the current particle count. */
 int dampm_download(dampm_ctx* ctx, const char* field, double* out);
 
+/* Output without stalling the step loop (the reference writes its output
+ * files from inside the step loop, main/optim_par.cpp:311-337): gathers up
+ * to 64 particle fields (the names of dampm_download) into reference order
+ * on the context's stream, copies them to host_out[k] on a second stream
+ * and returns once that is enqueued.  Steps enqueued afterwards run while
+ * the copies proceed (host_out must be page-locked for the copies to be
+ * asynchronous).  dampm_staged_wait() waits for the copies; the next
+ * dampm_stage_download waits for the previous one's first.  *np (may be
+ * NULL) receives the count of values each host_out array receives. */
+int dampm_stage_download(dampm_ctx* ctx, int n, const char* const* fields,
+                         double* const* host_out, long long* np);
+int dampm_staged_wait(dampm_ctx* ctx);
+
 /* Copies one nodal field ((Nex+1)*(Ney+1) values) of the last step:
  * vvxL, vvyL always; Mv, mom_vx, mom_vy, avx, avy, vvx, vvy, Ftot_vx,
  * Ftot_vy, F_ext_vx, F_ext_vy, F_int_vx, F_int_vy, FPxv, FPyv, Fric_x,

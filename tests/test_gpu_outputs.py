@@ -144,3 +144,31 @@ def test_empty_and_single_particle(cuda_lib):
     with Solver(d) as s:
         s.step(5)
         assert s.status()["np"] == 0
+
+
+@pytest.mark.gpu
+def test_staged_download_overlaps_later_steps(cuda_lib):
+    """Fields staged before a step hold the particles as they were when the
+    call was made, though later steps are enqueued before the copies are
+    waited for; they equal the synchronous download of the same state."""
+    from amsc_b200.dampm import pinned_array
+    d = scenarios.mudflow(N=128)
+    names = ("x", "y", "vpx", "hp", "Mp", "H", "mom_px", "label", "level")
+    with Solver(d) as s:
+        s.step(12)  # the particles are no longer in their initial order
+        want = {k: s.download(k) for k in names}
+        bufs = {k: pinned_array(s.num_particles + 5) for k in names}
+        n = s.stage_download(bufs)
+        assert n == s.num_particles
+        s.step(6)
+        s.staged_wait()
+        for k in names:
+            np.testing.assert_array_equal(bufs[k][:n], want[k], err_msg=k)
+        # the next call reuses the staging buffer after the last copies ended
+        want2 = {k: s.download(k) for k in names[:3]}
+        n2 = s.stage_download({k: bufs[k] for k in names[:3]})
+        s.staged_wait()
+        for k in names[:3]:
+            np.testing.assert_array_equal(bufs[k][:n2], want2[k], err_msg=k)
+        with pytest.raises(Exception):
+            s.stage_download({"no_such_field": bufs["x"]})
