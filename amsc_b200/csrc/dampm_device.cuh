@@ -18,6 +18,7 @@ struct Geom {
   double hx, hy;
   double Lx, Ly;  // Nex*hx, Ney*hy (main/optim_par.cpp:557-558)
   int hx_pow2, hy_pow2;  // h is a power of two: v/h == v*(1/h) exactly
+  double ihx, ihy;       // 1/hx, 1/hy (used where h is a power of two)
   // The part of the grid a slab owns (the whole grid outside slab mode):
   // particles of cell columns [pc_lo, pc_hi), node columns [nc_lo, nc_hi]
   // written by P2G.
@@ -79,18 +80,22 @@ __device__ __forceinline__ int node_of(int inode, int c, int r, int nrows) {
   }
 }
 
-// Cell (row, col) of a position: floor(y/hy), floor(x/hx), clamped.
-__device__ __forceinline__ int cell_row(double y, double hy, int nrows) {
-  double f = floor(y / hy);
+// Cell (row, col) of a position: floor(y/hy), floor(x/hx), clamped.  Where
+// h is a power of two the quotient equals the product with 1/h exactly
+// (both are the correctly rounded value of the same real number), and the
+// division is skipped.
+__device__ __forceinline__ int cell_index(double f, int n) {
   if (!(f >= 0.0)) return 0;
-  if (f > double(nrows - 1)) return nrows - 1;
+  if (f > double(n - 1)) return n - 1;
   return int(f);
 }
-__device__ __forceinline__ int cell_col(double x, double hx, int ncols) {
-  double f = floor(x / hx);
-  if (!(f >= 0.0)) return 0;
-  if (f > double(ncols - 1)) return ncols - 1;
-  return int(f);
+__device__ __forceinline__ int cell_row(double y, const Geom& G) {
+  if (G.hy_pow2) return cell_index(floor(y * G.ihy), G.nrows);
+  return cell_index(floor(y / G.hy), G.nrows);
+}
+__device__ __forceinline__ int cell_col(double x, const Geom& G) {
+  if (G.hx_pow2) return cell_index(floor(x * G.ihx), G.ncols);
+  return cell_index(floor(x / G.hx), G.ncols);
 }
 
 // The functions below are templates on the real type R of the particle

@@ -31,6 +31,10 @@ constexpr int kP2GThreads = 128;
 #ifndef DAMPM_P2G_MIN_BLOCKS
 #define DAMPM_P2G_MIN_BLOCKS 4
 #endif
+#ifndef DAMPM_CHAIN_UNROLL
+#define DAMPM_CHAIN_UNROLL 2  // P2G chain steps unrolled per loop trip
+#endif
+constexpr int kChainUnroll = DAMPM_CHAIN_UNROLL;
 constexpr int kCap = DAMPM_P2G_CAP;
 constexpr int kP2GMinBlocks = DAMPM_P2G_MIN_BLOCKS;
 constexpr int kG2PThreads = 256;

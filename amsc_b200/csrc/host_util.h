@@ -20,6 +20,8 @@ inline Geom make_geom(const dampm_grid& g) {
   int e;
   G.hx_pow2 = std::frexp(g.hx, &e) == 0.5 ? 1 : 0;
   G.hy_pow2 = std::frexp(g.hy, &e) == 0.5 ? 1 : 0;
+  G.ihx = 1.0 / g.hx;
+  G.ihy = 1.0 / g.hy;
   G.pc_lo = 0;
   G.pc_hi = g.Nex;
   G.nc_lo = 0;

@@ -89,7 +89,7 @@ __global__ void k_init_particles(ParticlesT<R> p, const double* __restrict__ Z,
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
     const double x = p.x[i], y = p.y[i];
-    const int r = cell_row(y, G.hy, G.nrows), c = cell_col(x, G.hx, G.ncols);
+    const int r = cell_row(y, G), c = cell_col(x, G);
     p.key[i] = r + c * G.nrows + key_off;
     p.idx[i] = i;
     p.label[i] = i;
@@ -144,8 +144,8 @@ __global__ void k_keys(Particles p, Geom G, Scalars* S) {
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
-    const int r = cell_row(p.y[i], G.hy, G.nrows);
-    const int c = cell_col(p.x[i], G.hx, G.ncols);
+    const int r = cell_row(p.y[i], G);
+    const int c = cell_col(p.x[i], G);
     p.key[i] = r + c * G.nrows;
     p.idx[i] = i;
   }
@@ -191,8 +191,8 @@ __device__ __forceinline__ void next_record(const Geom& G, const Phys& P,
                                             const double* __restrict__ Z, R x,
                                             R y, R hp, R H, R Vp, R& xi, R& eta,
                                             R& gx, R& gy) {
-  const int r = cell_row(double(y), G.hy, G.nrows);
-  const int c = cell_col(double(x), G.hx, G.ncols);
+  const int r = cell_row(double(y), G);
+  const int c = cell_col(double(x), G);
   const R ihx = R(1) / R(G.hx), ihy = R(1) / R(G.hy);
   local_xy_g(x, y, c, r, G, ihx, ihy, xi, eta);
   // g2pd Z -> dZxp, dZyp (main/optim_par.cpp:387)
@@ -883,7 +883,7 @@ struct Chains {
   R f[kMaxQ], fc[kMaxQ], s[kMaxQ], sc[kMaxQ];
 };
 
-// One particle's contributions to the chains of quantity group kG: `upper`
+// One particle's contributions to the chains of quantity group kG: kUpper
 // selects the cell (r-1: local nodes 1 (fin) and 3 (start); r: local nodes 0
 // and 2).  With fb = eta or (1-eta):
 //   fin   N = (1-xi)*fb, Nx = mihx*fb, Ny = (1-xi)*(ihy or mihy)
@@ -891,15 +891,15 @@ struct Chains {
 // -- shp/shg of main/gpu_kernels.cpp:33-59 for those local nodes.  kFin off
 // runs the started chains alone (a unit's leading column).  Group 0 also
 // adds Mp and the momentum to the particle ledger (`led`, once per particle).
-template <class R, int kG, bool kFin>
+template <class R, int kG, bool kFin, bool kUpper>
 __device__ __forceinline__ void chain_step(Chains<R>& a, const P2GSmemT<R>& s, int j,
-                                           bool upper, const ShapeT<R>& sh, bool led,
+                                           const ShapeT<R>& sh, bool led,
                                            double& lp0, double& lp1, double& lp2) {
   const int l2 = swz_pair<R>(j), l1 = swz_one<R>(j);
   const V2<R> xe = s.pr[0][l2];
   const R xi = xe.x, eta = xe.y;
   const R fa = R(1) - xi;
-  const R fb = upper ? eta : (R(1) - eta);
+  const R fb = kUpper ? eta : (R(1) - eta);
   if constexpr (kG == 0 || kG == 1) {
     constexpr int nq = kG == 0 ? 3 : 4;
     const R Nf = fa * fb;
@@ -929,7 +929,7 @@ __device__ __forceinline__ void chain_step(Chains<R>& a, const P2GSmemT<R>& s, i
 #pragma unroll
     for (int k = 0; k < nq; ++k) acc_add(a.s[k], a.sc[k], Ns * q[k]);
   } else {
-    const R hy = upper ? sh.ihy : sh.mihy;
+    const R hy = kUpper ? sh.ihy : sh.mihy;
     const R Nxs = sh.ihx * fb, Nys = xi * hy;
     const R f12 = s.sg[2][l1], vp = s.sg[4][l1];
     const R fo = kG == 2 ? s.sg[1][l1] : s.sg[3][l1];  // F11 or F22
@@ -945,20 +945,23 @@ __device__ __forceinline__ void chain_step(Chains<R>& a, const P2GSmemT<R>& s, i
 }
 
 // The particles of cells (r-1, cc) and (r, cc) are the adjacent ranges
-// [a0, a1) and [a1, b1) of the sorted order: one walk in order.
+// [a0, a1) and [a1, b1) of the sorted order, walked in order: the first
+// with the upper cell's shape factors, the second with the lower cell's
+// (whose particles the lane's own row counts into the particle ledger).
 template <class R, int kG, bool kFin>
 __device__ __forceinline__ void chain_range(Chains<R>& a, const P2GSmemT<R>& s, int a0,
                                             int a1, int b1, int bb, int be,
                                             const ShapeT<R>& sh, bool own,
                                             double& lp0, double& lp1, double& lp2) {
-  const int j1 = min(b1, be);
+  const int u1 = min(a1, be);
   int j = max(a0, bb);
-#pragma unroll 2
-  for (; j < j1; ++j) {
-    const bool upper = j < a1;
-    chain_step<R, kG, kFin>(a, s, j - bb, upper, sh, kG == 0 && own && !upper, lp0, lp1,
-                            lp2);
-  }
+#pragma unroll kChainUnroll
+  for (; j < u1; ++j) chain_step<R, kG, kFin, true>(a, s, j - bb, sh, false, lp0, lp1, lp2);
+  const int j1 = min(b1, be);
+  const bool led = kG == 0 && own;
+  j = max(a1, bb);
+#pragma unroll kChainUnroll
+  for (; j < j1; ++j) chain_step<R, kG, kFin, false>(a, s, j - bb, sh, led, lp0, lp1, lp2);
 }
 
 template <class R, int kG>
@@ -1415,8 +1418,7 @@ __device__ __forceinline__ void g2p_particle(
     const ShapeT<R>& sh, double dtd, int record, int want_grad, int key_off,
     unsigned long long& m0, unsigned long long& m1, unsigned long long& m2, int& bad,
     int& nkey) {
-  const int nrows = G.nrows, ncols = G.ncols;
-  const double hx = G.hx, hy = G.hy;
+  const int nrows = G.nrows;
   const R ihx = sh.ihx, mihx = sh.mihx;
   const R ihy = sh.ihy, mihy = sh.mihy;
   const R eps = R(1e-10);
@@ -1507,7 +1509,7 @@ __device__ __forceinline__ void g2p_particle(
   dst.Vp[j] = Vp;
   dst.H[j] = H;
   dst.idx[j] = in.idx;
-  const int nr = cell_row(double(y), hy, nrows), ncl = cell_col(double(x), hx, ncols);
+  const int nr = cell_row(double(y), G), ncl = cell_col(double(x), G);
   nkey = nr + ncl * nrows + key_off;
   dst.key[j] = nkey;
   if (want_grad) {
