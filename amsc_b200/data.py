@@ -37,9 +37,15 @@ OPTIONAL_DEFAULTS = {
     # no counterpart in the reference (which ignores the key): merge only
     # pairs closer than ms_pair_dist * min(hx, hy); 0 = no limit
     "ms_pair_dist": 0.0,
+    # no counterpart among the reference's DATA keys: which merge/split runs
+    # at the cadence -- 0 the one gpu_offload calls (main/merge_split_ops_cmes.h),
+    # 1 the ELFS variant of main/merge_split_ops.h -- and the ELFS
+    # divergence trigger (its ms_config::stretch_thresh default)
+    "ms_variant": 0,
+    "ms_stretch_thresh": 1e7,
 }
 _INT_KEYS = {"Nex", "Ney", "BC_FLAG", "MERGE_SPLIT_ON", "NSTEPS", "ms_min_level",
-             "ms_max_level", "ms_min_particles_per_cell", "ms_call_interval"}
+             "ms_max_level", "ms_min_particles_per_cell", "ms_call_interval", "ms_variant"}
 
 
 class DataError(KeyError):

@@ -64,6 +64,7 @@ def _base_scalars(**kw) -> dict:
         "ms_shear_split": 1e30, "ms_hp_min": 0.05, "ms_max_dv": 0.01,
         "ms_min_level": -2, "ms_max_level": 2, "ms_min_particles_per_cell": 2,
         "ms_call_interval": 10, "ms_max_ops": 1e9, "ms_pair_dist": 0.0,
+        "ms_variant": 0, "ms_stretch_thresh": 1e7,
     }
     s.update(kw)
     return s

@@ -62,6 +62,8 @@ typedef struct {
   int ms_min_level, ms_max_level, ms_min_particles_per_cell, ms_call_interval;
   double ms_max_ops;
   double ms_pair_dist;  // pair-distance gate (0: none, the reference's pairing)
+  int ms_variant;            // 0: merge_split_ops_cmes.h, 1: merge_split_ops.h (ELFS)
+  double ms_stretch_thresh;  // ELFS ms_config::stretch_thresh
 } oracle_data;
 
 }  // extern "C"
@@ -440,49 +442,17 @@ inline void principal_stretch_dir(double exx, double eyy, double exy,
   }
 }
 
-// decide_actions: merge_split_ops_cmes.h:116-253 (grd_to_ptcl = CSR order)
-void decide_actions(Oracle& o, double dt, std::vector<int>& act,
-                    std::vector<int>& partner) {
-  const idx_t N = o.np;
-  act.assign(N, KEEP);
-  partner.assign(N, -1);
-  const double min_h = std::min(o.hx, o.hy);
-  const double r_split = o.d.ms_alpha * min_h;
-  const double r_merge = o.d.ms_beta * min_h;
-  const double shear_split = o.d.ms_shear_split;
-  const double split_hp_min = o.d.ms_split_hp_min;
-  const double hp_min = o.d.ms_hp_min;
-  const int min_level = o.d.ms_min_level, max_level = o.d.ms_max_level;
-  const int max_ops = (int)o.d.ms_max_ops;  // gpu_offload.cpp:317
-  const int min_ppc = o.d.ms_min_particles_per_cell;
-  const double* Ap = o.dprops.at("Ap").data();
-  const double* hp = o.dprops.at("hp").data();
-  const double* exx_ = o.dprops.at("vpx_dx").data();
-  const double* eyy_ = o.dprops.at("vpy_dy").data();
-  const double* exy1 = o.dprops.at("vpx_dy").data();
-  const double* exy2 = o.dprops.at("vpy_dx").data();
-  const idx_t* lvl = o.iprops.at("level").data();
-  for (idx_t ip = 0; ip < N; ++ip) {
-    const double r_i = std::sqrt(Ap[ip]);
-    const double exx = exx_[ip], eyy = eyy_[ip];
-    const double exy = 0.5 * (exy1[ip] + exy2[ip]);
-    const double gdot = std::sqrt(2.0 * (exx * exx + eyy * eyy + 2.0 * exy * exy));
-    const bool stretched = (r_i > r_split);
-    const bool sheared = (gdot * dt > shear_split);
-    const bool thick = (r_i < r_merge);
-    const bool thin_skip = (hp[ip] < split_hp_min);
-    if ((stretched || sheared) && !thin_skip && (int(lvl[ip]) > min_level))
-      act[ip] = SPLIT;
-    else if (thick && hp[ip] > hp_min && int(lvl[ip]) < max_level)
-      act[ip] = MERGE_PRIMARY;
-  }
+// The per-cell part of decide_actions, cells in order with their particles
+// in index order (grd_to_ptcl = CSR order): the split cap, the greedy
+// pairing of co-moving merge candidates and the undo of merges while a cell
+// would hold fewer than min_ppc particles.  merge_split_ops_cmes.h:174-249
+// (split_w 2, min_ppc = min_particles_per_cell, the optional gate) and
+// merge_split_ops.h:406-497 (split_w 4, min_ppc 2, no gate) differ only in
+// those three.  Writes the counts to ms_counts[0..1].
+void pair_in_cells(Oracle& o, std::vector<int>& act, std::vector<int>& partner, int max_ops,
+                   double max_dv2, double gate2, int split_w, int min_ppc) {
   const double* vpx = o.dprops.at("vpx").data();
   const double* vpy = o.dprops.at("vpy").data();
-  const double max_dv2 = o.d.ms_max_dv * o.d.ms_max_dv;
-  // the optional pair-distance gate (no counterpart in the reference)
-  const double gmin_h = (o.d.hy < o.d.hx) ? o.d.hy : o.d.hx;
-  const double gr = o.d.ms_pair_dist * gmin_h;
-  const double gate2 = o.d.ms_pair_dist > 0.0 ? gr * gr : 0.0;
   long long n_split = 0, n_merge = 0;
   for (idx_t cell = 0; cell < o.ncells(); ++cell) {
     const idx_t b = o.cell_start[cell], e = o.cell_start[cell + 1];
@@ -533,7 +503,7 @@ void decide_actions(Oracle& o, double dt, std::vector<int>& act,
     for (idx_t j = b; j < e; ++j) {
       const int a = act[o.cell_ptcls[j]];
       if (a == KEEP) projected += 1;
-      else if (a == SPLIT) projected += 2;
+      else if (a == SPLIT) projected += split_w;
       else if (a == MERGE_PRIMARY) projected += 1;
     }
     while (projected < min_ppc) {
@@ -556,6 +526,50 @@ void decide_actions(Oracle& o, double dt, std::vector<int>& act,
   }
   o.ms_counts[0] = n_split;
   o.ms_counts[1] = n_merge;
+}
+
+// decide_actions: merge_split_ops_cmes.h:116-253 (grd_to_ptcl = CSR order)
+void decide_actions(Oracle& o, double dt, std::vector<int>& act,
+                    std::vector<int>& partner) {
+  const idx_t N = o.np;
+  act.assign(N, KEEP);
+  partner.assign(N, -1);
+  const double min_h = std::min(o.hx, o.hy);
+  const double r_split = o.d.ms_alpha * min_h;
+  const double r_merge = o.d.ms_beta * min_h;
+  const double shear_split = o.d.ms_shear_split;
+  const double split_hp_min = o.d.ms_split_hp_min;
+  const double hp_min = o.d.ms_hp_min;
+  const int min_level = o.d.ms_min_level, max_level = o.d.ms_max_level;
+  const int max_ops = (int)o.d.ms_max_ops;  // gpu_offload.cpp:317
+  const int min_ppc = o.d.ms_min_particles_per_cell;
+  const double* Ap = o.dprops.at("Ap").data();
+  const double* hp = o.dprops.at("hp").data();
+  const double* exx_ = o.dprops.at("vpx_dx").data();
+  const double* eyy_ = o.dprops.at("vpy_dy").data();
+  const double* exy1 = o.dprops.at("vpx_dy").data();
+  const double* exy2 = o.dprops.at("vpy_dx").data();
+  const idx_t* lvl = o.iprops.at("level").data();
+  for (idx_t ip = 0; ip < N; ++ip) {
+    const double r_i = std::sqrt(Ap[ip]);
+    const double exx = exx_[ip], eyy = eyy_[ip];
+    const double exy = 0.5 * (exy1[ip] + exy2[ip]);
+    const double gdot = std::sqrt(2.0 * (exx * exx + eyy * eyy + 2.0 * exy * exy));
+    const bool stretched = (r_i > r_split);
+    const bool sheared = (gdot * dt > shear_split);
+    const bool thick = (r_i < r_merge);
+    const bool thin_skip = (hp[ip] < split_hp_min);
+    if ((stretched || sheared) && !thin_skip && (int(lvl[ip]) > min_level))
+      act[ip] = SPLIT;
+    else if (thick && hp[ip] > hp_min && int(lvl[ip]) < max_level)
+      act[ip] = MERGE_PRIMARY;
+  }
+  const double max_dv2 = o.d.ms_max_dv * o.d.ms_max_dv;
+  // the optional pair-distance gate (no counterpart in the reference)
+  const double gmin_h = (o.d.hy < o.d.hx) ? o.d.hy : o.d.hx;
+  const double gr = o.d.ms_pair_dist * gmin_h;
+  const double gate2 = o.d.ms_pair_dist > 0.0 ? gr * gr : 0.0;
+  pair_in_cells(o, act, partner, max_ops, max_dv2, gate2, 2, min_ppc);
 }
 
 // execute_merge_split: merge_split_ops_cmes.h:258-427
@@ -707,6 +721,282 @@ void adaptive_merge_split(Oracle& o, double dt) {
     if (a != KEEP) { any = true; break; }
   if (any) execute_merge_split(o, act, partner);
   o.ms_counts[3] = o.np;
+}
+
+// ---------------------------------------------------------------------------
+// ELFS merge/split: main/merge_split_ops.h (refine near the free surface,
+// coarsen far from it; splits 1 -> 4)
+// ---------------------------------------------------------------------------
+// Cells with particles (grd_to_ptcl's non-empty lists).
+std::vector<char> wet_cells(const Oracle& o) {
+  std::vector<char> wet(o.ncells(), 0);
+  for (idx_t c = 0; c < o.ncells(); ++c) wet[c] = o.cell_start[c + 1] > o.cell_start[c];
+  return wet;
+}
+
+// mark_exterior_cells, merge_split_ops.h:86-164: the empty cells connected
+// to an empty cell on the grid's edge through empty cells (4-neighbours).
+// The set does not depend on the visiting order; this walks it depth first.
+std::vector<char> exterior_cells(const Oracle& o, const std::vector<char>& wet) {
+  const idx_t nr = o.nrows, nc = o.ncols;
+  std::vector<char> ext(o.ncells(), 0);
+  std::vector<idx_t> stack;
+  auto seed = [&](idx_t r, idx_t c) {
+    const idx_t k = r + nr * c;
+    if (!wet[k] && !ext[k]) {
+      ext[k] = 1;
+      stack.push_back(k);
+    }
+  };
+  for (idx_t c = 0; c < nc; ++c) {
+    seed(0, c);
+    seed(nr - 1, c);
+  }
+  for (idx_t r = 0; r < nr; ++r) {
+    seed(r, 0);
+    seed(r, nc - 1);
+  }
+  while (!stack.empty()) {
+    const idx_t k = stack.back();
+    stack.pop_back();
+    const idx_t r = k % nr, c = k / nr;
+    if (r > 0) seed(r - 1, c);
+    if (r + 1 < nr) seed(r + 1, c);
+    if (c > 0) seed(r, c - 1);
+    if (c + 1 < nc) seed(r, c + 1);
+  }
+  return ext;
+}
+
+// compute_boundary_distance, merge_split_ops.h:170-260: hops through wet
+// cells (4-neighbours) from the wet cells off the grid's edge that have an
+// exterior cell left or right of them (the seeds, 0), times min(hx, hy);
+// cells no hop reaches keep DBL_MAX.  A breadth-first search by levels: the
+// hop count of a cell is unique, whatever the order inside a level.
+std::vector<double> boundary_distance(const Oracle& o, const std::vector<char>& wet,
+                                      const std::vector<char>& ext) {
+  const idx_t nr = o.nrows, nc = o.ncols;
+  const double h = std::min(o.hx, o.hy);
+  std::vector<double> dist(o.ncells(), std::numeric_limits<double>::max());
+  std::vector<int> hops(o.ncells(), -1);
+  std::vector<idx_t> level, next;
+  for (idx_t c = 0; c < nc; ++c)
+    for (idx_t r = 0; r < nr; ++r) {
+      const idx_t k = r + nr * c;
+      if (!wet[k]) continue;
+      if (r == 0 || r == nr - 1 || c == 0 || c == nc - 1) continue;
+      if (ext[r + nr * (c - 1)] || ext[r + nr * (c + 1)]) {
+        hops[k] = 0;
+        dist[k] = 0.0;
+        level.push_back(k);
+      }
+    }
+  for (int d = 0; !level.empty(); ++d) {
+    next.clear();
+    for (idx_t k : level) {
+      const idx_t r = k % nr, c = k / nr;
+      const idx_t nb[4] = {r > 0 ? k - 1 : -1, r + 1 < nr ? k + 1 : -1,
+                           c > 0 ? k - nr : -1, c + 1 < nc ? k + nr : -1};
+      for (idx_t q : nb) {
+        if (q < 0 || !wet[q] || hops[q] >= 0) continue;
+        hops[q] = d + 1;
+        dist[q] = (d + 1) * h;
+        next.push_back(q);
+      }
+    }
+    level.swap(next);
+  }
+  return dist;
+}
+
+// compute_elfs, merge_split_ops.h:266-343: the cell distance, refined for
+// particles within max(hx, hy) of the surface by the distance to the
+// nearest exterior cell box among the two cells left and right in the row.
+std::vector<double> elfs_values(const Oracle& o, const std::vector<double>& dist,
+                                const std::vector<char>& ext) {
+  const idx_t nr = o.nrows, nc = o.ncols;
+  const double hx = o.hx, hy = o.hy;
+  const double refine = std::max(hx, hy);
+  std::vector<double> e(o.np);
+  for (idx_t ip = 0; ip < o.np; ++ip) {
+    const idx_t cell = o.p2c[ip];
+    const double base = dist[cell];
+    if (base > refine) {
+      e[ip] = base;
+      continue;
+    }
+    const double px = o.x[ip], py = o.y[ip];
+    double md = base;
+    const idx_t r = cell % nr, c0 = cell / nr;
+    for (int dc = -2; dc <= 2; ++dc) {
+      const idx_t c = c0 + dc;
+      if (c < 0 || c >= nc) continue;
+      if (!ext[r + nr * c]) continue;
+      const double cx_lo = c * hx, cx_hi = (c + 1) * hx;
+      const double cy_lo = r * hy, cy_hi = (r + 1) * hy;
+      const double qx = px < cx_lo ? cx_lo : (px > cx_hi ? cx_hi : px);
+      const double qy = py < cy_lo ? cy_lo : (py > cy_hi ? cy_hi : py);
+      const double dx = px - qx, dy = py - qy;
+      const double d = std::sqrt(dx * dx + dy * dy);
+      if (d < md) md = d;
+    }
+    e[ip] = md;
+  }
+  return e;
+}
+
+// decide_actions, merge_split_ops.h:349-510: split near the surface (elfs <
+// alpha * sqrt(Ap)) or where the divergence exceeds stretch_thresh, merge
+// far from it (elfs > beta * sqrt(Ap), hp > hp_min), then the cells.
+void decide_actions_elfs(Oracle& o, std::vector<int>& act, std::vector<int>& partner) {
+  const idx_t N = o.np;
+  act.assign(N, KEEP);
+  partner.assign(N, -1);
+  const std::vector<char> wet = wet_cells(o);
+  const std::vector<char> ext = exterior_cells(o, wet);
+  const std::vector<double> dist = boundary_distance(o, wet, ext);
+  const std::vector<double> elfs = elfs_values(o, dist, ext);
+  const double alpha = o.d.ms_alpha, beta = o.d.ms_beta;
+  const int min_level = o.d.ms_min_level, max_level = o.d.ms_max_level;
+  const double* Ap = o.dprops.at("Ap").data();
+  const double* hp = o.dprops.at("hp").data();
+  const double* exx = o.dprops.at("vpx_dx").data();
+  const double* eyy = o.dprops.at("vpy_dy").data();
+  const idx_t* lvl = o.iprops.at("level").data();
+  for (idx_t ip = 0; ip < N; ++ip) {
+    const double r_i = std::sqrt(Ap[ip]);
+    const double div = exx[ip] + eyy[ip];
+    if ((elfs[ip] < alpha * r_i) || (div > o.d.ms_stretch_thresh)) {
+      if (lvl[ip] > min_level) act[ip] = SPLIT;
+    } else if (elfs[ip] > beta * r_i && hp[ip] > o.d.ms_hp_min) {
+      if (lvl[ip] < max_level) act[ip] = MERGE_PRIMARY;
+    }
+  }
+  pair_in_cells(o, act, partner, (int)o.d.ms_max_ops, o.d.ms_max_dv * o.d.ms_max_dv, 0.0, 4,
+                2);
+}
+
+// execute_merge_split, merge_split_ops.h:513-717: weights {1, 4, 1, 0};
+// a split puts four children at (+-r/2, +-r/2) around the parent (r =
+// sqrt(Ap), clamped into the domain) with the extensive fields divided by
+// 4; a merge puts the pair's centre of mass with the extensive fields
+// summed, the rest mass-averaged and the primary's label kept.
+void execute_merge_split_elfs(Oracle& o, const std::vector<int>& act,
+                              const std::vector<int>& partner) {
+  const idx_t N = o.np;
+  const int weights[] = {1, 4, 1, 0};
+  std::vector<idx_t> offset(N, 0);
+  idx_t Nnew = 0;
+  for (idx_t i = 0; i < N; ++i) {
+    offset[i] = Nnew;
+    Nnew += weights[act[i]];
+  }
+  std::vector<double> nx(Nnew), ny(Nnew);
+  std::vector<std::string> dpk, ipk;
+  for (auto const& kv : o.dprops) dpk.push_back(kv.first);
+  for (auto const& kv : o.iprops) ipk.push_back(kv.first);
+  const int ndp = int(dpk.size()), nip = int(ipk.size());
+  std::vector<std::vector<double>> ndp_v(ndp, std::vector<double>(Nnew));
+  std::vector<std::vector<idx_t>> nip_v(nip, std::vector<idx_t>(Nnew));
+  std::vector<int> ext(ndp, 0);
+  int iMp = -1, ivpx = -1, ivpy = -1, ixp = -1, iyp = -1, impx = -1, impy = -1, iAp = -1;
+  for (int k = 0; k < ndp; ++k) {
+    const std::string& n = dpk[k];
+    ext[k] = is_extensive(n) ? 1 : 0;
+    if (n == "Mp") iMp = k;
+    else if (n == "vpx") ivpx = k;
+    else if (n == "vpy") ivpy = k;
+    else if (n == "xp") ixp = k;
+    else if (n == "yp") iyp = k;
+    else if (n == "mom_px") impx = k;
+    else if (n == "mom_py") impy = k;
+    else if (n == "Ap") iAp = k;
+  }
+  int ilevel = -1, ilabel = -1;
+  for (int k = 0; k < nip; ++k) {
+    if (ipk[k] == "level") ilevel = k;
+    else if (ipk[k] == "label") ilabel = k;
+  }
+  std::vector<const double*> in_dp(ndp);
+  for (int k = 0; k < ndp; ++k) in_dp[k] = o.dprops.at(dpk[k]).data();
+  std::vector<const idx_t*> in_ip(nip);
+  for (int k = 0; k < nip; ++k) in_ip[k] = o.iprops.at(ipk[k]).data();
+  const double Lx = o.ncols * o.hx, Ly = o.nrows * o.hy;
+  const double eps = 1e-10;
+  auto clampx = [&](double v) { return v < eps ? eps : (v > Lx - eps ? Lx - eps : v); };
+  auto clampy = [&](double v) { return v < eps ? eps : (v > Ly - eps ? Ly - eps : v); };
+  par_for(o, N, [&](idx_t i) {
+    const int a = act[i];
+    const idx_t oo = offset[i];
+    if (a == KEEP) {
+      nx[oo] = o.x[i];
+      ny[oo] = o.y[i];
+      for (int k = 0; k < ndp; ++k) ndp_v[k][oo] = in_dp[k][i];
+      for (int k = 0; k < nip; ++k) nip_v[k][oo] = in_ip[k][i];
+    } else if (a == SPLIT) {
+      const double r_i = std::sqrt(in_dp[iAp][i]);
+      const double off = r_i / 2.0;
+      const double px = o.x[i], py = o.y[i];
+      const double cx[4] = {clampx(px + off), clampx(px + off), clampx(px - off),
+                            clampx(px - off)};
+      const double cy[4] = {clampy(py + off), clampy(py - off), clampy(py + off),
+                            clampy(py - off)};
+      for (int q = 0; q < 4; ++q) {
+        const idx_t t = oo + q;
+        nx[t] = cx[q];
+        ny[t] = cy[q];
+        for (int k = 0; k < ndp; ++k) ndp_v[k][t] = in_dp[k][i] / (ext[k] ? 4.0 : 1.0);
+        for (int k = 0; k < nip; ++k) nip_v[k][t] = in_ip[k][i];
+        if (ixp >= 0) ndp_v[ixp][t] = cx[q];
+        if (iyp >= 0) ndp_v[iyp][t] = cy[q];
+        if (impx >= 0) ndp_v[impx][t] = ndp_v[iMp][t] * ndp_v[ivpx][t];
+        if (impy >= 0) ndp_v[impy][t] = ndp_v[iMp][t] * ndp_v[ivpy][t];
+        if (ilevel >= 0) nip_v[ilevel][t] = in_ip[ilevel][i] - 1;
+        if (ilabel >= 0) nip_v[ilabel][t] = -1;
+      }
+    } else if (a == MERGE_PRIMARY) {
+      const int j = partner[i];
+      const double M1 = in_dp[iMp][i], M2 = in_dp[iMp][j];
+      const double Mt = M1 + M2;
+      nx[oo] = (M1 * o.x[i] + M2 * o.x[j]) / Mt;
+      ny[oo] = (M1 * o.y[i] + M2 * o.y[j]) / Mt;
+      for (int k = 0; k < ndp; ++k)
+        ndp_v[k][oo] = ext[k] ? (in_dp[k][i] + in_dp[k][j])
+                              : (M1 * in_dp[k][i] + M2 * in_dp[k][j]) / Mt;
+      for (int k = 0; k < nip; ++k) nip_v[k][oo] = in_ip[k][i];
+      if (ixp >= 0) ndp_v[ixp][oo] = nx[oo];
+      if (iyp >= 0) ndp_v[iyp][oo] = ny[oo];
+      if (impx >= 0) ndp_v[impx][oo] = ndp_v[iMp][oo] * ndp_v[ivpx][oo];
+      if (impy >= 0) ndp_v[impy][oo] = ndp_v[iMp][oo] * ndp_v[ivpy][oo];
+      if (ilevel >= 0) nip_v[ilevel][oo] = in_ip[ilevel][i] + 1;
+    }
+  });
+  o.x = std::move(nx);
+  o.y = std::move(ny);
+  for (int k = 0; k < ndp; ++k) o.dprops[dpk[k]] = std::move(ndp_v[k]);
+  for (int k = 0; k < nip; ++k) o.iprops[ipk[k]] = std::move(nip_v[k]);
+  o.np = Nnew;
+}
+
+// adaptive_merge_split, merge_split_ops.h:720-755
+void adaptive_merge_split_elfs(Oracle& o) {
+  std::vector<int> act, partner;
+  decide_actions_elfs(o, act, partner);
+  o.ms_counts[2] = o.np;
+  bool any = false;
+  for (int a : act)
+    if (a != KEEP) { any = true; break; }
+  if (any) execute_merge_split_elfs(o, act, partner);
+  o.ms_counts[3] = o.np;
+}
+
+// The merge/split the scenario selects: the gpu_offload one
+// (merge_split_ops_cmes.h) or the ELFS variant (merge_split_ops.h).
+void merge_split_call(Oracle& o, double dt) {
+  if (o.d.ms_variant == 1)
+    adaptive_merge_split_elfs(o);
+  else
+    adaptive_merge_split(o, dt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1030,7 +1320,7 @@ int oracle_run(void* h, int nsteps) {
     if (o.ms_enabled && o.d.ms_call_interval > 0 &&
         o.it % o.d.ms_call_interval == 0 && o.it > 0) {
       init_particle_mesh(o);
-      adaptive_merge_split(o, dt);
+      merge_split_call(o, dt);
     }
     step_body(o, dt);
     o.t += dt;
@@ -1045,7 +1335,7 @@ int oracle_run(void* h, int nsteps) {
 void oracle_merge_split(void* h, double dt) {
   Oracle& o = *static_cast<Oracle*>(h);
   init_particle_mesh(o);
-  adaptive_merge_split(o, dt);
+  merge_split_call(o, dt);
 }
 
 long long oracle_num_particles(void* h) { return static_cast<Oracle*>(h)->np; }

@@ -33,7 +33,8 @@ class oracle_data(C.Structure):
                 ("ms_hp_min", C.c_double), ("ms_max_dv", C.c_double),
                 ("ms_min_level", C.c_int), ("ms_max_level", C.c_int),
                 ("ms_min_particles_per_cell", C.c_int), ("ms_call_interval", C.c_int),
-                ("ms_max_ops", C.c_double), ("ms_pair_dist", C.c_double)]
+                ("ms_max_ops", C.c_double), ("ms_pair_dist", C.c_double),
+                ("ms_variant", C.c_int), ("ms_stretch_thresh", C.c_double)]
 
 
 def build(force: bool = False) -> str:
@@ -99,7 +100,8 @@ def _od(d) -> oracle_data:
                        float(s["ms_max_dv"]), int(s["ms_min_level"]),
                        int(s["ms_max_level"]), int(s["ms_min_particles_per_cell"]),
                        int(s["ms_call_interval"]), float(s["ms_max_ops"]),
-                       float(s.get("ms_pair_dist", 0.0)))
+                       float(s.get("ms_pair_dist", 0.0)), int(s.get("ms_variant", 0)),
+                       float(s.get("ms_stretch_thresh", 1e7)))
 
 
 class Oracle:

@@ -16,6 +16,10 @@ exists).
                            (main/merge_split_ops_cmes.h) on a perturbed state
                            of the bench case (recipe: ms_case()): SHA-256 of
                            every input and output column, the particle counts.
+  ms_elfs_bench1000.json   reference ELFS adaptive_merge_split
+                           (main/merge_split_ops.h) on another perturbed state
+                           of the bench case (recipe: elfs_case()), for each
+                           configuration of ELFS_CONFIGS: the same digests.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -68,6 +72,34 @@ def ms_case():
     return d, state, o.get("x"), o.get("y"), level, o.get("label").astype(np.int32), ms
 
 
+# ELFS ms_config values (main/merge_split_ops.h:17-30): its defaults (a
+# binding max_ops of 50), no cap, and a low divergence trigger
+ELFS_CONFIGS = {
+    "defaults": dict(alpha=2.0, beta=3.0, hp_min=0.05, max_dv=0.01, stretch_thresh=1e7,
+                     min_level=-2, max_level=2, call_interval=10, max_ops=50.0),
+    "uncapped": dict(alpha=2.0, beta=3.0, hp_min=0.05, max_dv=0.01, stretch_thresh=1e7,
+                     min_level=-2, max_level=2, call_interval=10, max_ops=1e9),
+    "stretch": dict(alpha=1.0, beta=2.0, hp_min=0.05, max_dv=0.05, stretch_thresh=0.5,
+                    min_level=-2, max_level=2, call_interval=10, max_ops=1e9),
+}
+
+
+def elfs_case():
+    """A bench state after 30 steps (a flow with a free surface inside the
+    grid) with perturbed areas, velocities and levels."""
+    from oracle.oracle import Oracle
+    d = scenarios.bench_slab(1000, nsteps=100)
+    o = Oracle(d, threads=1)
+    o.run(30)
+    rng = np.random.default_rng(11)
+    n = o.np
+    state = {k: o.get(k) for k in DPROPS}
+    state["Ap"] = state["Ap"] * rng.choice([0.3, 1.0, 1.0, 2.0], size=n)
+    state["vpx"] = state["vpx"] + rng.normal(0, 0.002, n)
+    level = rng.integers(-2, 3, n).astype(np.int32)
+    return d, state, o.get("x"), o.get("y"), level, o.get("label").astype(np.int32)
+
+
 def main():
     if not refrun.build():
         sys.exit("reference build (oracle/_ref) unavailable")
@@ -97,6 +129,17 @@ def main():
         json.dump({"ms": ms, "dt": 1e-3, "np_in": int(x.shape[0]), "np_out": int(res["x"].shape[0]),
                    "in": {k: digest(v) for k, v in inputs.items()},
                    "out": {k: digest(v) for k, v in res.items()}}, f, indent=1, sort_keys=True)
+
+    d, state, x, y, level, label = elfs_case()
+    inputs = dict(state, x=x, y=y, level=level.astype(np.float64), label=label.astype(np.float64))
+    out = {"in": {k: digest(v) for k, v in inputs.items()}, "np_in": int(x.shape[0]),
+           "configs": {}}
+    for name, ms in ELFS_CONFIGS.items():
+        res = refrun.run_merge_split_elfs(grid, ms, state, x, y, level, label)
+        out["configs"][name] = {"ms": ms, "np_out": int(res["x"].shape[0]),
+                                "out": {k: digest(v) for k, v in res.items()}}
+    with open(os.path.join(HERE, "ms_elfs_bench1000.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
     print("written", sorted(os.listdir(HERE)))
 
 

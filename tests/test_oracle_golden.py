@@ -77,3 +77,33 @@ def test_merge_split_bitwise():
     assert counts[0] > 0 and counts[1] > 0  # splits and merges both happened
     for k, dg in gold["out"].items():
         assert digest(o.get(k)) == dg, k
+
+
+@pytest.mark.parametrize("config", ["defaults", "uncapped", "stretch"])
+def test_elfs_merge_split_bitwise(config):
+    """The ELFS variant (main/merge_split_ops.h): exterior flood fill,
+    boundary distance, ELFS values, marks, pairing under the split and merge
+    caps, and the 1 -> 4 split, against the reference's own code."""
+    import sys
+    sys.path.insert(0, G)
+    from make_golden import elfs_case
+    gold = json.load(open(os.path.join(G, "ms_elfs_bench1000.json")))
+    d, state, x, y, level, label = elfs_case()
+    inputs = dict(state, x=x, y=y, level=level.astype(np.float64), label=label.astype(np.float64))
+    for k, v in inputs.items():
+        assert digest(v) == gold["in"][k], f"input recipe changed: {k}"
+    g = gold["configs"][config]
+    for k, v in g["ms"].items():
+        d.scalars["ms_" + k] = v
+    d.scalars["ms_variant"] = 1
+    o = Oracle(d, threads=1)
+    for k, v in state.items():
+        o.set(k, v)
+    o.set("x", x)
+    o.set("y", y)
+    o.set("level", level.astype(np.float64))
+    counts = o.merge_split(1e-3)
+    assert counts[2] == gold["np_in"] and counts[3] == g["np_out"]
+    assert counts[0] > 0 and counts[1] > 0  # splits and merges both happened
+    for k, dg in g["out"].items():
+        assert digest(o.get(k)) == dg, k
