@@ -55,6 +55,8 @@ struct dampm_ctx {
   MsBuffers msb{};
   bool terrain_ok = false, particles_ok = false;
   bool ms_enabled = false;
+  int ms_variant = kMsCmes;       // which merge/split runs (ms_kernels.h)
+  double ms_stretch = 1e7;        // the ELFS variant's divergence trigger
   bool record = false;
   bool record_alloc = false;
   long long it_host = 0;  // passes enqueued since upload (= device it while active)
@@ -70,7 +72,8 @@ struct dampm_ctx {
   bool use_graphs = true;
   static constexpr int kKeyBytes = 2 * sizeof(Particles) + sizeof(Nodes) + sizeof(Geom) +
                                    sizeof(Phys) + sizeof(long long) + sizeof(int) +
-                                   sizeof(dampm_ms_params) + 3 * sizeof(int);
+                                   sizeof(dampm_ms_params) + sizeof(int) + sizeof(double) +
+                                   3 * sizeof(int);
   struct GraphSlot {
     cudaGraphExec_t exec = nullptr;
     int passes = 0, phase = 0;
@@ -294,7 +297,8 @@ int enqueue_front(dampm_ctx* ctx) {
     enqueue_sort(ctx);
     ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc,
                                 ctx->G, ctx->P, ctx->Z, ctx->ms, ctx->S, ctx->cap,
-                                ctx->stream, /*use_step_dt=*/1, 0.0);
+                                ctx->stream, /*use_step_dt=*/1, 0.0, ctx->ms_variant,
+                                ctx->ms_stretch);
     k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
     k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
                                                              ctx->p.slot, ctx->S);
@@ -403,6 +407,8 @@ void graph_key_of(const dampm_ctx* ctx, int passes, int phase, unsigned char* k)
   put(&ctx->cap, sizeof(long long));
   put(&ctx->p2g_grid, sizeof(int));
   put(&ctx->ms, sizeof(dampm_ms_params));
+  put(&ctx->ms_variant, sizeof(int));
+  put(&ctx->ms_stretch, sizeof(double));
   const int cyc[3] = {ms_cadence(ctx) ? 1 : 0, passes, phase};
   put(cyc, sizeof(cyc));
 }
@@ -816,6 +822,21 @@ int dampm_enable_merge_split(dampm_ctx* ctx, int enable) {
   return DAMPM_OK;
 }
 
+int dampm_set_ms_variant(dampm_ctx* ctx, int variant, double stretch_thresh) {
+  if (!ctx) return DAMPM_ERR_ARG;
+  if (variant != DAMPM_MS_CMES && variant != DAMPM_MS_ELFS)
+    return fail(ctx, DAMPM_ERR_ARG, "unknown merge/split variant");
+  if (variant == DAMPM_MS_ELFS) {
+    const int rc = ms_alloc_elfs(ctx->msb, ctx->nc, [&](void** q, size_t bytes) {
+      return dalloc(ctx, reinterpret_cast<unsigned char**>(q), bytes);
+    });
+    if (rc) return rc;
+  }
+  ctx->ms_variant = variant;
+  ctx->ms_stretch = stretch_thresh;
+  return DAMPM_OK;
+}
+
 int dampm_record_outputs(dampm_ctx* ctx, int enable) {
   if (!ctx) return DAMPM_ERR_ARG;
   if (ctx->slab && enable) return fail(ctx, DAMPM_ERR_STATE, "slab mode records no outputs");
@@ -933,7 +954,8 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
   enqueue_unsort(ctx);
   enqueue_sort(ctx);
   ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
-             ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt);
+             ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt,
+             ctx->ms_variant, ctx->ms_stretch);
   k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
   k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
                                                            ctx->p.slot, ctx->S);

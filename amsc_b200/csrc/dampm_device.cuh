@@ -58,6 +58,7 @@ struct Scalars {
 constexpr int kStatusCapacity = 1;
 constexpr int kStatusNonFinite = 2;
 constexpr int kStatusSlab = 4;  // a particle arrived outside the slab's columns
+constexpr int kStatusMsLimit = 8;  // a merge/split loop ran past its bound
 
 // --- order-preserving double <-> u64 map for atomicMax reductions --------
 __device__ __forceinline__ unsigned long long ordered_key(double v) {

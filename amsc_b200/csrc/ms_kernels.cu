@@ -14,6 +14,19 @@
 //                 (:268-274)
 //   emit        : split 1->2 along the principal stretch, merge 2->1 at the
 //                 centre of mass (:321-418); copy back; np := Nnew
+//
+// The ELFS variant (main/merge_split_ops.h) replaces the marks and the emit:
+//   exterior    : empty cells joined by a union-find over 4-neighbours; the
+//                 sets that reach the grid edge are the exterior (:86-164)
+//   distance    : hops through cells with particles from the surface cells
+//                 (exterior left or right), one block, level by level
+//                 (:170-260)
+//   mark        : ELFS value per particle (:266-343), split near the
+//                 surface or on divergence, merge far from it (:385-402)
+//   pairing     : as above with a split counting 4 and at least 2 per cell
+//                 (:406-497)
+//   emit        : split 1->4 at (+-r/2, +-r/2), merge 2->1 keeping the
+//                 primary's label (:513-717)
 #include <cfloat>
 
 #include "dampm_device.cuh"
@@ -31,6 +44,8 @@ struct MsCfg {
   double pair_gate2;  // squared pair-distance limit; 0: none
   double dt_host;
   int use_step_dt;
+  int split_w;        // particles a split leaves (2; ELFS 4)
+  double stretch;     // ELFS divergence trigger
 };
 
 __global__ void k_ms_materialize(Particles p, Phys P, const Scalars* S,
@@ -126,7 +141,7 @@ __global__ void k_ms_split_cap(const int* perm, const int* rank, int* act,
 __device__ long long pair_cell(int b, int e, const int* perm, int* act,
                                int* partner, int* paired, const Particles& p,
                                double max_dv2, double gate2, int min_ppc,
-                               long long budget) {
+                               int split_w, long long budget) {
   long long n = 0;
   for (int j = b; j < e; ++j) paired[j] = 0;
   for (int ji = b; ji < e && n < budget; ++ji) {
@@ -166,7 +181,7 @@ __device__ long long pair_cell(int b, int e, const int* perm, int* act,
   int projected = 0;
   for (int j = b; j < e; ++j) {
     const int a = act[perm[j]];
-    projected += (a == KEEP) ? 1 : (a == SPLIT) ? 2 : (a == MERGE_PRIMARY) ? 1 : 0;
+    projected += (a == KEEP) ? 1 : (a == SPLIT) ? split_w : (a == MERGE_PRIMARY) ? 1 : 0;
   }
   while (projected < min_ppc) {
     bool undone = false;
@@ -226,7 +241,7 @@ __global__ void k_ms_pair_parallel(const int* start, int ncells,
     const int b = start[cell], e = start[cell + 1];
     if (e - b < 1) continue;
     local += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.pair_gate2,
-                       c.min_ppc, 0x7fffffffffffffffLL);
+                       c.min_ppc, c.split_w, 0x7fffffffffffffffLL);
   }
   if (local) atomicAdd((unsigned long long*)&S->ms_counts[1], (unsigned long long)local);
 }
@@ -244,12 +259,12 @@ __global__ void k_ms_pair_serial(const int* start, int ncells, const int* perm,
     const int b = start[cell], e = start[cell + 1];
     if (e - b < 1) continue;
     n_merge += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.pair_gate2,
-                         c.min_ppc, c.max_ops - n_merge);
+                         c.min_ppc, c.split_w, c.max_ops - n_merge);
   }
   S->ms_counts[1] = n_merge;
 }
 
-__global__ void k_ms_weights(const int* act, int* w, int* partner, int cap,
+__global__ void k_ms_weights(const int* act, int* w, int* partner, int cap, int split_w,
                              const Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
@@ -258,7 +273,7 @@ __global__ void k_ms_weights(const int* act, int* w, int* partner, int cap,
     int v = 0;
     if (i < np) {
       const int a = act[i];
-      v = (a == KEEP) ? 1 : (a == SPLIT) ? 2 : (a == MERGE_PRIMARY) ? 1 : 0;
+      v = (a == KEEP) ? 1 : (a == SPLIT) ? split_w : (a == MERGE_PRIMARY) ? 1 : 0;
     }
     w[i] = v;
   }
@@ -402,6 +417,273 @@ __global__ void k_ms_finish(const int* offs, long long cap, Scalars* S) {
   S->fresh = 1;
 }
 
+// ---- ELFS variant (main/merge_split_ops.h) -------------------------------
+
+// Root of empty cell v in the union-find forest uf (every link points to a
+// smaller cell id, roots to themselves), halving the path on the way.
+// Reads go through L2 (other blocks link concurrently); a stale read only
+// returns an older ancestor, which the callers' compare-and-swap corrects.
+__device__ __forceinline__ int uf_find(int* uf, int v) {
+  volatile int* vu = uf;
+  int par = vu[v];
+  if (par != v) {
+    int prev = v, next;
+    while (par > (next = vu[par])) {
+      vu[prev] = next;
+      prev = par;
+      par = next;
+    }
+  }
+  return par;
+}
+
+// Joins the sets of empty cells a and b: the larger root is linked to the
+// smaller by compare-and-swap; a failed swap returns the root's new
+// (smaller) parent and the loop goes on with it.  Every retry lowers one of
+// the two ids, so the loop ends within `limit` rounds (twice the cell
+// count); past it the status word takes kStatusMsLimit.
+__device__ __forceinline__ void uf_unite(int* uf, int a, int b, int limit, Scalars* S) {
+  int ra = uf_find(uf, a), rb = uf_find(uf, b);
+  for (int guard = 0; ra != rb; ++guard) {
+    if (guard > limit) {
+      atomicOr(&S->status, kStatusMsLimit);
+      return;
+    }
+    if (ra < rb) {
+      const int old = atomicCAS(&uf[rb], rb, ra);
+      if (old == rb) return;
+      rb = old;
+    } else {
+      const int old = atomicCAS(&uf[ra], ra, rb);
+      if (old == ra) return;
+      ra = old;
+    }
+  }
+}
+
+// Per cell: empty cells start as their own set, cells with particles are
+// out of the forest (-1); no root reaches the edge yet; no hop count.
+__global__ void k_elfs_cells(const int* __restrict__ start, int ncells, int* uf, int* eroot,
+                             int* hops, int* bqn, const Scalars* S) {
+  if (!S->active) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) bqn[0] = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += gridDim.x * blockDim.x) {
+    uf[c] = start[c + 1] > start[c] ? -1 : c;
+    eroot[c] = 0;
+    hops[c] = -1;
+  }
+}
+
+// Each empty cell joins its lower and right neighbours when they are empty.
+__global__ void k_elfs_union(int* uf, int nrows, int ncols, Scalars* S) {
+  if (!S->active) return;
+  const int ncells = nrows * ncols;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += gridDim.x * blockDim.x) {
+    if (uf[c] < 0) continue;
+    const int r = c % nrows, col = c / nrows;
+    if (r + 1 < nrows && uf[c + 1] >= 0) uf_unite(uf, c, c + 1, 2 * ncells + 2, S);
+    if (col + 1 < ncols && uf[c + nrows] >= 0) uf_unite(uf, c, c + nrows, 2 * ncells + 2, S);
+  }
+}
+
+// Every empty cell points to its root; the roots of empty edge cells are
+// marked (mark_exterior_cells' seeds, :103-121).
+__global__ void k_elfs_roots(int* uf, int* eroot, int nrows, int ncols, const Scalars* S) {
+  if (!S->active) return;
+  const int ncells = nrows * ncols;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += gridDim.x * blockDim.x) {
+    if (uf[c] < 0) continue;
+    const int root = uf_find(uf, c);
+    uf[c] = root;
+    const int r = c % nrows, col = c / nrows;
+    if (r == 0 || r == nrows - 1 || col == 0 || col == ncols - 1) eroot[root] = 1;
+  }
+}
+
+// exterior cell: empty, in a set that reaches the edge (uf flattened)
+__device__ __forceinline__ bool elfs_exterior(const int* uf, const int* eroot, int q) {
+  const int r = uf[q];
+  return r >= 0 && eroot[r] != 0;
+}
+
+// The search's first level: cells with particles off the grid edge with an
+// exterior cell left or right of them (compute_boundary_distance, :194-225).
+__global__ void k_elfs_seeds(const int* uf, const int* eroot, int* hops, int* bq, int* bqn,
+                             int nrows, int ncols, const Scalars* S) {
+  if (!S->active) return;
+  const int ncells = nrows * ncols;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += gridDim.x * blockDim.x) {
+    if (uf[c] >= 0) continue;  // empty
+    const int r = c % nrows, col = c / nrows;
+    if (r == 0 || r == nrows - 1 || col == 0 || col == ncols - 1) continue;
+    if (elfs_exterior(uf, eroot, c - nrows) || elfs_exterior(uf, eroot, c + nrows)) {
+      hops[c] = 0;
+      bq[atomicAdd(bqn, 1)] = c;
+    }
+  }
+}
+
+// Breadth-first search by levels through the cells with particles (:228-
+// 259), in one block: each level's frontier claims its unreached
+// neighbours by compare-and-swap (hop count level + 1) and lists them for
+// the next level.  A cell is listed once, so there are at most ncells
+// levels; the hop counts do not depend on the order inside a level.
+__global__ void __launch_bounds__(1024)
+    k_elfs_bfs(const int* uf, int* hops, int* bq, const int* bqn, int nrows, int ncols,
+               const Scalars* S) {
+  if (!S->active) return;
+  const int ncells = nrows * ncols;
+  __shared__ int nnext;
+  int* src = bq;
+  int* dst = bq + ncells;
+  int n = *bqn;
+  for (int level = 0; n > 0 && level < ncells; ++level) {
+    if (threadIdx.x == 0) nnext = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int k = src[i];
+      const int r = k % nrows, col = k / nrows;
+      const int nb[4] = {r > 0 ? k - 1 : -1, r + 1 < nrows ? k + 1 : -1,
+                         col > 0 ? k - nrows : -1, col + 1 < ncols ? k + nrows : -1};
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int q = nb[t];
+        if (q < 0 || uf[q] >= 0) continue;  // outside, or empty
+        if (atomicCAS(&hops[q], -1, level + 1) == -1) dst[atomicAdd(&nnext, 1)] = q;
+      }
+    }
+    __syncthreads();
+    n = nnext;
+    int* t = src;
+    src = dst;
+    dst = t;
+    __syncthreads();
+  }
+}
+
+// decide_actions' marks (:385-402) with compute_elfs (:266-343): the
+// cell's distance (hops * min(hx, hy), DBL_MAX where no hop reached),
+// refined within max(hx, hy) of the surface by the distance to the nearest
+// exterior cell box among the two cells left and right in the row.
+__global__ void k_elfs_mark(Particles p, const int* __restrict__ hops, const int* uf,
+                            const int* eroot, Geom G, MsCfg c, int* act, int cap,
+                            Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  const int nrows = G.nrows, ncols = G.ncols;
+  const double hx = G.hx, hy = G.hy;
+  const double h = (hx < hy) ? hx : hy;
+  const double refine = (hx < hy) ? hy : hx;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap;
+       i += gridDim.x * blockDim.x) {
+    int a = KEEP;
+    if (i < np) {
+      const int cell = p.key[i];
+      const int hc = hops[cell];
+      const double base = hc >= 0 ? hc * h : DBL_MAX;
+      double e = base;
+      if (!(base > refine)) {
+        const double px = p.x[i], py = p.y[i];
+        const int r = cell % nrows, c0 = cell / nrows;
+        for (int dc = -2; dc <= 2; ++dc) {
+          const int cc = c0 + dc;
+          if (cc < 0 || cc >= ncols) continue;
+          if (!elfs_exterior(uf, eroot, r + nrows * cc)) continue;
+          const double cx_lo = cc * hx, cx_hi = (cc + 1) * hx;
+          const double cy_lo = r * hy, cy_hi = (r + 1) * hy;
+          const double qx = px < cx_lo ? cx_lo : (px > cx_hi ? cx_hi : px);
+          const double qy = py < cy_lo ? cy_lo : (py > cy_hi ? cy_hi : py);
+          const double dx = px - qx, dy = py - qy;
+          const double d = sqrt(dx * dx + dy * dy);
+          if (d < e) e = d;
+        }
+      }
+      const double r_i = sqrt(p.Ap[i]);
+      const double div = p.vpx_dx[i] + p.vpy_dy[i];
+      const int lvl = p.level[i];
+      if ((e < c.alpha * r_i) || (div > c.stretch)) {
+        if (lvl > c.min_level) a = SPLIT;
+      } else if (e > c.beta * r_i && p.hp[i] > c.hp_min) {
+        if (lvl < c.max_level) a = MERGE_PRIMARY;
+      }
+    }
+    act[i] = a;
+  }
+}
+
+// execute_merge_split (:513-717) for the field slots of k_ms_emit: a split
+// leaves four children at (+-r/2, +-r/2) around the parent (r = sqrt(Ap),
+// clamped into the domain) with the extensive fields divided by 4 and the
+// momentum rebuilt; a merge leaves the centre of mass with the extensive
+// fields summed, the rest mass-averaged and the primary's label.
+__global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
+                               const int* partner, const int* offs, Geom G,
+                               long long cap, Scalars* S) {
+  if (!S->active) return;
+  const int np = S->np;
+  const int nnew = offs[cap];
+  if (nnew > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
+    return;
+  }
+  const double eps = 1e-10;
+  const double Lx = G.ncols * G.hx, Ly = G.nrows * G.hy;
+  auto clampx = [&](double v) { return v < eps ? eps : (v > Lx - eps ? Lx - eps : v); };
+  auto clampy = [&](double v) { return v < eps ? eps : (v > Ly - eps ? Ly - eps : v); };
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    const int a = act[i];
+    const int o = offs[i];
+    if (a == KEEP) {
+#pragma unroll
+      for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
+      out.label[o] = in.label[i];
+      out.level[o] = in.level[i];
+    } else if (a == SPLIT) {
+      const double off = sqrt(in.f[11][i]) / 2.0;
+      const double px = in.f[0][i], py = in.f[1][i];
+      const double xs[4] = {clampx(px + off), clampx(px + off), clampx(px - off),
+                            clampx(px - off)};
+      const double ys[4] = {clampy(py + off), clampy(py - off), clampy(py + off),
+                            clampy(py - off)};
+      const int level = in.level[i];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int t = o + q;
+#pragma unroll
+        for (int k = 0; k < kMsFields; ++k)
+          out.f[k][t] = in.f[k][i] / (extensive(k) ? 4.0 : 1.0);
+        out.f[0][t] = xs[q];
+        out.f[1][t] = ys[q];
+        out.f[20][t] = xs[q];
+        out.f[21][t] = ys[q];
+        out.f[12][t] = out.f[8][t] * out.f[2][t];
+        out.f[13][t] = out.f[8][t] * out.f[3][t];
+        out.level[t] = level - 1;
+        out.label[t] = -1;
+      }
+    } else if (a == MERGE_PRIMARY) {
+      const int j = partner[i];
+      const double M1 = in.f[8][i], M2 = in.f[8][j];
+      const double Mt = M1 + M2;
+#pragma unroll
+      for (int k = 0; k < kMsFields; ++k)
+        out.f[k][o] = extensive(k) ? (in.f[k][i] + in.f[k][j])
+                                   : (M1 * in.f[k][i] + M2 * in.f[k][j]) / Mt;
+      out.f[20][o] = out.f[0][o];
+      out.f[21][o] = out.f[1][o];
+      out.f[12][o] = out.f[8][o] * out.f[2][o];
+      out.f[13][o] = out.f[8][o] * out.f[3][o];
+      out.level[o] = in.level[i] + 1;
+      out.label[o] = in.label[i];
+    }
+  }
+}
+
 int grid_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -422,7 +704,9 @@ int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
 int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
                int ncells, Geom G, Phys P, const double* Z,
                const dampm_ms_params& cfg, Scalars* S, long long cap,
-               cudaStream_t st, int use_step_dt, double dt) {
+               cudaStream_t st, int use_step_dt, double dt, int variant,
+               double stretch_thresh) {
+  const bool elfs = variant == kMsElfs;
   MsCfg c{};
   c.alpha = cfg.alpha;
   c.beta = cfg.beta;
@@ -441,13 +725,31 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   }
   c.dt_host = dt;
   c.use_step_dt = use_step_dt;
+  c.split_w = 2;
+  c.stretch = stretch_thresh;
+  if (elfs) {  // main/merge_split_ops.h:406-497: a split counts 4, at least 2 per cell
+    c.split_w = 4;
+    c.min_ppc = 2;
+    c.pair_gate2 = 0.0;
+  }
   int n = 0;
   const int gp = grid_for(cap, 256);
   const int ic = int(cap);
   k_ms_reset_counts<<<1, 1, 0, st>>>(S);
   k_ms_materialize<<<gp, 256, 0, st>>>(p, P, S, m.mx, m.my);
   n += 2;
-  k_ms_mark<<<gp, 256, 0, st>>>(p, G, c, m.act, ic, S);
+  if (elfs) {
+    const int gc = grid_for(ncells, 256);
+    k_elfs_cells<<<gc, 256, 0, st>>>(start, ncells, m.uf, m.eroot, m.hops, m.bqn, S);
+    k_elfs_union<<<gc, 256, 0, st>>>(m.uf, G.nrows, G.ncols, S);
+    k_elfs_roots<<<gc, 256, 0, st>>>(m.uf, m.eroot, G.nrows, G.ncols, S);
+    k_elfs_seeds<<<gc, 256, 0, st>>>(m.uf, m.eroot, m.hops, m.bq, m.bqn, G.nrows, G.ncols, S);
+    k_elfs_bfs<<<1, 1024, 0, st>>>(m.uf, m.hops, m.bq, m.bqn, G.nrows, G.ncols, S);
+    k_elfs_mark<<<gp, 256, 0, st>>>(p, m.hops, m.uf, m.eroot, G, c, m.act, ic, S);
+    n += 5;
+  } else {
+    k_ms_mark<<<gp, 256, 0, st>>>(p, G, c, m.act, ic, S);
+  }
   k_ms_init_partner<<<gp, 256, 0, st>>>(m.partner, ic, S);
   k_ms_split_flags<<<gp, 256, 0, st>>>(perm, m.act, m.flag, ic, S);
   n += 3;
@@ -458,7 +760,7 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
       start, ncells, perm, m.act, m.partner, m.paired, p, c, S);
   k_ms_pair_serial<<<1, 1, 0, st>>>(start, ncells, perm, m.act, m.partner,
                                     m.paired, p, c, S);
-  k_ms_weights<<<gp, 256, 0, st>>>(m.act, m.w, m.partner, ic, S);
+  k_ms_weights<<<gp, 256, 0, st>>>(m.act, m.w, m.partner, ic, c.split_w, S);
   n += 5;
   n += scan_enqueue(m.w, m.offs, ic, m.tile_sum, m.ntiles, S, st);
   Fields in{}, out{};
@@ -474,7 +776,10 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   in.level = p.level;
   out.label = m.slabel;
   out.level = m.slevel;
-  k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
+  if (elfs)
+    k_ms_emit_elfs<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
+  else
+    k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
   k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
   k_ms_pair_mom<<<gp, 256, 0, st>>>(m.mx, m.my, p, S);

@@ -20,6 +20,12 @@ struct MsBuffers {
   double* sd[kMsFields] = {};
   double *mx = nullptr, *my = nullptr;  // the momentum pair as two fields
   int *slabel = nullptr, *slevel = nullptr;
+  // the ELFS variant's cell arrays (allocated when it is selected): the
+  // empty cells' union-find forest (-1: a cell with particles), the roots
+  // that reach the grid edge, the hop counts from the free surface, the
+  // two frontier queues of the search and its counter
+  int *uf = nullptr, *eroot = nullptr, *hops = nullptr, *bq = nullptr, *bqn = nullptr;
+  int elfs_cells = 0;
 };
 
 template <class Alloc>
@@ -47,12 +53,33 @@ int ms_alloc(MsBuffers& m, long long cap, int /*ncells*/, Alloc alloc) {
   return 0;
 }
 
+template <class Alloc>
+int ms_alloc_elfs(MsBuffers& m, int ncells, Alloc alloc) {
+  if (m.elfs_cells >= ncells) return 0;
+  int** arr[] = {&m.uf, &m.eroot, &m.hops};
+  for (int** q : arr) {
+    int rc = alloc((void**)q, sizeof(int) * size_t(ncells + 1));
+    if (rc) return rc;
+  }
+  int rc = alloc((void**)&m.bq, sizeof(int) * 2 * size_t(ncells + 1));
+  if (rc) return rc;
+  rc = alloc((void**)&m.bqn, sizeof(int) * 4);
+  if (rc) return rc;
+  m.elfs_cells = ncells;
+  return 0;
+}
+
+// The merge/split a context runs: the one gpu_offload calls
+// (main/merge_split_ops_cmes.h) or the ELFS variant (main/merge_split_ops.h).
+enum MsVariant { kMsCmes = DAMPM_MS_CMES, kMsElfs = DAMPM_MS_ELFS };
+
 // Enqueues one adaptive_merge_split on the current binning (start/perm must
 // describe the current positions).  dt comes from the step's device scalar
 // when use_step_dt, else `dt`.  Returns the number of kernel launches.
 int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
                int ncells, Geom G, Phys P, const double* Z,
                const dampm_ms_params& cfg, Scalars* S, long long cap,
-               cudaStream_t stream, int use_step_dt, double dt);
+               cudaStream_t stream, int use_step_dt, double dt, int variant = kMsCmes,
+               double stretch_thresh = 1e7);
 
 }  // namespace dampm

@@ -75,6 +75,7 @@ def _declare(lib):
         "dampm_status": (C.c_int, [P, C.POINTER(C.c_int), _DP, _DP, C.POINTER(C.c_longlong)]),
         "dampm_enable_merge_split": (C.c_int, [P, C.c_int]),
         "dampm_merge_split": (C.c_int, [P, C.c_double, C.POINTER(C.c_longlong)]),
+        "dampm_set_ms_variant": (C.c_int, [P, C.c_int, C.c_double]),
         "dampm_download": (C.c_int, [P, C.c_char_p, _DP]),
         "dampm_download_nodal": (C.c_int, [P, C.c_char_p, _DP]),
         "dampm_record_outputs": (C.c_int, [P, C.c_int]),
@@ -203,6 +204,11 @@ class Solver:
         self.h = h
         self._keep = [g, p, m]
         self._check(self.lib.dampm_enable_merge_split(self.h, 1 if merge_split else 0))
+        # the ELFS merge/split variant (DATA key ms_variant = 1)
+        if int(d.scalars.get("ms_variant", 0)) != 0:
+            self._check(self.lib.dampm_set_ms_variant(
+                self.h, int(d.scalars["ms_variant"]),
+                float(d.scalars.get("ms_stretch_thresh", 1e7))))
         self._check(self.lib.dampm_record_outputs(self.h, 1 if record else 0))
         A = d.arrays
         self._check(self.lib.dampm_upload_terrain(self.h, _ptr(_f64(A["Z"])),

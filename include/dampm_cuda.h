@@ -154,9 +154,27 @@ int dampm_status(dampm_ctx* ctx, int* it, double* t, double* dt_last,
 int dampm_enable_merge_split(dampm_ctx* ctx, int enable);
 
 /* One standalone adaptive_merge_split(dt) on the current state
- * (main/merge_split_ops_cmes.h:432-447).  counts (may be NULL) receives
- * {splits, merges, np_before, np_after}. */
+ * (main/merge_split_ops_cmes.h:432-447; with DAMPM_MS_ELFS selected,
+ * main/merge_split_ops.h:720-755, which takes no dt).  counts (may be NULL)
+ * receives {splits, merges, np_before, np_after}. */
 int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]);
+
+/* Which merge/split the context runs, at the cadence and standalone:
+ *   DAMPM_MS_CMES  the one gpu_offload calls, adaptive_merge_split of
+ *                  main/merge_split_ops_cmes.h (the default);
+ *   DAMPM_MS_ELFS  the ELFS variant, adaptive_merge_split of
+ *                  main/merge_split_ops.h:720-755 (the reference builds it
+ *                  but calls it nowhere): split where the particle is
+ *                  within alpha*sqrt(Ap) of the free surface or its velocity
+ *                  divergence exceeds stretch_thresh, merge pairs beyond
+ *                  beta*sqrt(Ap); splits are 1 -> 4.
+ * The ELFS variant reads alpha, beta, hp_min, max_dv, min_level, max_level,
+ * max_ops and call_interval of dampm_ms_params as the fields of the same
+ * names of its ms_config (main/merge_split_ops.h:17-30) and ignores the
+ * others; stretch_thresh is its ms_config::stretch_thresh (default 1e7).
+ * Selecting it allocates four ints per cell of device memory. */
+enum dampm_ms_variant { DAMPM_MS_CMES = 0, DAMPM_MS_ELFS = 1 };
+int dampm_set_ms_variant(dampm_ctx* ctx, int variant, double stretch_thresh);
 
 /* Copies one particle field to host memory in reference index order.
  * Names: x, y, Mp, Vp, H, hp, vpx, vpy, F_11, F_12, F_21, F_22, Ap, mom_px,
