@@ -8,8 +8,9 @@
 //   pairing     : one thread per cell, greedy nearest co-moving partner in
 //                 index order, then undo merges while the cell would drop
 //                 below min_particles_per_cell (:186-248).  When the global
-//                 merge budget could bind, one thread walks all cells in
-//                 order instead (exact n_merge semantics).
+//                 merge budget could bind, one thread walks the cells holding
+//                 a candidate in order instead (exact n_merge semantics),
+//                 until the budget is spent.
 //   scan        : exclusive scan of the weights {1,2,1,0} in index order
 //                 (:268-274)
 //   emit        : split 1->2 along the principal stretch, merge 2->1 at the
@@ -246,22 +247,64 @@ __global__ void k_ms_pair_parallel(const int* start, int ncells,
   if (local) atomicAdd((unsigned long long*)&S->ms_counts[1], (unsigned long long)local);
 }
 
-// one thread, cells in order, exact global n_merge budget
-__global__ void k_ms_pair_serial(const int* start, int ncells, const int* perm,
-                                 int* act, int* partner, int* paired,
-                                 Particles p, MsCfg c, Scalars* S) {
+// When the merge budget may bind (candidates / 2 >= max_ops) the cells are
+// paired in order by one thread, which walks only the cells holding a
+// candidate: flag[j] marks sorted position j holding one, an exclusive scan
+// gives rank, and list[rank[j]] = j lists them in (cell, index) order.
+__device__ __forceinline__ bool budget_may_bind(const Scalars* S, const MsCfg& c) {
+  return S->ms_counts[2] / 2 >= c.max_ops;
+}
+
+__global__ void k_ms_cand_flags(const int* perm, const int* act, int* flag, int cap,
+                                MsCfg c, const Scalars* S) {
   if (!S->active) return;
-  if (S->ms_counts[2] / 2 < c.max_ops) return;
+  const bool bind = budget_may_bind(S, c);
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cap;
+       j += gridDim.x * blockDim.x)
+    flag[j] = (bind && j < np && act[perm[j]] == MERGE_PRIMARY) ? 1 : 0;
+}
+
+__global__ void k_ms_cand_list(const int* rank, int* list, int cap, MsCfg c,
+                               const Scalars* S) {
+  if (!S->active || !budget_may_bind(S, c)) return;
+  const int np = S->np;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np;
+       j += gridDim.x * blockDim.x)
+    if (rank[j + 1] > rank[j]) list[rank[j]] = j;
+}
+
+// One thread, the candidates' cells in order, the exact global n_merge
+// budget.  A cell without a candidate pairs nothing and undoes nothing, so
+// skipping it changes nothing; once the budget is spent no later cell can
+// merge, and k_ms_demote turns their candidates back to KEEP (as the
+// reference's per-cell loop does, :186-201).
+__global__ void k_ms_pair_serial(const int* start, const int* perm, const int* list,
+                                 const int* rank, int cap, int* act, int* partner,
+                                 int* paired, Particles p, MsCfg c, Scalars* S) {
+  if (!S->active || !budget_may_bind(S, c)) return;
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double max_dv2 = c.max_dv * c.max_dv;
+  const int ncand = rank[cap];
   long long n_merge = 0;
-  for (int cell = 0; cell < ncells; ++cell) {
+  int q = 0;
+  while (q < ncand && n_merge < c.max_ops) {
+    const int cell = p.key[perm[list[q]]];
     const int b = start[cell], e = start[cell + 1];
-    if (e - b < 1) continue;
     n_merge += pair_cell(b, e, perm, act, partner, paired, p, max_dv2, c.pair_gate2,
                          c.min_ppc, c.split_w, c.max_ops - n_merge);
+    while (q < ncand && list[q] < e) ++q;  // the cell's other candidates
   }
   S->ms_counts[1] = n_merge;
+}
+
+// candidates of the cells after the budget was spent: KEEP
+__global__ void k_ms_demote(int* act, const int* partner, MsCfg c, const Scalars* S) {
+  if (!S->active || !budget_may_bind(S, c)) return;
+  const int np = S->np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x)
+    if (act[i] == MERGE_PRIMARY && partner[i] < 0) act[i] = KEEP;
 }
 
 __global__ void k_ms_weights(const int* act, int* w, int* partner, int cap, int split_w,
@@ -758,8 +801,13 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
   k_ms_count_cand<<<gp, 256, 0, st>>>(m.act, ic, S);
   k_ms_pair_parallel<<<grid_for(ncells, 128), 128, 0, st>>>(
       start, ncells, perm, m.act, m.partner, m.paired, p, c, S);
-  k_ms_pair_serial<<<1, 1, 0, st>>>(start, ncells, perm, m.act, m.partner,
+  k_ms_cand_flags<<<gp, 256, 0, st>>>(perm, m.act, m.flag, ic, c, S);
+  n += 1 + scan_enqueue(m.flag, m.rank, ic, m.tile_sum, m.ntiles, S, st);
+  k_ms_cand_list<<<gp, 256, 0, st>>>(m.rank, m.w, ic, c, S);
+  k_ms_pair_serial<<<1, 1, 0, st>>>(start, perm, m.w, m.rank, ic, m.act, m.partner,
                                     m.paired, p, c, S);
+  k_ms_demote<<<gp, 256, 0, st>>>(m.act, m.partner, c, S);
+  n += 2;
   k_ms_weights<<<gp, 256, 0, st>>>(m.act, m.w, m.partner, ic, c.split_w, S);
   n += 5;
   n += scan_enqueue(m.w, m.offs, ic, m.tile_sum, m.ntiles, S, st);
