@@ -336,12 +336,16 @@ def run_ensemble(args, world, rank, local):
     clocks = sampler.stop()
     el_ms = _allreduce(e0.elapsed_time(e1), world)
     launches = b.usage()["launches"] - l0
-    b.sync()
-    done = sum(1 for h in hs if not b.query(h)["running"])
-    outs = [b.download(h, "hp") for h in hs]
+    # a scenario whose state goes non-finite is stopped by its status word
+    # (fixed dt = 0.02 s is above the CFL limit of some members); it counts as
+    # failed, not as a finished scenario
+    st = b.states()
+    failed = [k for k, h in enumerate(hs) if st[h]["failed"]]
+    done = sum(1 for h in hs if not st[h]["running"] and not st[h]["failed"])
+    outs = [b.download(h, "hp") for h in hs if not st[h]["failed"]]
     e2e_s = _allreduce(time.perf_counter() - t0, world)
     b.close()
-    total = _allreduce(float(n), world, "sum")
+    total = _allreduce(float(done), world, "sum")
     value = total / (el_ms * 1e-3)
     # the plain path: the same scenarios one at a time through dampm_ctx
     m = min(args.plain_sample, n)
@@ -380,6 +384,8 @@ def run_ensemble(args, world, rank, local):
                                      f"{K} passes each, device time"},
             "batch_vs_plain": (value / world) / plain_value if plain_value else None,
             "finished": done,
+            "failed": {"count": len(failed), "seeds": [seeds[k] for k in failed][:16],
+                       "note": "stopped by the status word (non-finite state); not counted"},
             "autotune": tuned,
             "roofline": {"bound": "hbm", "kernel": "whole pass", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",

@@ -9,7 +9,7 @@
 * C4 ensemble members of different sides inside one batch, and a C5 request
   served in a mix, each compared directly with the oracle run alone.
 
-Tolerance 0 (bitwise) throughout; the contract's bar is 1e-10 relative.
+Tolerance 0 (bitwise) throughout; the parity bar is 1e-10 relative.
 """
 import os
 

@@ -1,10 +1,10 @@
 """GPU vs CPU oracle: the FP64 step is bitwise identical to the restated
 reference (main/optim_par.cpp) on the same DATA.
 
-The north-star bar is 1e-10 relative on particle fields; the FP64 path is
-built so that every operation rounds as the reference's C++ does, so these
-tests ask for equality (tolerance 0) and report the largest difference when
-it fails."""
+The parity bar for the FP64 path is 1e-10 relative on particle fields; the
+path is built so that every operation rounds as the reference's C++ does, so
+these tests ask for equality (tolerance 0) and report the largest difference
+when it fails."""
 import numpy as np
 import pytest
 
@@ -14,7 +14,7 @@ from oracle.oracle import Oracle
 
 STATE = ("x", "y", "vpx", "vpy", "hp", "F_11", "F_12", "F_21", "F_22", "Mp", "Vp", "H")
 DERIVED = ("Ap", "mom_px", "mom_py", "Fb_x", "Fb_y")
-REL_TOL = 0.0  # bitwise; the contract tolerance is 1e-10 relative
+REL_TOL = 0.0  # bitwise; the parity bar is 1e-10 relative
 
 
 def _compare(gpu, ora, names, tol=REL_TOL):
