@@ -41,6 +41,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
            "-Xcompiler", "-fPIC", "-shared", "-o", LIB + ".tmp"]
+    # build options of the kernels (dampm_kernels.h, dampm_device.cuh), e.g.
+    # DAMPM_NVCC_DEFS="-DDAMPM_P2G_CAP=384"
+    cmd += os.environ.get("DAMPM_NVCC_DEFS", "").split()
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
