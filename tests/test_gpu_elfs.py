@@ -74,3 +74,12 @@ def test_elfs_cadence_mudflow(cuda_lib):
         assert st["it"] == o.it and st["np"] == o.np
         assert o.np != d.np
         compare(s, o, FIELDS[:19])
+
+
+@pytest.mark.gpu
+def test_unknown_variant_is_refused(cuda_lib):
+    d = scenarios.bench_slab(1000, nsteps=10)
+    with Solver(d) as s:
+        assert cuda_lib.dampm_set_ms_variant(s.h, 7, 1e7) == -1     # DAMPM_ERR_ARG
+        assert cuda_lib.dampm_set_ms_variant(s.h, 1, 1e7) == 0      # DAMPM_MS_ELFS
+        assert cuda_lib.dampm_set_ms_variant(s.h, 0, 1e7) == 0      # back to the default
