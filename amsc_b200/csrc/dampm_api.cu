@@ -295,10 +295,11 @@ int enqueue_front(dampm_ctx* ctx) {
   if (ms_due) {
     enqueue_unsort(ctx);
     enqueue_sort(ctx);
-    ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc,
+    ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->q, ctx->start, ctx->perm, ctx->nc,
                                 ctx->G, ctx->P, ctx->Z, ctx->ms, ctx->S, ctx->cap,
                                 ctx->stream, /*use_step_dt=*/1, 0.0, ctx->ms_variant,
                                 ctx->ms_stretch);
+    swap_moving(ctx->p, ctx->q);
     k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
     k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
                                                              ctx->p.slot, ctx->S);
@@ -485,15 +486,11 @@ int ensure_graph(dampm_ctx* ctx, int passes, int phase, dampm_ctx::GraphSlot** o
 }
 
 // The buffers after `passes` passes replayed from a graph: each pass
-// exchanges them once, a merge/split pass once more.
+// exchanges them once; a merge/split pass twice more (into reference order
+// before the call, and the emit into the free half), which leaves the
+// parity as it is.
 void advance_buffers(dampm_ctx* ctx, int passes) {
-  int swaps = passes;
-  if (ms_cadence(ctx)) {
-    const int L = ctx->ms.call_interval;
-    for (long long it = ctx->it_host + 1; it <= ctx->it_host + passes; ++it)
-      if (it % L == 0) ++swaps;
-  }
-  if (swaps & 1) swap_moving(ctx->p, ctx->q);
+  if (passes & 1) swap_moving(ctx->p, ctx->q);
 }
 
 // Reads the device scalars.  strict: a set status bit is returned as an
@@ -953,9 +950,10 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
   CK(cudaStreamSynchronize(ctx->stream));
   enqueue_unsort(ctx);
   enqueue_sort(ctx);
-  ms_enqueue(ctx->msb, ctx->p, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
+  ms_enqueue(ctx->msb, ctx->p, ctx->q, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
              ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt,
              ctx->ms_variant, ctx->ms_stretch);
+  swap_moving(ctx->p, ctx->q);
   k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
   k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
                                                            ctx->p.slot, ctx->S);

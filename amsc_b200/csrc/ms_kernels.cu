@@ -204,22 +204,39 @@ __device__ long long pair_cell(int b, int e, const int* perm, int* act,
   return n;
 }
 
+// Counts the merge candidates (into ms_counts[2], read by the pairing) and
+// the splits left after the cap (ms_counts[0]): a block reduction, then one
+// global atomic per block and count.
 __global__ void k_ms_count_cand(const int* act, int cap, Scalars* S) {
   if (!S->active) return;
-  __shared__ long long sm;
-  if (threadIdx.x == 0) sm = 0;
-  __syncthreads();
-  long long c = 0, s = 0;
+  __shared__ unsigned long long part[2][32];
+  unsigned long long c = 0, s = 0;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
-    c += (act[i] == MERGE_PRIMARY);
-    s += (act[i] == SPLIT);
+    const int a = act[i];
+    c += (a == MERGE_PRIMARY);
+    s += (a == SPLIT);
   }
-  atomicAdd((unsigned long long*)&sm, (unsigned long long)c);
-  atomicAdd((unsigned long long*)&S->ms_counts[0], (unsigned long long)s);
+  for (int o = 16; o > 0; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    part[0][w] = c;
+    part[1][w] = s;
+  }
   __syncthreads();
-  if (threadIdx.x == 0) atomicAdd((unsigned long long*)&S->ms_counts[2], (unsigned long long)sm);
+  if (threadIdx.x == 0) {
+    unsigned long long tc = 0, ts = 0;
+    for (int k = 0; k < nw; ++k) {
+      tc += part[0][k];
+      ts += part[1][k];
+    }
+    if (tc) atomicAdd((unsigned long long*)&S->ms_counts[2], tc);
+    if (ts) atomicAdd((unsigned long long*)&S->ms_counts[0], ts);
+  }
 }
 
 __global__ void k_ms_reset_counts(Scalars* S) {
@@ -342,14 +359,26 @@ __device__ __forceinline__ bool extensive(int k) {
   return k == 8 || k == 9 || k == 11 || k == 12 || k == 13;
 }
 
+// every field of every particle to the same slot of out (the grid's share)
+__device__ __forceinline__ void emit_identity(const Fields& in, const Fields& out, int np) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < kMsFields; ++k) out.f[k][i] = in.f[k][i];
+    out.label[i] = in.label[i];
+    out.level[i] = in.level[i];
+  }
+}
+
 __global__ void k_ms_emit(Fields in, Fields out, const int* act,
                           const int* partner, const int* offs, Geom G,
                           long long cap, Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   const int nnew = offs[cap];
-  if (nnew > cap) {
+  if (nnew > cap) {  // the state goes through unchanged (the caller exchanges buffers)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
+    emit_identity(in, out, np);
     return;
   }
   const double eps = 1e-10;
@@ -432,6 +461,9 @@ __global__ void k_ms_emit(Fields in, Fields out, const int* act,
   }
 }
 
+// The emit writes the moving fields straight into the free half of the
+// double buffer (which then becomes the state); the fields kept in
+// reference order (Ap, Fb, xp, yp, label, level) come back from scratch.
 __global__ void k_ms_copy_back(Fields from, Fields to, const int* offs,
                                long long cap, Scalars* S) {
   if (!S->active) return;
@@ -439,8 +471,11 @@ __global__ void k_ms_copy_back(Fields from, Fields to, const int* offs,
   if (nnew > cap) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnew;
        i += gridDim.x * blockDim.x) {
-#pragma unroll
-    for (int k = 0; k < kMsFields; ++k) to.f[k][i] = from.f[k][i];
+    to.f[11][i] = from.f[11][i];
+    to.f[14][i] = from.f[14][i];
+    to.f[15][i] = from.f[15][i];
+    to.f[20][i] = from.f[20][i];
+    to.f[21][i] = from.f[21][i];
     to.label[i] = from.label[i];
     to.level[i] = from.level[i];
   }
@@ -669,8 +704,9 @@ __global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
   if (!S->active) return;
   const int np = S->np;
   const int nnew = offs[cap];
-  if (nnew > cap) {
+  if (nnew > cap) {  // the state goes through unchanged (the caller exchanges buffers)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
+    emit_identity(in, out, np);
     return;
   }
   const double eps = 1e-10;
@@ -727,6 +763,8 @@ __global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
   }
 }
 
+bool ms_moving_slot_host(int k) { return k <= 10 || (k >= 16 && k <= 19); }
+
 int grid_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -744,7 +782,7 @@ int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
 
 }  // namespace
 
-int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
+int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const int* perm,
                int ncells, Geom G, Phys P, const double* Z,
                const dampm_ms_params& cfg, Scalars* S, long long cap,
                cudaStream_t st, int use_step_dt, double dt, int variant,
@@ -816,9 +854,13 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
                            p.F12, p.F22, p.Mp,  p.Vp,  p.H,      p.Ap,
                            m.mx,  m.my,  p.Fbx, p.Fby, p.vpx_dx, p.vpx_dy,
                            p.vpy_dx, p.vpy_dy, p.xp, p.yp};
+  double* qf[kMsFields] = {q.x,   q.y,   q.vpx, q.vpy, q.hp,     q.F11,
+                           q.F12, q.F22, q.Mp,  q.Vp,  q.H,      nullptr,
+                           nullptr, nullptr, nullptr, nullptr, q.vpx_dx, q.vpx_dy,
+                           q.vpy_dx, q.vpy_dy, nullptr, nullptr};
   for (int k = 0; k < kMsFields; ++k) {
     in.f[k] = pf[k];
-    out.f[k] = m.sd[k];
+    out.f[k] = ms_moving_slot_host(k) ? qf[k] : m.sd[k];
   }
   in.label = p.label;
   in.level = p.level;
@@ -830,8 +872,10 @@ int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
     k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
   k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
-  k_ms_pair_mom<<<gp, 256, 0, st>>>(m.mx, m.my, p, S);
-  launch_prep<double>(gp, 256, st, p, Z, G, P, S, 0);
+  // q (its moving fields written by the emit, the others shared) is the
+  // state from here on
+  k_ms_pair_mom<<<gp, 256, 0, st>>>(m.sd[12], m.sd[13], q, S);
+  launch_prep<double>(gp, 256, st, q, Z, G, P, S, 0);
   n += 5;
   return n;
 }

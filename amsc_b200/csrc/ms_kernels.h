@@ -76,7 +76,10 @@ enum MsVariant { kMsCmes = DAMPM_MS_CMES, kMsElfs = DAMPM_MS_ELFS };
 // Enqueues one adaptive_merge_split on the current binning (start/perm must
 // describe the current positions).  dt comes from the step's device scalar
 // when use_step_dt, else `dt`.  Returns the number of kernel launches.
-int ms_enqueue(MsBuffers& m, Particles p, const int* start, const int* perm,
+// p: the state (reference order), q: the free half of its double buffer,
+// which receives the emitted moving fields and holds the state afterwards
+// (the caller exchanges the two).
+int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const int* perm,
                int ncells, Geom G, Phys P, const double* Z,
                const dampm_ms_params& cfg, Scalars* S, long long cap,
                cudaStream_t stream, int use_step_dt, double dt, int variant = kMsCmes,
