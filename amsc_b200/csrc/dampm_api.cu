@@ -274,14 +274,6 @@ void enqueue_sort(dampm_ctx* ctx) {
   ctx->launches += 6;
 }
 
-// The particles into reference order (merge/split works in it): p -> q, then
-// the buffers are exchanged.
-void enqueue_unsort(dampm_ctx* ctx) {
-  launch_unsort<double>(grid_for(ctx->cap, 256), ctx->stream, ctx->p, ctx->q, ctx->S);
-  swap_moving(ctx->p, ctx->q);
-  ctx->launches += 1;
-}
-
 // One pass of the loop body in two halves: step start, sort and P2G; then
 // G2P and step end (slab mode exchanges node columns between them).
 int enqueue_front(dampm_ctx* ctx) {
@@ -292,8 +284,7 @@ int enqueue_front(dampm_ctx* ctx) {
   ev_mark(ctx, 3);
   k_step_begin<<<1, 1, 0, ctx->stream>>>(ctx->S, ctx->G, ctx->P);
   ctx->launches += 1;
-  if (ms_due) {
-    enqueue_unsort(ctx);
+  if (ms_due) {  // on the binning of the particles as they lie in storage
     enqueue_sort(ctx);
     ctx->launches += ms_enqueue(ctx->msb, ctx->p, ctx->q, ctx->start, ctx->perm, ctx->nc,
                                 ctx->G, ctx->P, ctx->Z, ctx->ms, ctx->S, ctx->cap,
@@ -486,11 +477,16 @@ int ensure_graph(dampm_ctx* ctx, int passes, int phase, dampm_ctx::GraphSlot** o
 }
 
 // The buffers after `passes` passes replayed from a graph: each pass
-// exchanges them once; a merge/split pass twice more (into reference order
-// before the call, and the emit into the free half), which leaves the
-// parity as it is.
+// exchanges them once, a merge/split pass once more (its emit writes the
+// free half).
 void advance_buffers(dampm_ctx* ctx, int passes) {
-  if (passes & 1) swap_moving(ctx->p, ctx->q);
+  int swaps = passes;
+  if (ms_cadence(ctx)) {
+    const int L = ctx->ms.call_interval;
+    for (long long it = ctx->it_host + 1; it <= ctx->it_host + passes; ++it)
+      if (it % L == 0) ++swaps;
+  }
+  if (swaps & 1) swap_moving(ctx->p, ctx->q);
 }
 
 // Reads the device scalars.  strict: a set status bit is returned as an
@@ -948,7 +944,6 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
   CK(cudaMemcpyAsync(&S->active, &ctx->Sh->active, sizeof(int),
                      cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  enqueue_unsort(ctx);
   enqueue_sort(ctx);
   ms_enqueue(ctx->msb, ctx->p, ctx->q, ctx->start, ctx->perm, ctx->nc, ctx->G, ctx->P,
              ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt,

@@ -194,10 +194,6 @@ __global__ void k_ledger_final(const double* led_part, const int* ucount,
 void launch_g2p(int grid, cudaStream_t st, Particles cur, Particles nxt, const int* perm,
                 const int* skey, Nodes nodes, const double* Z, Geom G, Phys P, Scalars* S,
                 int* count, int* leave, int record, int want_grad);
-// the particles of `src` into reference order in `dst` (slot idx[j])
-template <class R>
-void launch_unsort(int grid, cudaStream_t st, ParticlesT<R> src, ParticlesT<R> dst,
-                   const Scalars* S);
 
 // ---- batches of independent scenarios --------------------------------------
 // One scenario of a batch: its geometry, physics and place in the packed

@@ -49,27 +49,37 @@ struct MsCfg {
   double stretch;     // ELFS divergence trigger
 };
 
-__global__ void k_ms_materialize(Particles p, Phys P, const Scalars* S,
-                                 double* __restrict__ mx, double* __restrict__ my) {
+// Per storage slot: Ap, momentum and Fb as the reference stores them (the
+// uploaded or emitted values while `fresh`, else derived from the state),
+// and the reference-order fields xp, yp, label, level gathered through idx.
+__global__ void k_ms_materialize(Particles p, Phys P, const Scalars* S, MsBuffers m) {
   if (!S->active) return;
   const bool fresh = S->fresh != 0;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
-    if (fresh) {  // uploaded Ap, momentum and Fb stand as they are
-      const double2 m = p.mp[i];
-      mx[i] = m.x;
-      my[i] = m.y;
+    const int r = p.idx[i];
+    m.xps[i] = p.xp[r];
+    m.yps[i] = p.yp[r];
+    m.labs[i] = p.label[r];
+    m.levs[i] = p.level[r];
+    if (fresh) {  // uploaded or emitted Ap, momentum and Fb stand as they are
+      const double2 mm = p.mp[i];
+      m.mx[i] = mm.x;
+      m.my[i] = mm.y;
+      m.aps[i] = p.Ap[r];
+      m.fbxs[i] = p.Fbx[r];
+      m.fbys[i] = p.Fby[r];
       continue;
     }
     const double hp = p.hp[i];
-    p.Ap[i] = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
-    mx[i] = p.vpx[i] * p.Mp[i];
-    my[i] = p.vpy[i] * p.Mp[i];
+    m.aps[i] = hp > 1.e-2 ? p.Vp[i] / hp : 0.0;
+    m.mx[i] = p.vpx[i] * p.Mp[i];
+    m.my[i] = p.vpy[i] * p.Mp[i];
     double fx, fy;
     voellmy(P, p.vpx[i], p.vpy[i], hp, fx, fy);
-    p.Fbx[i] = fx;
-    p.Fby[i] = fy;
+    m.fbxs[i] = fx;
+    m.fbys[i] = fy;
   }
 }
 
@@ -324,18 +334,21 @@ __global__ void k_ms_demote(int* act, const int* partner, MsCfg c, const Scalars
     if (act[i] == MERGE_PRIMARY && partner[i] < 0) act[i] = KEEP;
 }
 
-__global__ void k_ms_weights(const int* act, int* w, int* partner, int cap, int split_w,
+// w in reference order: the weight of slot i goes to w[idx[i]] (idx is a
+// permutation of [0, np)), so that the scan gives each particle its place in
+// the compacted reference order; w[np..cap) is zero.
+__global__ void k_ms_weights(const int* act, const int* ridx, int* w, int cap, int split_w,
                              const Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap;
        i += gridDim.x * blockDim.x) {
-    int v = 0;
     if (i < np) {
       const int a = act[i];
-      v = (a == KEEP) ? 1 : (a == SPLIT) ? split_w : (a == MERGE_PRIMARY) ? 1 : 0;
+      w[ridx[i]] = (a == KEEP) ? 1 : (a == SPLIT) ? split_w : (a == MERGE_PRIMARY) ? 1 : 0;
+    } else {
+      w[i] = 0;
     }
-    w[i] = v;
   }
 }
 
@@ -359,26 +372,29 @@ __device__ __forceinline__ bool extensive(int k) {
   return k == 8 || k == 9 || k == 11 || k == 12 || k == 13;
 }
 
-// every field of every particle to the same slot of out (the grid's share)
-__device__ __forceinline__ void emit_identity(const Fields& in, const Fields& out, int np) {
+// every field of every particle to its reference position idx[i] of out
+// (the state as it was, in reference order; the grid's share)
+__device__ __forceinline__ void emit_identity(const Fields& in, const Fields& out, int np,
+                                              const int* ridx) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
+    const int o = ridx[i];
 #pragma unroll
-    for (int k = 0; k < kMsFields; ++k) out.f[k][i] = in.f[k][i];
-    out.label[i] = in.label[i];
-    out.level[i] = in.level[i];
+    for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
+    out.label[o] = in.label[i];
+    out.level[o] = in.level[i];
   }
 }
 
 __global__ void k_ms_emit(Fields in, Fields out, const int* act,
-                          const int* partner, const int* offs, Geom G,
+                          const int* partner, const int* offs, const int* ridx, Geom G,
                           long long cap, Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   const int nnew = offs[cap];
   if (nnew > cap) {  // the state goes through unchanged (the caller exchanges buffers)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
-    emit_identity(in, out, np);
+    emit_identity(in, out, np, ridx);
     return;
   }
   const double eps = 1e-10;
@@ -386,7 +402,7 @@ __global__ void k_ms_emit(Fields in, Fields out, const int* act,
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
     const int a = act[i];
-    const int o = offs[i];
+    const int o = offs[ridx[i]];
     if (a == KEEP) {
 #pragma unroll
       for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
@@ -699,14 +715,14 @@ __global__ void k_elfs_mark(Particles p, const int* __restrict__ hops, const int
 // momentum rebuilt; a merge leaves the centre of mass with the extensive
 // fields summed, the rest mass-averaged and the primary's label.
 __global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
-                               const int* partner, const int* offs, Geom G,
+                               const int* partner, const int* offs, const int* ridx, Geom G,
                                long long cap, Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   const int nnew = offs[cap];
   if (nnew > cap) {  // the state goes through unchanged (the caller exchanges buffers)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
-    emit_identity(in, out, np);
+    emit_identity(in, out, np, ridx);
     return;
   }
   const double eps = 1e-10;
@@ -716,7 +732,7 @@ __global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
     const int a = act[i];
-    const int o = offs[i];
+    const int o = offs[ridx[i]];
     if (a == KEEP) {
 #pragma unroll
       for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
@@ -817,7 +833,17 @@ int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const i
   const int gp = grid_for(cap, 256);
   const int ic = int(cap);
   k_ms_reset_counts<<<1, 1, 0, st>>>(S);
-  k_ms_materialize<<<gp, 256, 0, st>>>(p, P, S, m.mx, m.my);
+  k_ms_materialize<<<gp, 256, 0, st>>>(p, P, S, m);
+  // the state as the decision and the emit read it: moving fields at their
+  // storage slots, the reference-order ones from the per-slot scratch
+  Particles pv = p;
+  pv.Ap = m.aps;
+  pv.Fbx = m.fbxs;
+  pv.Fby = m.fbys;
+  pv.xp = m.xps;
+  pv.yp = m.yps;
+  pv.label = m.labs;
+  pv.level = m.levs;
   n += 2;
   if (elfs) {
     const int gc = grid_for(ncells, 256);
@@ -826,10 +852,10 @@ int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const i
     k_elfs_roots<<<gc, 256, 0, st>>>(m.uf, m.eroot, G.nrows, G.ncols, S);
     k_elfs_seeds<<<gc, 256, 0, st>>>(m.uf, m.eroot, m.hops, m.bq, m.bqn, G.nrows, G.ncols, S);
     k_elfs_bfs<<<1, 1024, 0, st>>>(m.uf, m.hops, m.bq, m.bqn, G.nrows, G.ncols, S);
-    k_elfs_mark<<<gp, 256, 0, st>>>(p, m.hops, m.uf, m.eroot, G, c, m.act, ic, S);
+    k_elfs_mark<<<gp, 256, 0, st>>>(pv, m.hops, m.uf, m.eroot, G, c, m.act, ic, S);
     n += 5;
   } else {
-    k_ms_mark<<<gp, 256, 0, st>>>(p, G, c, m.act, ic, S);
+    k_ms_mark<<<gp, 256, 0, st>>>(pv, G, c, m.act, ic, S);
   }
   k_ms_init_partner<<<gp, 256, 0, st>>>(m.partner, ic, S);
   k_ms_split_flags<<<gp, 256, 0, st>>>(perm, m.act, m.flag, ic, S);
@@ -846,14 +872,14 @@ int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const i
                                     m.paired, p, c, S);
   k_ms_demote<<<gp, 256, 0, st>>>(m.act, m.partner, c, S);
   n += 2;
-  k_ms_weights<<<gp, 256, 0, st>>>(m.act, m.w, m.partner, ic, c.split_w, S);
+  k_ms_weights<<<gp, 256, 0, st>>>(m.act, p.idx, m.w, ic, c.split_w, S);
   n += 5;
   n += scan_enqueue(m.w, m.offs, ic, m.tile_sum, m.ntiles, S, st);
   Fields in{}, out{};
-  double* pf[kMsFields] = {p.x,   p.y,   p.vpx, p.vpy, p.hp,     p.F11,
-                           p.F12, p.F22, p.Mp,  p.Vp,  p.H,      p.Ap,
-                           m.mx,  m.my,  p.Fbx, p.Fby, p.vpx_dx, p.vpx_dy,
-                           p.vpy_dx, p.vpy_dy, p.xp, p.yp};
+  double* pf[kMsFields] = {pv.x,   pv.y,   pv.vpx, pv.vpy, pv.hp,     pv.F11,
+                           pv.F12, pv.F22, pv.Mp,  pv.Vp,  pv.H,      pv.Ap,
+                           m.mx,   m.my,   pv.Fbx, pv.Fby, pv.vpx_dx, pv.vpx_dy,
+                           pv.vpy_dx, pv.vpy_dy, pv.xp, pv.yp};
   double* qf[kMsFields] = {q.x,   q.y,   q.vpx, q.vpy, q.hp,     q.F11,
                            q.F12, q.F22, q.Mp,  q.Vp,  q.H,      nullptr,
                            nullptr, nullptr, nullptr, nullptr, q.vpx_dx, q.vpx_dy,
@@ -862,15 +888,24 @@ int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const i
     in.f[k] = pf[k];
     out.f[k] = ms_moving_slot_host(k) ? qf[k] : m.sd[k];
   }
-  in.label = p.label;
-  in.level = p.level;
+  in.label = pv.label;
+  in.level = pv.level;
   out.label = m.slabel;
   out.level = m.slevel;
   if (elfs)
-    k_ms_emit_elfs<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
+    k_ms_emit_elfs<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, p.idx, G, cap, S);
   else
-    k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, G, cap, S);
-  k_ms_copy_back<<<gp, 256, 0, st>>>(out, in, m.offs, cap, S);
+    k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, p.idx, G, cap, S);
+  // the reference-order fields back into their arrays
+  Fields fixed{};
+  fixed.f[11] = p.Ap;
+  fixed.f[14] = p.Fbx;
+  fixed.f[15] = p.Fby;
+  fixed.f[20] = p.xp;
+  fixed.f[21] = p.yp;
+  fixed.label = p.label;
+  fixed.level = p.level;
+  k_ms_copy_back<<<gp, 256, 0, st>>>(out, fixed, m.offs, cap, S);
   k_ms_finish<<<1, 1, 0, st>>>(m.offs, cap, S);
   // q (its moving fields written by the emit, the others shared) is the
   // state from here on

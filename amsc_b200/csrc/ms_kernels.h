@@ -20,6 +20,11 @@ struct MsBuffers {
   double* sd[kMsFields] = {};
   double *mx = nullptr, *my = nullptr;  // the momentum pair as two fields
   int *slabel = nullptr, *slevel = nullptr;
+  // the reference-order fields of each storage slot for the decision and
+  // the emit (Ap and Fb derived or gathered, xp, yp, label, level gathered
+  // through idx), so that a call works on the sorted storage as it lies
+  double *aps = nullptr, *fbxs = nullptr, *fbys = nullptr, *xps = nullptr, *yps = nullptr;
+  int *labs = nullptr, *levs = nullptr;
   // the ELFS variant's cell arrays (allocated when it is selected): the
   // empty cells' union-find forest (-1: a cell with particles), the roots
   // that reach the grid edge, the hop counts from the free surface, the
@@ -33,7 +38,7 @@ int ms_alloc(MsBuffers& m, long long cap, int /*ncells*/, Alloc alloc) {
   m.cap = cap;
   m.ntiles = int((cap + kScanTile - 1) / kScanTile);
   int** ints[] = {&m.act, &m.partner, &m.w, &m.offs, &m.flag, &m.rank,
-                        &m.paired, &m.slabel, &m.slevel};
+                        &m.paired, &m.slabel, &m.slevel, &m.labs, &m.levs};
   for (int** q : ints) {
     int rc = alloc((void**)q, sizeof(int) * size_t(cap + 1));
     if (rc) return rc;
@@ -50,6 +55,11 @@ int ms_alloc(MsBuffers& m, long long cap, int /*ncells*/, Alloc alloc) {
   if (rc) return rc;
   rc = alloc((void**)&m.my, sizeof(double) * size_t(cap));
   if (rc) return rc;
+  double** dd[] = {&m.aps, &m.fbxs, &m.fbys, &m.xps, &m.yps};
+  for (double** q : dd) {
+    rc = alloc((void**)q, sizeof(double) * size_t(cap));
+    if (rc) return rc;
+  }
   return 0;
 }
 
@@ -76,9 +86,10 @@ enum MsVariant { kMsCmes = DAMPM_MS_CMES, kMsElfs = DAMPM_MS_ELFS };
 // Enqueues one adaptive_merge_split on the current binning (start/perm must
 // describe the current positions).  dt comes from the step's device scalar
 // when use_step_dt, else `dt`.  Returns the number of kernel launches.
-// p: the state (reference order), q: the free half of its double buffer,
-// which receives the emitted moving fields and holds the state afterwards
-// (the caller exchanges the two).
+// p: the state (its storage in the sorted order of the last step, idx the
+// reference index of each slot), q: the free half of its double buffer,
+// which receives the emitted particles in the compacted reference order and
+// holds the state afterwards (the caller exchanges the two).
 int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const int* perm,
                int ncells, Geom G, Phys P, const double* Z,
                const dampm_ms_params& cfg, Scalars* S, long long cap,

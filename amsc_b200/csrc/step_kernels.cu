@@ -1723,15 +1723,6 @@ void launch_g2p(int grid, cudaStream_t st, Particles cur, Particles nxt, const i
                                                          P, S, count, leave);
 }
 
-// Storage into reference order: the particle in slot j of src goes to slot
-// idx[j] of dst (merge/split works in reference order).
-template <class R>
-__global__ void k_unsort(ParticlesT<R> src, ParticlesT<R> dst, const Scalars* S) {
-  const int np = S->np;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += gridDim.x * blockDim.x)
-    copy_moving(src, j, dst, src.idx[j]);
-}
-
 size_t p2g_smem_bytes() { return sizeof(P2GSmemT<double>); }
 
 __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b,
@@ -2061,12 +2052,6 @@ void launch_b_g2p(int grid, cudaStream_t st, ParticlesT<R> cur, ParticlesT<R> nx
 }
 
 template <class R>
-void launch_unsort(int grid, cudaStream_t st, ParticlesT<R> src, ParticlesT<R> dst,
-                   const Scalars* S) {
-  k_unsort<R><<<grid, 256, 0, st>>>(src, dst, S);
-}
-
-template <class R>
 void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> src,
                    const int4* mblk) {
   k_b_move<R><<<grid, kG2PThreads, 0, st>>>(dst, src, mblk);
@@ -2085,8 +2070,6 @@ void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> s
   template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,      \
                                 const int*, const int*, const V2<R>*, const double*,  \
                                 const Scn*, Scalars*, const int2*, Scalars*, int*);   \
-  template void launch_unsort<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,     \
-                                 const Scalars*);                                     \
   template void launch_b_move<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,     \
                                  const int4*);
 DAMPM_INSTANTIATE(double)
