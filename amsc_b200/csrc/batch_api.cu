@@ -61,6 +61,7 @@ struct dampm_batch {
   int *count = nullptr, *start = nullptr, *perm = nullptr;
   int* skey = nullptr;  // the cell key of each sorted position
   int *tile_sum = nullptr, *clist = nullptr, *clist_n = nullptr, *cbig = nullptr;
+  unsigned char* tflag = nullptr;  // the scan tiles of a pass (k_b_tile_flags)
   int* cmid = nullptr;  // cells with more than 16 particles
   int* ustart = nullptr;
   long long* upex = nullptr;
@@ -236,7 +237,7 @@ int read_scalars(dampm_batch* b) {
 }
 
 // One pass of every live scenario: kPassLaunches kernel launches.
-constexpr int kPassLaunches = 13;
+constexpr int kPassLaunches = 14;
 int enqueue_pass(dampm_batch* b) {
   cudaStream_t st = b->stream;
   const int nscn = int(b->scns.size());
@@ -248,11 +249,14 @@ int enqueue_pass(dampm_batch* b) {
   const int* idx = b->precision == DAMPM_FP32 ? b->p32[b->cur].idx : b->p64[b->cur].idx;
   k_b_step_begin<<<1, 1024, 0, st>>>(b->scn, b->S, nscn, b->Sg);
   const int gp = grid_blocks(b->P_tot, 256);
-  // the counting sort of every scenario at once (G2P counted the keys)
+  // the counting sort of every scenario at once (G2P counted the keys), over
+  // the tiles the scenarios' key ranges meet
+  k_b_tile_flags<<<grid_blocks(ntiles, 256), 256, 0, st>>>(b->scn, b->S, nscn, b->Sg,
+                                                            b->tflag, ntiles);
   k_scan_sums<<<ntiles, kScanThreads, 0, st>>>(b->count, ncell, b->tile_sum, b->clist_n,
-                                               b->Sg, 1);
+                                               b->Sg, 0, b->tflag);
   k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(b->count, ncell, b->tile_sum, b->start,
-                                                b->clist, b->clist_n, b->Sg, 1);
+                                                b->clist, b->clist_n, b->Sg, 0, b->tflag);
   k_scatter<<<gp, 256, 0, st>>>(key, slot, idx, b->start, b->perm, b->skey, b->sortbuf,
                                 b->Sg);
   k_segment_order<<<148 * 4, 256, 0, st>>>(b->start, b->clist, b->clist_n, b->perm,
@@ -266,7 +270,7 @@ int enqueue_pass(dampm_batch* b) {
       b->col_weight, b->ustart, b->upex, b->uplan, b->strip_n);
   k_b_units_flat<<<1, kPlanThreads, sizeof(int) * (b->strips_tot + 1), st>>>(
       b->strip_n, b->strips_tot, b->strip_scn, b->scn, nscn, b->uplan, b->ulist,
-      b->ucount, b->scn_units, b->Sg);
+      b->ucount, b->scn_units, b->S, b->Sg);
   if (b->precision == DAMPM_FP32)
     launch_b_p2g<float>(b->p2g_grid, st, b->p32[b->cur], b->perm, b->start,
                         static_cast<float2*>(b->vvL),
@@ -423,6 +427,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   rc = rc ? rc : balloc(b, &b->clist, nn + 4);
   rc = rc ? rc : balloc(b, &b->clist_n, 4);
   rc = rc ? rc : balloc(b, &b->tile_sum, nn / kScanTile + 2);
+  rc = rc ? rc : balloc(b, &b->tflag, nn / kScanTile + 2);
   rc = rc ? rc : balloc(b, &b->perm, pc);
   rc = rc ? rc : balloc(b, &b->skey, pc);
   rc = rc ? rc : balloc(b, &b->cbig, pc / 256 + 4);
@@ -526,6 +531,11 @@ int dampm_batch_add(dampm_batch* b, const dampm_grid* grid, const dampm_params* 
   Scalars s0{};
   s0.fresh = 1;
   s0.np = int(np);
+  // the first plan covers all of the scenario's cells
+  s0.krange[0] = 0x7fffffff;
+  s0.krange[1] = -1;
+  s0.knext[0] = d.c_off;
+  s0.knext[1] = d.c_off + int(h.nc) - 1;
   b->Sh[pos] = s0;
   BCK(cudaMemcpyAsync(b->S + pos, b->Sh + pos, sizeof(Scalars), cudaMemcpyHostToDevice,
                       st));
@@ -592,6 +602,11 @@ int dampm_batch_compact(dampm_batch* b) {
     strips += old.nstrips;
     U += (long long)old.nstrips * (h.grid.Nex + 1);
     S.push_back(b->Sh[s]);
+    // its cells move: the first plan after the move covers all of them
+    S.back().krange[0] = 0x7fffffff;
+    S.back().krange[1] = -1;
+    S.back().knext[0] = h.d.c_off;
+    S.back().knext[1] = h.d.c_off + int(h.nc) - 1;
     keep.push_back(h);
   }
   const int nxt = 1 - b->cur, znxt = 1 - b->zcur;

@@ -257,9 +257,10 @@ void enqueue_sort(dampm_ctx* ctx) {
   const int gp = grid_for(ctx->cap, 256);
   k_scan_sums<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(ctx->count, ctx->nc,
                                                              ctx->tile_sum, ctx->clist_n,
-                                                             ctx->S, 1);
+                                                             ctx->S, 1, nullptr);
   k_scan_apply<<<ctx->ntiles, kScanThreads, 0, ctx->stream>>>(
-      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S, 1);
+      ctx->count, ctx->nc, ctx->tile_sum, ctx->start, ctx->clist, ctx->clist_n, ctx->S, 1,
+      nullptr);
   k_scatter<<<gp, 256, 0, ctx->stream>>>(ctx->p.key, ctx->p.slot, ctx->p.idx, ctx->start,
                                          ctx->perm, ctx->skey, ctx->sortbuf, ctx->S);
   k_segment_order<<<148 * 4, 256, 0, ctx->stream>>>(ctx->start, ctx->clist,

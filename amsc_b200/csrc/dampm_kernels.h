@@ -154,11 +154,12 @@ void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const do
 __global__ void k_count(const int* key, int* count, int* slot,
                         const Scalars* S);
 __global__ void k_count_n(const int* key, int* count, int* slot, int n);
+// tflag (may be null): scan only the flagged tiles (k_b_tile_flags)
 __global__ void k_scan_sums(const int* count, int n, int* tile_sum, int* list_n,
-                            const Scalars* S, int ranged);
+                            const Scalars* S, int ranged, const unsigned char* tflag);
 __global__ void k_scan_apply(int* count, int n, const int* tile_sum,
                              int* start, int* list, int* list_n,
-                             const Scalars* S, int ranged);
+                             const Scalars* S, int ranged, const unsigned char* tflag);
 // pk: 2 x capacity entries; the scatter writes the first half, which the
 // per-cell ordering sorts (the crowded cells use both halves)
 __global__ void k_scatter(const int* key, const int* slot, const int* idx, const int* start,
@@ -218,7 +219,9 @@ __global__ void k_b_units_plan(const int* cstart, const Scn* scn, const Scalars*
 __global__ void k_b_units_flat(const int* strip_n, int strips, const int* strip_scn,
                                const Scn* scn, int nscn, const int2* plan,
                                int4* ulist, int* ucount, int2* scn_units,
-                               const Scalars* Sg);
+                               Scalars* S, const Scalars* Sg);
+__global__ void k_b_tile_flags(const Scn* scn, const Scalars* S, int nscn, const Scalars* Sg,
+                               unsigned char* tflag, int ntiles);
 template <class R>
 void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
                   const int* cstart, V2<R>* vvL, double* led_part, const Scn* scn,

@@ -791,8 +791,9 @@ int grid_for(long long n, int threads) {
 // exclusive scan of a[0..n) -> out[0..n] (a is zeroed), n = cap
 int scan_enqueue(int* a, int* out, int n, int* tile_sum, int ntiles,
                  const Scalars* S, cudaStream_t st) {
-  k_scan_sums<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, nullptr, S, 0);
-  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, nullptr, nullptr, S, 0);
+  k_scan_sums<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, nullptr, S, 0, nullptr);
+  k_scan_apply<<<ntiles, kScanThreads, 0, st>>>(a, n, tile_sum, out, nullptr, nullptr, S, 0,
+                                                nullptr);
   return 2;
 }
 

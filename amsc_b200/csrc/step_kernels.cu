@@ -272,7 +272,10 @@ __global__ void k_count(const int* __restrict__ key, int* __restrict__ count,
 // start is either 0 (below every key) or np (above), as before, so the old
 // values stand.  k_scan_sums writes the tile totals; k_scan_apply adds, per
 // tile, the totals of the preceding tiles in the range to a block scan.
-// count is zeroed on the way (ready for the next step's atomics).  When
+// count is zeroed on the way (ready for the next step's atomics).  With
+// tile flags (batches) only the flagged tiles are scanned: the others hold
+// no particle of any scenario, now or at the last sort, so their totals are
+// zero and their starts stand.  When
 // `list` is given, cells holding two or more particles are appended to it
 // (the cells whose order k_segment_order has to establish).
 __device__ __forceinline__ int block_incl_scan(int v, int* wsum) {
@@ -343,13 +346,18 @@ __device__ __forceinline__ void scan_tiles_of(const Scalars* S, int n, int range
 
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_sums(const int* __restrict__ count, int n, int* __restrict__ tile_sum,
-                int* __restrict__ list_n, const Scalars* S, int ranged) {
+                int* __restrict__ list_n, const Scalars* S, int ranged,
+                const unsigned char* __restrict__ tflag) {
   if (!S->active) return;
   if (list_n && blockIdx.x == 0 && threadIdx.x < 3) list_n[threadIdx.x] = 0;
   int t0, t1;
   scan_tiles_of(S, n, ranged, t0, t1);
   const int t = blockIdx.x;
   if (t < t0 || t > t1) return;  // block-uniform
+  if (tflag && !tflag[t]) {  // a tile no scenario's keys meet: no particles
+    if (threadIdx.x == 0) tile_sum[t] = 0;
+    return;
+  }
   __shared__ int wsum[32];
   const int4 c = load_count4(count, t * kScanTile + threadIdx.x * 4, n);
   const int tot = block_sum(c.x + c.y + c.z + c.w, wsum);
@@ -359,12 +367,14 @@ __global__ void __launch_bounds__(kScanThreads)
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_apply(int* __restrict__ count, int n, const int* __restrict__ tile_sum,
                  int* __restrict__ start, int* __restrict__ list,
-                 int* __restrict__ list_n, const Scalars* S, int ranged) {
+                 int* __restrict__ list_n, const Scalars* S, int ranged,
+                 const unsigned char* __restrict__ tflag) {
   if (!S->active) return;
   int t0, t1;
   scan_tiles_of(S, n, ranged, t0, t1);
   const int t = blockIdx.x;
   if (t < t0 || t > t1) return;  // block-uniform
+  if (tflag && !tflag[t]) return;  // its starts stand (see k_b_tile_flags)
   __shared__ int wsum[32];
   // particles in the range's tiles before this one
   int pre = 0;
@@ -1033,7 +1043,8 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
                                           const Geom& G, long long T, int strip,
                                           int* __restrict__ st,
                                           long long* __restrict__ px,
-                                          int2* __restrict__ plan, int col_weight) {
+                                          int2* __restrict__ plan, int col_weight,
+                                          int c_lo, int c_hi) {
   __shared__ long long wt_ll[32];
   __shared__ int wt_i[32];
   __shared__ long long last_id;
@@ -1042,10 +1053,10 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
   const int rlo = max(r0 - 1, 0), rhi = min(r0 + kTR - 1, nrows - 1);
   long long carry = 0, prev_id = -1;
   int K = 0;
-  for (int base = 0; base <= ncols; base += blockDim.x) {
+  for (int base = c_lo; base <= c_hi; base += blockDim.x) {
     const int nc = base + threadIdx.x;
     long long w = 0;
-    if (nc < ncols) w = column_count(cstart, rlo, rhi, nc, nrows) + col_weight;
+    if (nc <= c_hi && nc < ncols) w = column_count(cstart, rlo, rhi, nc, nrows) + col_weight;
     long long tot;
     const long long incl = block_incl_scan<long long>(w, wt_ll, tot);
     const long long pex = carry + incl - w;
@@ -1058,7 +1069,7 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
       idp = threadIdx.x == 0 ? prev_id : wt_ll[(threadIdx.x >> 5) - 1];
     if (threadIdx.x == blockDim.x - 1) last_id = id;
     __syncthreads();
-    const int flag = (nc == 0) || (nc < ncols && id != idp);
+    const int flag = (nc == c_lo) || (nc <= c_hi && nc < ncols && id != idp);
     int ktot;
     const int kin = block_incl_scan<int>(flag, wt_i, ktot);
     if (flag) {
@@ -1078,7 +1089,7 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
     if (k < K) {
       cA = st[k];
       const bool more = k + 1 < K;
-      cB = more ? st[k + 1] : ncols + 1;
+      cB = more ? st[k + 1] : c_hi + 1;
       const long long sumw = (more ? px[k + 1] : ptotal) - px[k];
       const long long n = sumw - (long long)col_weight * (min(cB, ncols) - cA) +
                           (cA > 0 ? column_count(cstart, rlo, rhi, cA - 1, nrows) : 0);
@@ -1106,8 +1117,16 @@ __global__ void __launch_bounds__(kPlanThreads)
   if (!S->active) return;
   const int strip = blockIdx.x;
   const size_t b = (size_t)strip * seg;
+  // node columns of the cells the particles are binned to (the key range the
+  // scatter just rolled over), plus the column right of them
+  const int L = S->krange[0], H = S->krange[1];
+  if (L > H) {  // no particle
+    if (threadIdx.x == 0) strip_n[strip] = 0;
+    return;
+  }
+  const int c_lo = L / G.nrows, c_hi = min(H / G.nrows + 1, G.ncols);
   const int J = plan_strip(cstart, G, unit_weight(S, target_units), strip,
-                           ustart + b, upex + b, plan + b, kColWeight);
+                           ustart + b, upex + b, plan + b, kColWeight, c_lo, c_hi);
   if (threadIdx.x == 0) strip_n[strip] = J;
 }
 
@@ -1787,9 +1806,54 @@ __global__ void __launch_bounds__(kPlanThreads)
   const Geom G = scn[s].G;
   const int local = b - scn[s].strip_off;
   const size_t base = (size_t)scn[s].useg_off + (size_t)local * (G.ncols + 1);
+  // node columns of the cells the scenario's particles are binned to (the
+  // keys its last G2P made), plus the column right of them; every column
+  // after a layout change
+  int c_lo = 0, c_hi = G.ncols;
+  if (!(Sg->krange[0] <= Sg->krange[1])) {
+    const int L = S[s].knext[0], H = S[s].knext[1];
+    if (L > H) {  // no particle
+      if (threadIdx.x == 0) strip_n[b] = 0;
+      return;
+    }
+    c_lo = (L - scn[s].c_off) / G.nrows;
+    c_hi = min((H - scn[s].c_off) / G.nrows + 1, G.ncols);
+  }
   const int J = plan_strip(cstart + scn[s].c_off, G, unit_weight(Sg, target_units),
-                           local, ustart + base, upex + base, plan + base, col_weight);
+                           local, ustart + base, upex + base, plan + base, col_weight,
+                           c_lo, c_hi);
   if (threadIdx.x == 0) strip_n[b] = J;
+}
+
+// The scan tiles of a batch pass: those that meet the batch-wide range
+// (every cell after a layout change) or a scenario's keys -- the keys its
+// cell starts describe (krange) or the keys its last G2P made (knext).  A
+// tile that meets neither holds no particle now or at the last sort, and
+// its cells' starts (the particles of the scenarios before them) stand
+// while the layout does.  One thread per tile; the scenarios' cells are
+// consecutive, so a binary search finds the first that meets the tile.
+__global__ void k_b_tile_flags(const Scn* __restrict__ scn, const Scalars* S, int nscn,
+                               const Scalars* Sg, unsigned char* __restrict__ tflag,
+                               int ntiles) {
+  if (!Sg->active) return;
+  const int gL = min(Sg->krange[0], Sg->knext[0]), gH = max(Sg->krange[1], Sg->knext[1]);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles;
+       t += gridDim.x * blockDim.x) {
+    const int c0 = t * kScanTile, c1 = c0 + kScanTile - 1;
+    bool f = gL <= gH && gL <= c1 && gH >= c0;
+    int lo = 0, hi = nscn;  // the first scenario whose cells end after c0
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (scn[mid].c_off + scn[mid].G.nrows * scn[mid].G.ncols <= c0) lo = mid + 1;
+      else hi = mid;
+    }
+    for (int s = lo; !f && s < nscn && scn[s].c_off <= c1; ++s) {
+      const int L = min(S[s].krange[0], S[s].knext[0]);
+      const int H = max(S[s].krange[1], S[s].knext[1]);
+      f = L <= H && L <= c1 && H >= c0;
+    }
+    tflag[t] = f ? 1 : 0;
+  }
 }
 
 // one block: the flat list {scenario, strip, cA, cB} in strip order, and each
@@ -1799,7 +1863,7 @@ __global__ void __launch_bounds__(kPlanThreads)
                    const int* __restrict__ strip_scn, const Scn* __restrict__ scn,
                    int nscn, const int2* __restrict__ plan, int4* __restrict__ ulist,
                    int* __restrict__ ucount, int2* __restrict__ scn_units,
-                   const Scalars* Sg) {
+                   Scalars* S, const Scalars* Sg) {
   if (!Sg->active) return;
   extern __shared__ int uoff[];  // strips + 1
   __shared__ int wt_i[32];
@@ -1831,6 +1895,12 @@ __global__ void __launch_bounds__(kPlanThreads)
   for (int s = threadIdx.x; s < nscn; s += blockDim.x) {
     const int b0 = scn[s].strip_off, b1 = b0 + scn[s].nstrips;
     scn_units[s] = make_int2(uoff[b0], uoff[b1]);
+    // each scenario's key ranges roll over: the starts now describe the
+    // keys its last G2P made, and the next G2P starts an empty range
+    S[s].krange[0] = S[s].knext[0];
+    S[s].krange[1] = S[s].knext[1];
+    S[s].knext[0] = 0x7fffffff;
+    S[s].knext[1] = -1;
   }
   if (threadIdx.x == 0) {
     ucount[0] = total;
@@ -1916,7 +1986,7 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
       nkey = nxt.key[j];
     }
     count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
-    key_range(ok ? nkey : 0x7fffffff, ok ? nkey : -1, kred, Sg);
+    key_range(ok ? nkey : 0x7fffffff, ok ? nkey : -1, kred, &S[s]);
     return;
   }
   const Geom G = scn[s].G;
@@ -1933,7 +2003,7 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
                  c_off, m0, m1, m2, bad, nkey);
   count_key(nkey, ok, count, nxt.slot + (ok ? j : 0));
   cfl_block_max(m0, m1, m2, red, &S[s]);
-  key_range(ok ? nkey : 0x7fffffff, ok ? nkey : -1, kred, Sg);
+  key_range(ok ? nkey : 0x7fffffff, ok ? nkey : -1, kred, &S[s]);
   flag_non_finite(bad, &S[s]);
 }
 
