@@ -292,7 +292,7 @@ int enqueue_front(dampm_ctx* ctx) {
                                 ctx->stream, /*use_step_dt=*/1, 0.0, ctx->ms_variant,
                                 ctx->ms_stretch);
     swap_moving(ctx->p, ctx->q);
-    k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
+    k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S, 0);
     k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
                                                              ctx->p.slot, ctx->S);
     ctx->launches += 2;
@@ -597,11 +597,11 @@ int resolve_field(dampm_ctx* ctx, const std::string& f, bool fresh, FieldSrc& r)
   else if (f == "vpy_dy") r.sorted = p.vpy_dy;
   else if (f == "label") r.iref = p.label;
   else if (f == "level") r.iref = p.level;
-  // fresh values sit in reference-ordered slots (idx = slot)
-  else if (f == "Ap") { if (fresh) r.sorted = p.Ap; else r.derived = 0; }
+  // fresh values (uploaded or emitted by merge/split) are kept in reference order
+  else if (f == "Ap") { if (fresh) r.ref = p.Ap; else r.derived = 0; }
   else if (f == "mom_px" || f == "mom_py") r.pair_half = f == "mom_px" ? 0 : 1;
-  else if (f == "Fb_x") { if (fresh) r.sorted = p.Fbx; else r.derived = 3; }
-  else if (f == "Fb_y") { if (fresh) r.sorted = p.Fby; else r.derived = 4; }
+  else if (f == "Fb_x") { if (fresh) r.ref = p.Fbx; else r.derived = 3; }
+  else if (f == "Fb_y") { if (fresh) r.ref = p.Fby; else r.derived = 4; }
   else if (ctx->record_alloc) {
     if (f == "apx") r.sorted = p.apx;
     else if (f == "apy") r.sorted = p.apy;
@@ -950,7 +950,7 @@ int dampm_merge_split(dampm_ctx* ctx, double dt, long long counts[4]) {
              ctx->Z, ctx->ms, ctx->S, ctx->cap, ctx->stream, /*use_step_dt=*/0, dt,
              ctx->ms_variant, ctx->ms_stretch);
   swap_moving(ctx->p, ctx->q);
-  k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S);
+  k_keys<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p, ctx->G, ctx->S, 0);
   k_count<<<grid_for(ctx->cap, 256), 256, 0, ctx->stream>>>(ctx->p.key, ctx->count,
                                                            ctx->p.slot, ctx->S);
   CK(cudaGetLastError());
@@ -1079,7 +1079,7 @@ int dampm_set_state(dampm_ctx* ctx, long long np, const double* const* fields,
                      ctx->stream));
   // the slots now hold the particles in reference order
   CK(cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream));
-  k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->G, ctx->S);
+  k_keys<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->G, ctx->S, 1);
   k_count_n<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p.key, ctx->count, p.slot, int(np));
   k_reduce_state<<<grid_for(np, 256), 256, 0, ctx->stream>>>(p, ctx->S);
   launch_prep<double>(grid_for(np, 256), 256, ctx->stream, p, ctx->Z, ctx->G, ctx->P,

@@ -140,9 +140,9 @@ template <class R>
 void launch_init_particles(int grid, int block, cudaStream_t st, ParticlesT<R> p,
                            const double* Z, const double* dZdx, const double* dZdy,
                            Geom G, Phys P, Scalars* S, int np, int key_off);
-// cell keys of the current positions, idx = slot (reference order); the
-// next sort scans every cell
-__global__ void k_keys(Particles p, Geom G, Scalars* S);
+// cell keys of the current positions (and idx = slot when set_idx: slots
+// in reference order); the next sort scans every cell
+__global__ void k_keys(Particles p, Geom G, Scalars* S, int set_idx);
 __global__ void k_reduce_state(Particles p, Scalars* S);
 template <class R>
 void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const double* Z,

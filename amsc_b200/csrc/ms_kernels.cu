@@ -335,19 +335,23 @@ __global__ void k_ms_demote(int* act, const int* partner, MsCfg c, const Scalars
 }
 
 // w in reference order: the weight of slot i goes to w[idx[i]] (idx is a
-// permutation of [0, np)), so that the scan gives each particle its place in
-// the compacted reference order; w[np..cap) is zero.
-__global__ void k_ms_weights(const int* act, const int* ridx, int* w, int cap, int split_w,
-                             const Scalars* S) {
+// permutation of [0, np)), so that the scan gives each particle its index in
+// the compacted reference order; wslot in slot order, whose scan gives its
+// storage slot; both are zero from np to cap.
+__global__ void k_ms_weights(const int* act, const int* ridx, int* w, int* wslot, int cap,
+                             int split_w, const Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap;
        i += gridDim.x * blockDim.x) {
     if (i < np) {
       const int a = act[i];
-      w[ridx[i]] = (a == KEEP) ? 1 : (a == SPLIT) ? split_w : (a == MERGE_PRIMARY) ? 1 : 0;
+      const int wt = (a == KEEP) ? 1 : (a == SPLIT) ? split_w : (a == MERGE_PRIMARY) ? 1 : 0;
+      w[ridx[i]] = wt;
+      wslot[i] = wt;
     } else {
       w[i] = 0;
+      wslot[i] = 0;
     }
   }
 }
@@ -372,29 +376,48 @@ __device__ __forceinline__ bool extensive(int k) {
   return k == 8 || k == 9 || k == 11 || k == 12 || k == 13;
 }
 
-// every field of every particle to its reference position idx[i] of out
-// (the state as it was, in reference order; the grid's share)
+// Emitted particles are stored in the order of their parents' storage slots
+// (the sorted order of the last step, so the next sort moves little): the
+// fields the step moves and the momentum pair at storage slot os, the
+// fields kept in reference order (Ap, Fb, xp, yp: slots 11, 14, 15, 20, 21;
+// label, level) at the particle's index orf of the compacted reference
+// order, and idx[os] = orf.
+__device__ __forceinline__ bool ms_ref_slot(int k) {
+  return k == 11 || k == 14 || k == 15 || k == 20 || k == 21;
+}
+__device__ __forceinline__ void store_particle(const Fields& out, int* __restrict__ out_idx,
+                                               const double (&v)[kMsFields], int label,
+                                               int level, int os, int orf) {
+#pragma unroll
+  for (int k = 0; k < kMsFields; ++k) out.f[k][ms_ref_slot(k) ? orf : os] = v[k];
+  out.label[orf] = label;
+  out.level[orf] = level;
+  out_idx[os] = orf;
+}
+
+// every particle as it is (slot i, index idx[i]); the grid's share
 __device__ __forceinline__ void emit_identity(const Fields& in, const Fields& out, int np,
-                                              const int* ridx) {
+                                              const int* ridx, int* out_idx) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
-    const int o = ridx[i];
+    double v[kMsFields];
 #pragma unroll
-    for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
-    out.label[o] = in.label[i];
-    out.level[o] = in.level[i];
+    for (int k = 0; k < kMsFields; ++k) v[k] = in.f[k][i];
+    store_particle(out, out_idx, v, in.label[i], in.level[i], i, ridx[i]);
   }
 }
 
-__global__ void k_ms_emit(Fields in, Fields out, const int* act,
-                          const int* partner, const int* offs, const int* ridx, Geom G,
-                          long long cap, Scalars* S) {
+// oslot: exclusive scan of the weights in storage-slot order; offs: the same
+// in reference order (scattered through idx)
+__global__ void k_ms_emit(Fields in, Fields out, const int* act, const int* partner,
+                          const int* offs, const int* oslot, const int* ridx,
+                          int* out_idx, Geom G, long long cap, Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   const int nnew = offs[cap];
   if (nnew > cap) {  // the state goes through unchanged (the caller exchanges buffers)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
-    emit_identity(in, out, np, ridx);
+    emit_identity(in, out, np, ridx, out_idx);
     return;
   }
   const double eps = 1e-10;
@@ -402,14 +425,13 @@ __global__ void k_ms_emit(Fields in, Fields out, const int* act,
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
     const int a = act[i];
-    const int o = offs[ridx[i]];
+    const int os = oslot[i], orf = offs[ridx[i]];
+    double v[kMsFields];
     if (a == KEEP) {
 #pragma unroll
-      for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
-      out.label[o] = in.label[i];
-      out.level[o] = in.level[i];
+      for (int k = 0; k < kMsFields; ++k) v[k] = in.f[k][i];
+      store_particle(out, out_idx, v, in.label[i], in.level[i], os, orf);
     } else if (a == SPLIT) {
-      const int o2 = o + 1;
       const int level = in.level[i];
       // principal_stretch_dir (merge_split_ops_cmes.h:93-110)
       const double exx = in.f[16][i], eyy = in.f[19][i];
@@ -428,31 +450,19 @@ __global__ void k_ms_emit(Fields in, Fields out, const int* act,
       const double r_i = sqrt(in.f[11][i]);
       const double off = 0.25 * r_i;
       const double cx = in.f[0][i], cy = in.f[1][i];
-      auto clampx = [&](double v) { return v < eps ? eps : (v > Lx - eps ? Lx - eps : v); };
-      auto clampy = [&](double v) { return v < eps ? eps : (v > Ly - eps ? Ly - eps : v); };
+      auto clampx = [&](double w) { return w < eps ? eps : (w > Lx - eps ? Lx - eps : w); };
+      auto clampy = [&](double w) { return w < eps ? eps : (w > Ly - eps ? Ly - eps : w); };
       const double nx1 = clampx(cx + off * ux), ny1 = clampy(cy + off * uy);
       const double nx2 = clampx(cx - off * ux), ny2 = clampy(cy - off * uy);
 #pragma unroll
-      for (int k = 0; k < kMsFields; ++k) {
-        const double val = in.f[k][i] / (extensive(k) ? 2.0 : 1.0);
-        out.f[k][o] = val;
-        out.f[k][o2] = val;
-      }
-      const double h = out.f[4][o];
-      out.f[11][o] = out.f[9][o] / h;
-      out.f[11][o2] = out.f[9][o2] / h;
-      out.f[0][o] = nx1; out.f[1][o] = ny1;
-      out.f[0][o2] = nx2; out.f[1][o2] = ny2;
-      out.f[20][o] = nx1; out.f[21][o] = ny1;
-      out.f[20][o2] = nx2; out.f[21][o2] = ny2;
-      out.f[12][o] = out.f[8][o] * out.f[2][o];
-      out.f[12][o2] = out.f[8][o2] * out.f[2][o2];
-      out.f[13][o] = out.f[8][o] * out.f[3][o];
-      out.f[13][o2] = out.f[8][o2] * out.f[3][o2];
-      out.level[o] = level - 1;
-      out.level[o2] = level - 1;
-      out.label[o] = -1;
-      out.label[o2] = -1;
+      for (int k = 0; k < kMsFields; ++k) v[k] = in.f[k][i] / (extensive(k) ? 2.0 : 1.0);
+      v[11] = v[9] / v[4];  // Ap = Vp / hp
+      v[12] = v[8] * v[2];
+      v[13] = v[8] * v[3];
+      v[0] = nx1; v[1] = ny1; v[20] = nx1; v[21] = ny1;
+      store_particle(out, out_idx, v, -1, level - 1, os, orf);
+      v[0] = nx2; v[1] = ny2; v[20] = nx2; v[21] = ny2;
+      store_particle(out, out_idx, v, -1, level - 1, os + 1, orf + 1);
     } else if (a == MERGE_PRIMARY) {
       const int j = partner[i];
       const int level = in.level[i];
@@ -462,17 +472,13 @@ __global__ void k_ms_emit(Fields in, Fields out, const int* act,
       const double ny = (M1 * in.f[1][i] + M2 * in.f[1][j]) / Mt;
 #pragma unroll
       for (int k = 0; k < kMsFields; ++k)
-        out.f[k][o] = extensive(k) ? (in.f[k][i] + in.f[k][j])
-                                   : (M1 * in.f[k][i] + M2 * in.f[k][j]) / Mt;
-      out.f[4][o] = out.f[9][o] / out.f[11][o];  // hp = Vp / Ap
-      out.f[0][o] = nx;
-      out.f[1][o] = ny;
-      out.f[20][o] = nx;
-      out.f[21][o] = ny;
-      out.f[12][o] = out.f[8][o] * out.f[2][o];
-      out.f[13][o] = out.f[8][o] * out.f[3][o];
-      out.level[o] = level + 1;
-      out.label[o] = -1;
+        v[k] = extensive(k) ? (in.f[k][i] + in.f[k][j])
+                            : (M1 * in.f[k][i] + M2 * in.f[k][j]) / Mt;
+      v[4] = v[9] / v[11];  // hp = Vp / Ap
+      v[0] = nx; v[1] = ny; v[20] = nx; v[21] = ny;
+      v[12] = v[8] * v[2];
+      v[13] = v[8] * v[3];
+      store_particle(out, out_idx, v, -1, level + 1, os, orf);
     }
   }
 }
@@ -714,30 +720,30 @@ __global__ void k_elfs_mark(Particles p, const int* __restrict__ hops, const int
 // clamped into the domain) with the extensive fields divided by 4 and the
 // momentum rebuilt; a merge leaves the centre of mass with the extensive
 // fields summed, the rest mass-averaged and the primary's label.
-__global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
-                               const int* partner, const int* offs, const int* ridx, Geom G,
-                               long long cap, Scalars* S) {
+__global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act, const int* partner,
+                               const int* offs, const int* oslot, const int* ridx,
+                               int* out_idx, Geom G, long long cap, Scalars* S) {
   if (!S->active) return;
   const int np = S->np;
   const int nnew = offs[cap];
   if (nnew > cap) {  // the state goes through unchanged (the caller exchanges buffers)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&S->status, kStatusCapacity);
-    emit_identity(in, out, np, ridx);
+    emit_identity(in, out, np, ridx, out_idx);
     return;
   }
   const double eps = 1e-10;
   const double Lx = G.ncols * G.hx, Ly = G.nrows * G.hy;
-  auto clampx = [&](double v) { return v < eps ? eps : (v > Lx - eps ? Lx - eps : v); };
-  auto clampy = [&](double v) { return v < eps ? eps : (v > Ly - eps ? Ly - eps : v); };
+  auto clampx = [&](double w) { return w < eps ? eps : (w > Lx - eps ? Lx - eps : w); };
+  auto clampy = [&](double w) { return w < eps ? eps : (w > Ly - eps ? Ly - eps : w); };
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
     const int a = act[i];
-    const int o = offs[ridx[i]];
+    const int os = oslot[i], orf = offs[ridx[i]];
+    double v[kMsFields];
     if (a == KEEP) {
 #pragma unroll
-      for (int k = 0; k < kMsFields; ++k) out.f[k][o] = in.f[k][i];
-      out.label[o] = in.label[i];
-      out.level[o] = in.level[i];
+      for (int k = 0; k < kMsFields; ++k) v[k] = in.f[k][i];
+      store_particle(out, out_idx, v, in.label[i], in.level[i], os, orf);
     } else if (a == SPLIT) {
       const double off = sqrt(in.f[11][i]) / 2.0;
       const double px = in.f[0][i], py = in.f[1][i];
@@ -747,19 +753,13 @@ __global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
                             clampy(py - off)};
       const int level = in.level[i];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int t = o + q;
+      for (int k = 0; k < kMsFields; ++k) v[k] = in.f[k][i] / (extensive(k) ? 4.0 : 1.0);
+      v[12] = v[8] * v[2];
+      v[13] = v[8] * v[3];
 #pragma unroll
-        for (int k = 0; k < kMsFields; ++k)
-          out.f[k][t] = in.f[k][i] / (extensive(k) ? 4.0 : 1.0);
-        out.f[0][t] = xs[q];
-        out.f[1][t] = ys[q];
-        out.f[20][t] = xs[q];
-        out.f[21][t] = ys[q];
-        out.f[12][t] = out.f[8][t] * out.f[2][t];
-        out.f[13][t] = out.f[8][t] * out.f[3][t];
-        out.level[t] = level - 1;
-        out.label[t] = -1;
+      for (int q = 0; q < 4; ++q) {
+        v[0] = xs[q]; v[1] = ys[q]; v[20] = xs[q]; v[21] = ys[q];
+        store_particle(out, out_idx, v, -1, level - 1, os + q, orf + q);
       }
     } else if (a == MERGE_PRIMARY) {
       const int j = partner[i];
@@ -767,14 +767,13 @@ __global__ void k_ms_emit_elfs(Fields in, Fields out, const int* act,
       const double Mt = M1 + M2;
 #pragma unroll
       for (int k = 0; k < kMsFields; ++k)
-        out.f[k][o] = extensive(k) ? (in.f[k][i] + in.f[k][j])
-                                   : (M1 * in.f[k][i] + M2 * in.f[k][j]) / Mt;
-      out.f[20][o] = out.f[0][o];
-      out.f[21][o] = out.f[1][o];
-      out.f[12][o] = out.f[8][o] * out.f[2][o];
-      out.f[13][o] = out.f[8][o] * out.f[3][o];
-      out.level[o] = in.level[i] + 1;
-      out.label[o] = in.label[i];
+        v[k] = extensive(k) ? (in.f[k][i] + in.f[k][j])
+                            : (M1 * in.f[k][i] + M2 * in.f[k][j]) / Mt;
+      v[20] = v[0];
+      v[21] = v[1];
+      v[12] = v[8] * v[2];
+      v[13] = v[8] * v[3];
+      store_particle(out, out_idx, v, in.label[i], in.level[i] + 1, os, orf);
     }
   }
 }
@@ -873,9 +872,10 @@ int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const i
                                     m.paired, p, c, S);
   k_ms_demote<<<gp, 256, 0, st>>>(m.act, m.partner, c, S);
   n += 2;
-  k_ms_weights<<<gp, 256, 0, st>>>(m.act, p.idx, m.w, ic, c.split_w, S);
+  k_ms_weights<<<gp, 256, 0, st>>>(m.act, p.idx, m.w, m.flag, ic, c.split_w, S);
   n += 5;
   n += scan_enqueue(m.w, m.offs, ic, m.tile_sum, m.ntiles, S, st);
+  n += scan_enqueue(m.flag, m.rank, ic, m.tile_sum, m.ntiles, S, st);
   Fields in{}, out{};
   double* pf[kMsFields] = {pv.x,   pv.y,   pv.vpx, pv.vpy, pv.hp,     pv.F11,
                            pv.F12, pv.F22, pv.Mp,  pv.Vp,  pv.H,      pv.Ap,
@@ -894,9 +894,11 @@ int ms_enqueue(MsBuffers& m, Particles p, Particles q, const int* start, const i
   out.label = m.slabel;
   out.level = m.slevel;
   if (elfs)
-    k_ms_emit_elfs<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, p.idx, G, cap, S);
+    k_ms_emit_elfs<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, m.rank, p.idx,
+                                       q.idx, G, cap, S);
   else
-    k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, p.idx, G, cap, S);
+    k_ms_emit<<<gp, 256, 0, st>>>(in, out, m.act, m.partner, m.offs, m.rank, p.idx, q.idx, G,
+                                  cap, S);
   // the reference-order fields back into their arrays
   Fields fixed{};
   fixed.f[11] = p.Ap;

@@ -137,17 +137,17 @@ __global__ void k_init_particles(ParticlesT<R> p, const double* __restrict__ Z,
   }
 }
 
-// Recomputes the cell key of every particle, with the slots in reference
-// order (idx = slot), after a merge/split emit or a state upload; the next
-// sort scans every cell.
-__global__ void k_keys(Particles p, Geom G, Scalars* S) {
+// Recomputes the cell key of every particle after a merge/split emit (which
+// wrote idx) or a state upload (slots in reference order: set_idx sets
+// idx = slot); the next sort scans every cell.
+__global__ void k_keys(Particles p, Geom G, Scalars* S, int set_idx) {
   const int np = S->np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += gridDim.x * blockDim.x) {
     const int r = cell_row(p.y[i], G);
     const int c = cell_col(p.x[i], G);
     p.key[i] = r + c * G.nrows;
-    p.idx[i] = i;
+    if (set_idx) p.idx[i] = i;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S->knext[0] = 0;
@@ -226,10 +226,11 @@ __global__ void k_prep(ParticlesT<R> p, const double* __restrict__ Z, Geom G,
       Ap = hp > R(1.e-2) ? p.Vp[i] / hp : R(0);
       rheology_friction<R>(P, p.vpx[i], p.vpy[i], hp, fbx, fby);
       p.mp[i] = V2<R>{p.vpx[i] * p.Mp[i], p.vpy[i] * p.Mp[i]};
-    } else {
-      Ap = p.Ap[i];
-      fbx = p.Fbx[i];
-      fby = p.Fby[i];
+    } else {  // the stored values, in reference order
+      const int r = p.idx[i];
+      Ap = p.Ap[r];
+      fbx = p.Fbx[r];
+      fby = p.Fby[r];
     }
     p.qf[i] = V2<R>{Ap * fbx, Ap * fby};
     R xi, eta, gx, gy;
