@@ -78,10 +78,9 @@ struct dampm_batch {
   long long launches = 0;
   // tuning: P2G units per CTA and the weight of a column in the unit plan
   int units_per_cta = kUnitsPerCta, col_weight = kColWeight;
-  // passes captured in a CUDA graph, replayed while the layout holds; one
-  // graph per half the passes start from (an odd pass count alternates)
+  // kBatchGraphPasses passes captured in a CUDA graph, replayed while the
+  // layout holds; one graph per half the passes start from
   int use_graphs = 1;
-  int graph_passes[2] = {0, 0};
   bool graph_dirty[2] = {true, true};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   std::vector<void*> allocs;
@@ -648,51 +647,68 @@ int dampm_batch_compact(dampm_batch* b) {
   return upload_tables(b);
 }
 
+// Passes per graph: even, so that a replay ends on the half it began.
+constexpr int kBatchGraphPasses = 16;
+
+// The graph of kBatchGraphPasses passes from half h, captured after any
+// change of layout (the launches' sizes and pointers depend only on the
+// layout and on the half the passes start from; every other change lives in
+// device memory).  Nothing runs.
+int ensure_batch_graph(dampm_batch* b, int h) {
+  if (!b->graph_dirty[h] && b->graph[h]) return DAMPM_OK;
+  if (b->graph[h]) {
+    cudaGraphExecDestroy(b->graph[h]);
+    b->graph[h] = nullptr;
+  }
+  const int cur0 = b->cur;
+  const long long l0 = b->launches;
+  b->cur = h;
+  BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = DAMPM_OK;
+  for (int k = 0; k < kBatchGraphPasses && rc == DAMPM_OK; ++k) rc = enqueue_pass(b);
+  b->launches = l0;
+  b->cur = cur0;  // nothing ran
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
+  const cudaError_t ei = cudaGraphInstantiate(&b->graph[h], g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    b->graph[h] = nullptr;
+    return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
+  }
+  b->graph_dirty[h] = false;
+  return DAMPM_OK;
+}
+
 int dampm_batch_step(dampm_batch* b, int nsteps) {
   if (!b || nsteps < 0) return DAMPM_ERR_ARG;
   if (b->scns.empty() || nsteps == 0) return DAMPM_OK;
-  if (!b->use_graphs || nsteps < 2) {
-    for (int k = 0; k < nsteps; ++k) {
-      int rc = enqueue_pass(b);
-      if (rc) return rc;
+  // no graph of our own inside the caller's capture
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool graphs = b->use_graphs &&
+                      cudaStreamIsCapturing(b->stream, &cs) == cudaSuccess &&
+                      cs == cudaStreamCaptureStatusNone;
+  int left = nsteps;
+  if (graphs && left >= kBatchGraphPasses) {
+    const int h = b->cur;
+    int rc = ensure_batch_graph(b, h);
+    if (rc) return rc;
+    for (; left >= kBatchGraphPasses; left -= kBatchGraphPasses) {
+      BCK(cudaGraphLaunch(b->graph[h], b->stream));
+      b->launches += (long long)kPassLaunches * kBatchGraphPasses;
     }
-    return DAMPM_OK;
   }
-  // nsteps passes as one CUDA graph: captured after any change of layout or
-  // pass count, replayed otherwise (the launches' sizes and pointers depend
-  // only on the layout and on the half the passes start from; every other
-  // change lives in device memory)
-  const int h = b->cur;
-  if (b->graph_dirty[h] || b->graph_passes[h] != nsteps || !b->graph[h]) {
-    if (b->graph[h]) {
-      cudaGraphExecDestroy(b->graph[h]);
-      b->graph[h] = nullptr;
-    }
-    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    const long long l0 = b->launches;
-    int rc = DAMPM_OK;
-    for (int k = 0; k < nsteps && rc == DAMPM_OK; ++k) rc = enqueue_pass(b);
-    b->launches = l0;
-    b->cur = h;  // nothing ran yet
-    cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-    if (rc) {
-      if (g) cudaGraphDestroy(g);
-      return rc;
-    }
-    if (e != cudaSuccess) return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(e));
-    const cudaError_t ei = cudaGraphInstantiate(&b->graph[h], g, 0);
-    cudaGraphDestroy(g);
-    if (ei != cudaSuccess) {
-      b->graph[h] = nullptr;
-      return bfail(b, DAMPM_ERR_CUDA, cudaGetErrorString(ei));
-    }
-    b->graph_passes[h] = nsteps;
-    b->graph_dirty[h] = false;
+  for (; left > 0; --left) {
+    int rc = enqueue_pass(b);
+    if (rc) return rc;
   }
-  BCK(cudaGraphLaunch(b->graph[h], b->stream));
-  if (nsteps & 1) b->cur = 1 - h;
-  b->launches += (long long)kPassLaunches * nsteps;
+  // the graph the next call starts from, captured now rather than inside it
+  if (graphs) return ensure_batch_graph(b, b->cur);
   return DAMPM_OK;
 }
 

@@ -372,10 +372,12 @@ int dampm_batch_remove(dampm_batch* b, int handle);
 int dampm_batch_compact(dampm_batch* b);
 
 /* Enqueues nsteps passes of every live scenario (asynchronous); a scenario
- * whose loop condition fails does nothing in a pass.  With two or more
- * passes they run as one CUDA graph, captured on the batch stream when the
- * layout or the pass count changed since the last call and replayed
- * otherwise (see dampm_batch_tune). */
+ * whose loop condition fails does nothing in a pass.  Each run of 16 passes
+ * replays one CUDA graph, captured on the batch stream after a change of
+ * layout; the passes left over are launched one by one.  Before returning,
+ * the call captures (without running it) the graph the next call starts
+ * from, if the layout changed.  Inside the caller's own capture of the
+ * stream every pass is launched one by one (see dampm_batch_tune). */
 int dampm_batch_step(dampm_batch* b, int nsteps);
 int dampm_batch_sync(dampm_batch* b);
 

@@ -100,11 +100,13 @@ def test_graphs_and_tuning_change_no_result(cuda_lib):
         hs = [b.add(d) for d in ds]
         b.tune(units_per_cta=8, col_weight=64, graphs=False)
         b.step(6)
+        # two replays of the 16-pass graph, then 5 passes one by one (the
+        # next call starts from the other half)
         b.tune(units_per_cta=2, col_weight=512, graphs=True)
-        b.step(6)
-        info = b.autotune(passes=2, units=(2, 4), weights=(192,))
+        b.step(37)
+        info = b.autotune(passes=16, units=(2, 4), weights=(192,))
         assert info["units_per_cta"] in (2, 4) and info["passes"] > 0
         b.sync()
-        total = 12 + info["passes"]
+        total = 43 + info["passes"]
         for h, d in zip(hs, ds):
             check_same(b, h, d, total)
