@@ -880,6 +880,13 @@ int dampm_step(dampm_ctx* ctx, int nsteps) {
     int rc = enqueue_pass(ctx);
     if (rc) return rc;
   }
+  // without merge/split, the graph the next call starts from (the buffers of
+  // an odd count of passes are exchanged), captured now rather than inside it
+  if (len > 0 && !ms_cadence(ctx)) {
+    dampm_ctx::GraphSlot* g = nullptr;
+    int rc = ensure_graph(ctx, len, phase, &g);
+    if (rc) return rc;
+  }
   ev_mark(ctx, 3);
   return DAMPM_OK;
 }

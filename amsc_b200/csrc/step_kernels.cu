@@ -986,6 +986,143 @@ __device__ __forceinline__ void chain_group(Chains<R>& a, const P2GSmemT<R>& s, 
     chain_range<R, kG, true>(a, s, a0, a1, b1, bb, be, sh, own, lp0, lp1, lp2);
 }
 
+// ---- a batch inside one crowded cell ---------------------------------------
+// When a whole batch lies in one cell (rc, cc), only two lanes of each warp
+// have work in it: lane rc+1 (the cell is its cell r-1: local nodes 1 and 3)
+// and lane rc (its cell r: local nodes 0 and 2), each walking the batch's
+// records one after another for its 2 to 8 chains.  Those chains -- 9
+// quantities at each of the 4 nodes, the fin chains only outside a lead
+// column -- and the cell's 3 ledger sums go through shared memory to one
+// thread each, which walks the records with the operations of chain_step in
+// the same order (so every sum is the same, bit for bit), and come back.
+// A thread's chains are one kind per warp (warp 0: N * value, warp 1: the
+// internal forces, warp 2: the ledger), so a warp's threads run the same
+// instructions on different operands.
+constexpr int kSoloMin = 32;  // records of a batch worth handing over
+
+// The row of the cell that holds all of [bb, be), or -1, from the lanes'
+// ranges of their two cells ([a0, a1): cell r-1, [a1, b1): cell r): every
+// warp holds the same ranges, so each finds the same row without a barrier.
+__device__ __forceinline__ int solo_row(int a0, int a1, int b1, int bb, int be, int r0) {
+  if (be - bb < kSoloMin) return -1;
+  const unsigned lo = __ballot_sync(0xffffffffu, b1 > a1 && a1 <= bb && be <= b1);
+  if (lo) return r0 + __ffs(lo) - 1;
+  const unsigned up = __ballot_sync(0xffffffffu, a1 > a0 && a0 <= bb && be <= a1);
+  if (up) return r0 + __ffs(up) - 2;
+  return -1;
+}
+
+// All threads of the block call it.  rc: the cell's row; chain (role, fs, q)
+// sits at X[2 id] with its compensation at X[2 id + 1], id = (2 role + fs) 9 + q,
+// role 0 for lane rc+1 and 1 for lane rc, fs 0 for the fin chains, 1 for the
+// started ones, q the quantity (0-2 group 0, 3-6 group 1, 7 and 8 groups 2, 3).
+template <class R>
+__device__ __forceinline__ void solo_batch(Chains<R>& a, P2GSmemT<R>& s, int rc, int r0,
+                                           int nrows, int grp, int slot0, int nq, bool lead,
+                                           bool own, int n, const ShapeT<R>& sh,
+                                           double& lp0, double& lp1, double& lp2) {
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int lup = rc + 1 - r0, llo = rc - r0;
+  const bool pup = lup >= 0 && lup < kTR && rc + 1 <= nrows;
+  const bool plo = llo >= 0 && llo < kTR && rc <= nrows;
+  R* X = &s.xch[0][0];
+  const int mine = (pup && lane == lup) ? 0 : ((plo && lane == llo) ? 1 : -1);
+  if (mine >= 0) {
+#pragma unroll
+    for (int k = 0; k < kMaxQ; ++k) {
+      if (k < nq) {
+        const int idf = (2 * mine) * 9 + slot0 + k, ids = idf + 9;
+        X[2 * idf] = a.f[k];
+        X[2 * idf + 1] = a.fc[k];
+        X[2 * ids] = a.s[k];
+        X[2 * ids + 1] = a.sc[k];
+      }
+    }
+    if (grp == 0 && mine == 1) {
+      s.led[0][0] = lp0;
+      s.led[1][0] = lp1;
+      s.led[2][0] = lp2;
+    }
+  }
+  __syncthreads();
+  if (w == 0 && lane < 28) {  // Mv, mom_x, mom_y, FPx, FPy, Fric_x, Fric_y
+    const int q = lane % 7, rf = lane / 7;
+    const int role = rf >> 1, fs = rf & 1;
+    if ((role == 0 ? pup : plo) && (fs == 1 || !lead)) {
+      const int id = rf * 9 + q;
+      R v = X[2 * id], c = X[2 * id + 1];
+      const bool single = q == 0;
+      const R* pb = reinterpret_cast<const R*>(s.pr[single ? 1 : (q + 1) >> 1]);
+      const int half = (q + 1) & 1;
+      for (int j = 0; j < n; ++j) {
+        const int l2 = swz_pair<R>(j), l1 = swz_one<R>(j);
+        const V2<R> xe = s.pr[0][l2];
+        const R xi = xe.x, eta = xe.y;
+        const R fa = R(1) - xi;
+        const R fb = role == 0 ? eta : (R(1) - eta);
+        const R N = (fs == 0 ? fa : xi) * fb;
+        const R val = single ? s.sg[0][l1] : pb[2 * l2 + half];
+        acc_add(v, c, N * val);
+      }
+      X[2 * id] = v;
+      X[2 * id + 1] = c;
+    }
+  } else if (w == 1 && lane < 8) {  // F_int_x, F_int_y
+    const int qb = lane & 1, rf = lane >> 1;
+    const int role = rf >> 1, fs = rf & 1;
+    if ((role == 0 ? pup : plo) && (fs == 1 || !lead)) {
+      const int id = rf * 9 + 7 + qb;
+      R v = X[2 * id], c = X[2 * id + 1];
+      const R hy = role == 0 ? sh.ihy : sh.mihy;
+      const R hxs = fs == 0 ? sh.mihx : sh.ihx;
+      const R* P1 = s.sg[qb == 0 ? 1 : 2];  // F11 or F12
+      const R* P2 = s.sg[qb == 0 ? 2 : 3];  // F12 or F22
+      for (int j = 0; j < n; ++j) {
+        const int l2 = swz_pair<R>(j), l1 = swz_one<R>(j);
+        const V2<R> xe = s.pr[0][l2];
+        const R xi = xe.x, eta = xe.y;
+        const R fa = R(1) - xi;
+        const R fb = role == 0 ? eta : (R(1) - eta);
+        const R Nx = hxs * fb;
+        const R Ny = (fs == 0 ? fa : xi) * hy;
+        const R vv = Nx * P1[l1] + Ny * P2[l1];
+        acc_add(v, c, vv * s.sg[4][l1]);
+      }
+      X[2 * id] = v;
+      X[2 * id + 1] = c;
+    }
+  } else if (w == 2 && lane < 3) {  // the particle ledger of lane rc (Mp, mom)
+    if (plo && own) {
+      double lp = s.led[lane][0];
+      const R* pb = reinterpret_cast<const R*>(s.pr[1]);
+      for (int j = 0; j < n; ++j) {
+        const int l2 = swz_pair<R>(j), l1 = swz_one<R>(j);
+        lp += lane == 0 ? s.sg[0][l1] : pb[2 * l2 + (lane - 1)];
+      }
+      s.led[lane][0] = lp;
+    }
+  }
+  __syncthreads();
+  if (mine >= 0) {
+#pragma unroll
+    for (int k = 0; k < kMaxQ; ++k) {
+      if (k < nq) {
+        const int idf = (2 * mine) * 9 + slot0 + k, ids = idf + 9;
+        a.f[k] = X[2 * idf];
+        a.fc[k] = X[2 * idf + 1];
+        a.s[k] = X[2 * ids];
+        a.sc[k] = X[2 * ids + 1];
+      }
+    }
+    if (grp == 0 && mine == 1) {
+      lp0 = s.led[0][0];
+      lp1 = s.led[1][0];
+      lp2 = s.led[2][0];
+    }
+  }
+  __syncthreads();  // the exchange space is free again
+}
+
 }  // namespace
 
 // ---- P2G work units -------------------------------------------------------
@@ -1245,11 +1382,19 @@ __device__ __forceinline__ void p2g_unit(
     const bool own = r >= r0 && r < r0 + kTR && cur.cc >= cA && cur.cc >= G.pc_lo &&
                      cur.cc < G.pc_hi;
     const bool lead = cur.cc < cA;  // started chains only
-    switch (grp) {
-      case 0: chain_group<R, 0>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      case 1: chain_group<R, 1>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      case 2: chain_group<R, 2>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
-      default: chain_group<R, 3>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+    const int rc = solo_row(a0, a1, b1, cur.bb, cur.be, r0);  // the same in every warp
+    if (rc >= 0) {
+      // own as the cell's lower lane sees it (its row lies in the unit)
+      const bool own_c = cur.cc >= cA && cur.cc >= G.pc_lo && cur.cc < G.pc_hi;
+      solo_batch<R>(a, s, rc, r0, nrows, grp, slot0, nq, lead, own_c, cur.be - cur.bb, sh,
+                    lp0, lp1, lp2);
+    } else {
+      switch (grp) {
+        case 0: chain_group<R, 0>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        case 1: chain_group<R, 1>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        case 2: chain_group<R, 2>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+        default: chain_group<R, 3>(a, s, lead, a0, a1, b1, cur.bb, cur.be, sh, own, lp0, lp1, lp2); break;
+      }
     }
     if (last_of_col) {
       if (lane_ok)

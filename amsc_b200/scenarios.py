@@ -296,6 +296,34 @@ def mudflow(N: int = 2048, h: float = 0.5, seed: int = DEFAULT_SEED,
     return DATA(arrays, sc)
 
 
+def crowded_cells(seed: int = 5, nsteps: int = 200) -> DATA:
+    """Cells crowded with hundreds to thousands of particles, as a fixed-dt
+    ensemble member that has gone unstable piles its particles against a
+    wall: a 48 x 48 grid of 0.5 m cells on a bumpy slope, an elliptic release
+    at 4 x 4 particles per cell, and three cells holding 700, 1500 (the same
+    cell column) and 5000 particles at uniform random positions.  Bingham +
+    Voellmy, adaptive CFL 0.4."""
+    rng = np.random.default_rng(seed)
+    N, h = 48, 0.5
+    L = N * h
+    Z, dZdx, dZdy = _bumpy_slope(N, N, h, 0.3, 8, (0.0, 2.0), (1.0, 4.0), rng, slope_ref=L)
+    xp, yp, hp, Ap = _ellipse_release(N, N, h, 4, 0.5 * L, 0.5 * L, 6.0, 4.0, 2.0)
+    xs, ys, hs, As = [xp], [yp], [hp], [Ap]
+    for col, row, m in ((20, 10, 700), (20, 14, 1500), (30, 24, 5000)):
+        xs.append((col + rng.uniform(0.02, 0.98, m)) * h)
+        ys.append((row + rng.uniform(0.02, 0.98, m)) * h)
+        hs.append(np.full(m, 0.5))
+        As.append(np.full(m, h * h / m))
+    arrays = _particles(np.concatenate(xs), np.concatenate(ys), np.concatenate(hs),
+                        np.concatenate(As), 1800.0)
+    arrays.update({"Z": Z, "dZdx": dZdx, "dZdy": dZdy})
+    sc = _base_scalars(Nex=N, Ney=N, hx=h, hy=h, rho=1800.0, T=1e30, xi=500.0, mu=50.0,
+                       phi=20.0, tauy=500.0, BINGHAM_ON=1.0, FRICTION_ON=1.0, CFL=0.4,
+                       BC_FLAG=1, MERGE_SPLIT_ON=0, eq_level=0.0, DT_FIXED=0.0,
+                       NSTEPS=nsteps)
+    return DATA(arrays, sc)
+
+
 def ensemble_member(seed: int, side_range=(64, 512), h: float = 1.0,
                     dt: float = 0.02, nsteps: int = 1000) -> DATA:
     """One scenario of the batched ensemble: square grid (side log-uniform),
