@@ -262,7 +262,7 @@ int enqueue_pass(dampm_batch* b) {
                                             b->sortbuf, b->cmid, b->Sg);
   k_segment_order_mid<<<148 * 8, 256, 0, st>>>(b->start, b->cmid, b->clist_n, b->perm,
                                                 b->sortbuf, b->cbig, b->Sg);
-  k_segment_order_big<<<148, 1024, 0, st>>>(b->start, b->cbig, b->clist_n, b->perm,
+  k_segment_order_big<<<148, 1024, sort_big_smem_bytes(), st>>>(b->start, b->cbig, b->clist_n, b->perm,
                                             b->sortbuf, b->P_cap, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
       b->start, b->scn, b->S, b->strip_scn, b->Sg, b->units_per_cta * b->p2g_grid,
@@ -457,6 +457,7 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
     cudaMemsetAsync(b->Sg, 0, sizeof(Scalars), b->stream);
     const int per_sm = f32 ? setup_b_p2g<float>() : setup_b_p2g<double>();
     if (per_sm == 0) rc = bfail(b, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+    if (!setup_sort()) rc = bfail(b, DAMPM_ERR_CUDA, "cannot configure the sort's shared memory");
     int nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

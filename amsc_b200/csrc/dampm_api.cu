@@ -269,7 +269,7 @@ void enqueue_sort(dampm_ctx* ctx) {
   k_segment_order_mid<<<148 * 8, 256, 0, ctx->stream>>>(ctx->start, ctx->cmid,
                                                        ctx->clist_n, ctx->perm, ctx->sortbuf,
                                                        ctx->cbig, ctx->S);
-  k_segment_order_big<<<148, 1024, 0, ctx->stream>>>(ctx->start, ctx->cbig, ctx->clist_n,
+  k_segment_order_big<<<148, 1024, sort_big_smem_bytes(), ctx->stream>>>(ctx->start, ctx->cbig, ctx->clist_n,
                                                      ctx->perm, ctx->sortbuf, ctx->cap,
                                                      ctx->S);
   ctx->launches += 6;
@@ -711,6 +711,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
     cudaMemsetAsync(ctx->S, 0, sizeof(Scalars), ctx->stream);
     int per_sm = setup_p2g(), nsm = 0, dev = 0;
     if (per_sm == 0) rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure P2G shared memory");
+    if (!setup_sort()) rc = fail(ctx, DAMPM_ERR_CUDA, "cannot configure the sort's shared memory");
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (per_sm < 1) per_sm = 1;

@@ -173,6 +173,10 @@ __global__ void k_segment_order_mid(const int* start, const int* mid, int* list_
 __global__ void k_segment_order_big(const int* start, const int* big,
                                     const int* list_n, int* perm, unsigned long long* pk,
                                     long long cap, const Scalars* S);
+// dynamic shared memory of k_segment_order_big; setup_sort sets its limit
+// (0 on failure)
+size_t sort_big_smem_bytes();
+int setup_sort();
 __global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
                              int target_units, int seg, int* ustart,
                              long long* upex, int2* plan, int* strip_n);

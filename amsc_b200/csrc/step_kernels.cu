@@ -473,7 +473,7 @@ __global__ void k_scatter(const int* __restrict__ key,
 // k_segment_order_big.
 constexpr int kThreadSort = 16;
 constexpr int kRankPer = 8;
-constexpr int kBigRun = 4096;
+constexpr int kBigRun = 16384;  // entries of a sorted run (128 KB of shared memory)
 constexpr unsigned long long kNoEntry = ~0ull;
 
 __device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m,
@@ -605,18 +605,19 @@ __global__ void __launch_bounds__(256, 4) k_segment_order_mid(const int* __restr
 
 // Crowded cells (more than 32 * kRankPer particles), one block of 1024
 // threads each: runs of up to kBigRun entries of tmp[b, b+m) (the pk the
-// scatter wrote) are sorted by a bitonic network in shared memory and
-// written back; longer cells then merge the sorted runs pairwise (each
-// output position finds its split by a binary search along the merge
-// path), ping-ponging between tmp[b, b+m) and tmp[cap + b, cap + b + m); the
-// slots go back to perm.
+// scatter wrote) are sorted by a bitonic network in shared memory (dynamic,
+// kBigRun entries) and written back; longer cells then merge the sorted runs
+// pairwise, ping-ponging between tmp[b, b+m) and tmp[cap + b, cap + b + m):
+// each thread finds where its piece of the output starts by a binary search
+// along the merge path, then merges the piece sequentially.  The slots go
+// back to perm.
 __global__ void __launch_bounds__(1024)
     k_segment_order_big(const int* __restrict__ start, const int* __restrict__ big,
                         const int* __restrict__ list_n, int* __restrict__ perm,
                         unsigned long long* __restrict__ tmp, long long cap,
                         const Scalars* S) {
   if (!S->active) return;
-  __shared__ unsigned long long sv[kBigRun];
+  extern __shared__ unsigned long long sv[];  // kBigRun entries
   const int nb = list_n[1];
   for (int q = blockIdx.x; q < nb; q += gridDim.x) {
     const int c = big[q];
@@ -649,19 +650,26 @@ __global__ void __launch_bounds__(1024)
     unsigned long long* src = tmp + b;
     unsigned long long* dst = tmp + cap + b;
     for (int w = kBigRun; w < m; w <<= 1) {
-      for (int k = threadIdx.x; k < m; k += blockDim.x) {
-        const int lo = (k / (2 * w)) * (2 * w);
+      for (int lo = 0; lo < m; lo += 2 * w) {  // runs [lo, lo+w) and [lo+w, lo+2w)
         const int la = min(w, m - lo), lb = max(0, min(w, m - lo - la));
+        const int tot = la + lb;
         const unsigned long long* A = src + lo;
         const unsigned long long* B = A + la;
-        const int kk = k - lo;
-        int i0 = max(0, kk - lb), i1 = min(kk, la);
+        const int per = (tot + int(blockDim.x) - 1) / int(blockDim.x);
+        const int k0 = min(int(threadIdx.x) * per, tot), k1 = min(k0 + per, tot);
+        if (k0 >= k1) continue;
+        // output k0 takes i of A and k0 - i of B
+        int i0 = max(0, k0 - lb), i1 = min(k0, la);
         while (i0 < i1) {
           const int mid = (i0 + i1) >> 1;
-          if (A[mid] < B[kk - mid - 1]) i0 = mid + 1; else i1 = mid;
+          if (A[mid] < B[k0 - mid - 1]) i0 = mid + 1; else i1 = mid;
         }
-        const int j = kk - i0;
-        dst[k] = (j >= lb || (i0 < la && A[i0] < B[j])) ? A[i0] : B[j];
+        int i = i0, j = k0 - i0;
+        for (int k = k0; k < k1; ++k) {
+          // i + j == k < tot, so j >= lb leaves i < la
+          const bool take_a = j >= lb || (i < la && A[i] < B[j]);
+          dst[lo + k] = take_a ? A[i++] : B[j++];
+        }
       }
       __syncthreads();
       unsigned long long* t = src;
@@ -1477,6 +1485,13 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     if (ui >= nunits) break;
     p2g_unit(p, perm, cstart, nodes, led_part, G, P, S, record, s, ui, ulist[ui]);
   }
+}
+
+size_t sort_big_smem_bytes() { return sizeof(unsigned long long) * kBigRun; }
+
+int setup_sort() {
+  return cudaFuncSetAttribute(k_segment_order_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(sort_big_smem_bytes())) == cudaSuccess;
 }
 
 int setup_p2g() {

@@ -300,16 +300,16 @@ def crowded_cells(seed: int = 5, nsteps: int = 200) -> DATA:
     """Cells crowded with hundreds to thousands of particles, as a fixed-dt
     ensemble member that has gone unstable piles its particles against a
     wall: a 48 x 48 grid of 0.5 m cells on a bumpy slope, an elliptic release
-    at 4 x 4 particles per cell, and three cells holding 700, 1500 (the same
-    cell column) and 5000 particles at uniform random positions.  Bingham +
-    Voellmy, adaptive CFL 0.4."""
+    at 4 x 4 particles per cell, and four cells holding 700, 1500 (the same
+    cell column), 5000 and 20000 particles at uniform random positions.
+    Bingham + Voellmy, adaptive CFL 0.4."""
     rng = np.random.default_rng(seed)
     N, h = 48, 0.5
     L = N * h
     Z, dZdx, dZdy = _bumpy_slope(N, N, h, 0.3, 8, (0.0, 2.0), (1.0, 4.0), rng, slope_ref=L)
     xp, yp, hp, Ap = _ellipse_release(N, N, h, 4, 0.5 * L, 0.5 * L, 6.0, 4.0, 2.0)
     xs, ys, hs, As = [xp], [yp], [hp], [Ap]
-    for col, row, m in ((20, 10, 700), (20, 14, 1500), (30, 24, 5000)):
+    for col, row, m in ((20, 10, 700), (20, 14, 1500), (30, 24, 5000), (40, 40, 20000)):
         xs.append((col + rng.uniform(0.02, 0.98, m)) * h)
         ys.append((row + rng.uniform(0.02, 0.98, m)) * h)
         hs.append(np.full(m, 0.5))

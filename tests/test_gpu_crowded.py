@@ -26,7 +26,8 @@ def _cells(d):
 def test_scenario_has_crowded_cells():
     d = scenarios.crowded_cells()
     cnt = np.bincount(_cells(d))
-    assert cnt.max() > 4096 and (cnt >= 512).sum() == 3  # one above a sorted run
+    # one cell above a sorted run of the per-cell order (16384 entries)
+    assert cnt.max() > 16384 and (cnt >= 512).sum() == 4
 
 
 @pytest.mark.gpu
@@ -41,8 +42,11 @@ def test_crowded_cells_bitwise_against_oracle(cuda_lib):
         assert st["it"] == o.it and st["t"] == o.t
         for k in FIELDS:
             np.testing.assert_array_equal(s.download(k), o.get(k), err_msg=k)
+        # the ledger totals are summed per P2G unit, then over the units (the
+        # oracle sums particle by particle): round-off of the order, 2e-12
+        # relative here, where 32,000 particles' masses span four decades
         led_g, led_o = s.ledgers(), o.ledger()
-        np.testing.assert_allclose(led_g[:6], led_o[:6], rtol=1e-12, atol=1e-9)
+        np.testing.assert_allclose(led_g[:6], led_o[:6], rtol=1e-11, atol=1e-9)
 
 
 @pytest.mark.gpu
