@@ -473,7 +473,7 @@ __global__ void k_scatter(const int* __restrict__ key,
 // k_segment_order_big.
 constexpr int kThreadSort = 16;
 constexpr int kRankPer = 8;
-constexpr int kBigRun = 16384;  // entries of a sorted run (128 KB of shared memory)
+constexpr int kBigRun = 8192;  // entries of a sorted run (two buffers: 128 KB of shared memory)
 constexpr unsigned long long kNoEntry = ~0ull;
 
 __device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m,
@@ -507,24 +507,60 @@ __device__ __forceinline__ void thread_sort_segment(int* __restrict__ seg, int m
     if (k < m) seg[k] = int(unsigned(v[k]));
 }
 
+// the 32 values of a warp (one per lane) in ascending order across the lanes
+__device__ __forceinline__ unsigned long long warp_bitonic32(unsigned long long v, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, j);
+      const bool up = ((lane & k) == 0);
+      const bool lower = ((lane & j) == 0);
+      // keep the min in the lower lane of an ascending pair
+      v = (lower == up) ? min(v, o) : max(v, o);
+    }
+  }
+  return v;
+}
+
+// One level of a merge sort along the merge path: src holds sorted runs of w
+// entries over [0, len) (the last one shorter), dst receives runs of 2w.
+// Each thread writes a contiguous piece of the output: it finds where the
+// piece starts in the two runs by a binary search, then merges sequentially
+// (again after a search where the piece enters the next pair of runs).
+__device__ __forceinline__ void merge_level(const unsigned long long* src,
+                                            unsigned long long* dst, int len, int w) {
+  const int per = (len + int(blockDim.x) - 1) / int(blockDim.x);
+  int k = min(int(threadIdx.x) * per, len);
+  const int k1 = min(k + per, len);
+  while (k < k1) {
+    const int lo = (k / (2 * w)) * (2 * w);
+    const int la = min(w, len - lo), lb = max(0, min(w, len - lo - la));
+    const unsigned long long* A = src + lo;
+    const unsigned long long* B = A + la;
+    const int kk = k - lo;
+    int i0 = max(0, kk - lb), i1 = min(kk, la);  // output kk takes i of A, kk - i of B
+    while (i0 < i1) {
+      const int mid = (i0 + i1) >> 1;
+      if (A[mid] < B[kk - mid - 1]) i0 = mid + 1; else i1 = mid;
+    }
+    int i = i0, j = kk - i0;
+    const int kend = min(k1, lo + la + lb);
+    for (; k < kend; ++k) {
+      // i + j < la + lb, so j >= lb leaves i < la
+      const bool take_a = j >= lb || (i < la && A[i] < B[j]);
+      dst[k] = take_a ? A[i++] : B[j++];
+    }
+  }
+}
+
 __device__ __forceinline__ void warp_sort_segment(int* __restrict__ perm, int b, int m,
                                                   int c, int lane,
                                                   const unsigned long long* __restrict__ pk,
                                                   int* __restrict__ big,
                                                   int* __restrict__ list_n) {
   if (m <= 32) {
-    unsigned long long v = (lane < m) ? pk[b + lane] : kNoEntry;
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, j);
-        const bool up = ((lane & k) == 0);
-        const bool lower = ((lane & j) == 0);
-        // keep the min in the lower lane of an ascending pair
-        v = (lower == up) ? min(v, o) : max(v, o);
-      }
-    }
+    const unsigned long long v = warp_bitonic32((lane < m) ? pk[b + lane] : kNoEntry, lane);
     if (lane < m) perm[b + lane] = int(unsigned(v));
   } else if (m <= 32 * kRankPer) {
     unsigned long long v[kRankPer];
@@ -605,46 +641,45 @@ __global__ void __launch_bounds__(256, 4) k_segment_order_mid(const int* __restr
 
 // Crowded cells (more than 32 * kRankPer particles), one block of 1024
 // threads each: runs of up to kBigRun entries of tmp[b, b+m) (the pk the
-// scatter wrote) are sorted by a bitonic network in shared memory (dynamic,
-// kBigRun entries) and written back; longer cells then merge the sorted runs
-// pairwise, ping-ponging between tmp[b, b+m) and tmp[cap + b, cap + b + m):
-// each thread finds where its piece of the output starts by a binary search
-// along the merge path, then merges the piece sequentially.  The slots go
-// back to perm.
+// scatter wrote) are sorted in shared memory -- groups of 32 by a bitonic
+// network in each warp's registers, then merged level by level along the
+// merge path between two buffers -- and written back; longer cells then
+// merge the sorted runs pairwise, ping-ponging between tmp[b, b+m) and
+// tmp[cap + b, cap + b + m): each thread finds where its piece of the output
+// starts by a binary search along the merge path, then merges the piece
+// sequentially.  The slots go back to perm.
 __global__ void __launch_bounds__(1024)
     k_segment_order_big(const int* __restrict__ start, const int* __restrict__ big,
                         const int* __restrict__ list_n, int* __restrict__ perm,
                         unsigned long long* __restrict__ tmp, long long cap,
                         const Scalars* S) {
   if (!S->active) return;
-  extern __shared__ unsigned long long sv[];  // kBigRun entries
+  extern __shared__ unsigned long long sv[];  // two buffers of kBigRun entries
   const int nb = list_n[1];
   for (int q = blockIdx.x; q < nb; q += gridDim.x) {
     const int c = big[q];
     const int b = start[c], m = start[c + 1] - b;
     for (int r0 = 0; r0 < m; r0 += kBigRun) {
       const int len = min(kBigRun, m - r0);
-      int P = 1;
-      while (P < len) P <<= 1;
-      for (int i = threadIdx.x; i < P; i += blockDim.x)
-        sv[i] = (i < len) ? tmp[b + r0 + i] : kNoEntry;
-      __syncthreads();
-      for (int k = 2; k <= P; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          for (int i = threadIdx.x; i < P; i += blockDim.x) {
-            const int ixj = i ^ j;
-            if (ixj > i) {
-              const unsigned long long a = sv[i], d = sv[ixj];
-              if ((a > d) == ((i & k) == 0)) {
-                sv[i] = d;
-                sv[ixj] = a;
-              }
-            }
-          }
-          __syncthreads();
-        }
+      unsigned long long* A = sv;
+      unsigned long long* B = sv + kBigRun;
+      // groups of 32 sorted in registers, one warp each, then merged level
+      // by level between the two buffers
+      const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      for (int g = threadIdx.x >> 5; g * 32 < len; g += nw) {
+        const int q = g * 32 + lane;
+        const unsigned long long v = warp_bitonic32(q < len ? tmp[b + r0 + q] : kNoEntry, lane);
+        if (q < len) A[q] = v;
       }
-      for (int i = threadIdx.x; i < len; i += blockDim.x) tmp[b + r0 + i] = sv[i];
+      __syncthreads();
+      for (int w = 32; w < len; w <<= 1) {
+        merge_level(A, B, len, w);
+        __syncthreads();
+        unsigned long long* t = A;
+        A = B;
+        B = t;
+      }
+      for (int i = threadIdx.x; i < len; i += blockDim.x) tmp[b + r0 + i] = A[i];
       __syncthreads();
     }
     unsigned long long* src = tmp + b;
@@ -1487,7 +1522,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
   }
 }
 
-size_t sort_big_smem_bytes() { return sizeof(unsigned long long) * kBigRun; }
+size_t sort_big_smem_bytes() { return 2 * sizeof(unsigned long long) * kBigRun; }
 
 int setup_sort() {
   return cudaFuncSetAttribute(k_segment_order_big, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -326,6 +326,8 @@ def run_ensemble(args, world, rank, local):
     _barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.profile_timed:
+        torch.cuda.profiler.start()
     e0.record(stream)
     tuned = None
     if args.autotune:
@@ -335,6 +337,8 @@ def run_ensemble(args, world, rank, local):
         b.step(K)
     e1.record(stream)
     torch.cuda.synchronize()
+    if args.profile_timed:
+        torch.cuda.profiler.stop()
     clocks = sampler.stop()
     el_ms = _allreduce(e0.elapsed_time(e1), world)
     launches = b.usage()["launches"] - l0
@@ -600,6 +604,9 @@ def main():
     ap.add_argument("--scenarios", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-timed", action="store_true",
+                    help="ensemble: bracket the timed passes with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-late", dest="late", action="store_false",
                     help="mudflow workload: skip the window at step 1000")
