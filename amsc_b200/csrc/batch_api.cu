@@ -65,8 +65,9 @@ struct dampm_batch {
   int* cmid = nullptr;  // cells with more than 16 particles
   int* ustart = nullptr;
   long long* upex = nullptr;
-  int2* uplan = nullptr;
+  int4* uplan = nullptr;  // {cA, cB, heavy, 0}
   int4* ulist = nullptr;
+  int* uorder = nullptr;  // the order P2G takes the units in
   int *strip_n = nullptr, *ucount = nullptr, *strip_scn = nullptr;
   double* led_part = nullptr;
   int2 *scn_units = nullptr, *gblk = nullptr;
@@ -266,18 +267,18 @@ int enqueue_pass(dampm_batch* b) {
                                             b->sortbuf, b->P_cap, b->Sg);
   k_b_units_plan<<<b->strips_tot, kPlanThreads, 0, st>>>(
       b->start, b->scn, b->S, b->strip_scn, b->Sg, b->units_per_cta * b->p2g_grid,
-      b->col_weight, b->ustart, b->upex, b->uplan, b->strip_n);
+      b->col_weight, b->ustart, b->upex, b->uplan, b->strip_n, b->ucount + 3);
   k_b_units_flat<<<1, kPlanThreads, sizeof(int) * (b->strips_tot + 1), st>>>(
-      b->strip_n, b->strips_tot, b->strip_scn, b->scn, nscn, b->uplan, b->ulist,
+      b->strip_n, b->strips_tot, b->strip_scn, b->scn, nscn, b->uplan, b->ulist, b->uorder,
       b->ucount, b->scn_units, b->S, b->Sg);
   if (b->precision == DAMPM_FP32)
     launch_b_p2g<float>(b->p2g_grid, st, b->p32[b->cur], b->perm, b->start,
                         static_cast<float2*>(b->vvL),
-                        b->led_part, b->scn, b->S, b->ulist, b->ucount, b->Sg);
+                        b->led_part, b->scn, b->S, b->ulist, b->uorder, b->ucount, b->Sg);
   else
     launch_b_p2g<double>(b->p2g_grid, st, b->p64[b->cur], b->perm, b->start,
                          static_cast<double2*>(b->vvL),
-                         b->led_part, b->scn, b->S, b->ulist, b->ucount, b->Sg);
+                         b->led_part, b->scn, b->S, b->ulist, b->uorder, b->ucount, b->Sg);
   k_b_ledger<<<nscn, 256, 0, st>>>(b->led_part, b->scn_units, b->scn, b->S, nscn,
                                    b->Sg);
   if (b->precision == DAMPM_FP32)
@@ -436,10 +437,13 @@ int dampm_batch_create(long long particle_cap, long long node_cap, int scenario_
   rc = rc ? rc : balloc(b, &b->upex, us);
   rc = rc ? rc : balloc(b, &b->uplan, us);
   rc = rc ? rc : balloc(b, &b->ulist, us);
+  rc = rc ? rc : balloc(b, &b->uorder, us);
   rc = rc ? rc : balloc(b, &b->led_part, us * 6);
   rc = rc ? rc : balloc(b, &b->strip_n, size_t(b->STRIP_cap));
   rc = rc ? rc : balloc(b, &b->strip_scn, size_t(b->STRIP_cap));
-  rc = rc ? rc : balloc(b, &b->ucount, 2);
+  rc = rc ? rc : balloc(b, &b->ucount, 4);
+  if (rc == DAMPM_OK && cudaMemsetAsync(b->ucount, 0, sizeof(int) * 4, b->stream) != cudaSuccess)
+    rc = bfail(b, DAMPM_ERR_CUDA, "cudaMemsetAsync failed");
   rc = rc ? rc : balloc(b, &b->scn_units, size_t(scenario_cap));
   rc = rc ? rc : balloc(b, &b->gblk, size_t(b->B_cap));
   rc = rc ? rc : balloc(b, &b->mblk, size_t(b->B_cap));

@@ -43,8 +43,9 @@ struct dampm_ctx {
   int strips = 0, useg = 0;  // strips; unit slots per strip (ncols + 1)
   int *ustart = nullptr, *strip_n = nullptr, *ucount = nullptr;
   long long* upex = nullptr;
-  int2* uplan = nullptr;
+  int4* uplan = nullptr;  // {cA, cB, heavy, 0}
   int4* ulist = nullptr;
+  int* uorder = nullptr;  // the order P2G takes the units in
   int *clist = nullptr, *clist_n = nullptr;  // cells with >= 2 particles
   int* cbig = nullptr;  // cells with more than 256 particles (capacity / 256)
   int* cmid = nullptr;  // cells with more than 16 particles (capacity / 17)
@@ -302,9 +303,10 @@ int enqueue_front(dampm_ctx* ctx) {
   ev_mark(ctx, 1);
   k_units_plan<<<ctx->strips, kPlanThreads, 0, ctx->stream>>>(
       ctx->start, ctx->G, ctx->S, kUnitsPerCta * ctx->p2g_grid, ctx->useg, ctx->ustart,
-      ctx->upex, ctx->uplan, ctx->strip_n);
+      ctx->upex, ctx->uplan, ctx->strip_n, ctx->ucount + 3);
   k_units_flat<<<1, kPlanThreads, sizeof(int) * (ctx->strips + 1), ctx->stream>>>(
-      ctx->strip_n, ctx->strips, ctx->useg, ctx->uplan, ctx->ulist, ctx->ucount, ctx->S);
+      ctx->strip_n, ctx->strips, ctx->useg, ctx->uplan, ctx->ulist, ctx->uorder, ctx->ucount,
+      ctx->S);
   if (ctx->record) {
     Nodes& n = ctx->nodes;
     double* nf[] = {n.Mv,  n.mvx,  n.mvy,   n.avx,   n.avy,  n.vvx, n.vvy,
@@ -314,7 +316,7 @@ int enqueue_front(dampm_ctx* ctx) {
     cudaMemsetAsync(n.vvL, 0, sizeof(double2) * ctx->nn, ctx->stream);
   }
   launch_p2g(ctx->p2g_grid, ctx->stream, ctx->p, ctx->perm, ctx->start, ctx->nodes,
-             ctx->led_part, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0, ctx->ulist,
+             ctx->led_part, ctx->G, ctx->P, ctx->S, ctx->record ? 1 : 0, ctx->ulist, ctx->uorder,
              ctx->ucount);
   ctx->launches += 2;
   ev_mark(ctx, 3);
@@ -698,8 +700,9 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   rc = rc ? rc : dalloc(ctx, &ctx->upex, size_t(ctx->n_led));
   rc = rc ? rc : dalloc(ctx, &ctx->uplan, size_t(ctx->n_led));
   rc = rc ? rc : dalloc(ctx, &ctx->ulist, size_t(ctx->n_led));
+  rc = rc ? rc : dalloc(ctx, &ctx->uorder, size_t(ctx->n_led));
   rc = rc ? rc : dalloc(ctx, &ctx->strip_n, size_t(ctx->strips));
-  rc = rc ? rc : dalloc(ctx, &ctx->ucount, 2);
+  rc = rc ? rc : dalloc(ctx, &ctx->ucount, 4);
   rc = rc ? rc : dalloc(ctx, &ctx->ledger_log, size_t(kLedgerLog) * 3);
   rc = rc ? rc : dalloc(ctx, &ctx->S, 1);
   if (rc == DAMPM_OK) {
@@ -707,6 +710,7 @@ int dampm_ctx_create(const dampm_grid* grid, const dampm_params* params,
   }
   if (rc == DAMPM_OK) {
     cudaMemsetAsync(ctx->count, 0, sizeof(int) * ctx->nc, ctx->stream);
+    cudaMemsetAsync(ctx->ucount, 0, sizeof(int) * 4, ctx->stream);
     cudaMemsetAsync(ctx->nodes.vvL, 0, sizeof(double2) * nn, ctx->stream);
     cudaMemsetAsync(ctx->S, 0, sizeof(Scalars), ctx->stream);
     int per_sm = setup_p2g(), nsm = 0, dev = 0;

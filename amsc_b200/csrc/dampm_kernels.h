@@ -179,16 +179,18 @@ size_t sort_big_smem_bytes();
 int setup_sort();
 __global__ void k_units_plan(const int* cstart, Geom G, const Scalars* S,
                              int target_units, int seg, int* ustart,
-                             long long* upex, int2* plan, int* strip_n);
+                             long long* upex, int4* plan, int* strip_n, int* heavy_n);
+// the flat unit list and uorder, the order P2G hands the units out in
+// (heavy units first)
 __global__ void k_units_flat(const int* strip_n, int strips, int seg,
-                             const int2* plan, int4* ulist, int* ucount,
+                             const int4* plan, int4* ulist, int* uorder, int* ucount,
                              const Scalars* S);
 // P2G of the single-scenario step (k_p2g specialised for recorded outputs);
 // setup_p2g sets its shared-memory attributes and returns the resident CTAs
 // per SM (0 on failure)
 void launch_p2g(int grid, cudaStream_t st, Particles p, const int* perm, const int* cstart,
                 Nodes nodes, double* led_part, Geom G, Phys P, const Scalars* S, int record,
-                const int4* ulist, const int* ucount);
+                const int4* ulist, const int* uorder, const int* ucount);
 int setup_p2g();
 constexpr int kLedgerLog = 1024;  // rows of the per-step ledger log
 __global__ void k_ledger_final(const double* led_part, const int* ucount,
@@ -219,17 +221,18 @@ __global__ void k_b_step_end(const Scn* scn, Scalars* S, int nscn);
 __global__ void k_b_units_plan(const int* cstart, const Scn* scn, const Scalars* S,
                                const int* strip_scn, const Scalars* Sg,
                                int target_units, int col_weight, int* ustart,
-                               long long* upex, int2* plan, int* strip_n);
+                               long long* upex, int4* plan, int* strip_n, int* heavy_n);
 __global__ void k_b_units_flat(const int* strip_n, int strips, const int* strip_scn,
-                               const Scn* scn, int nscn, const int2* plan,
-                               int4* ulist, int* ucount, int2* scn_units,
+                               const Scn* scn, int nscn, const int4* plan,
+                               int4* ulist, int* uorder, int* ucount, int2* scn_units,
                                Scalars* S, const Scalars* Sg);
 __global__ void k_b_tile_flags(const Scn* scn, const Scalars* S, int nscn, const Scalars* Sg,
                                unsigned char* tflag, int ntiles);
 template <class R>
 void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
                   const int* cstart, V2<R>* vvL, double* led_part, const Scn* scn,
-                  Scalars* S, const int4* ulist, const int* ucount, const Scalars* Sg);
+                  Scalars* S, const int4* ulist, const int* uorder, const int* ucount,
+                  const Scalars* Sg);
 // sets the batched P2G kernel's shared-memory attributes; returns the
 // resident CTAs per SM (0 on failure)
 template <class R>

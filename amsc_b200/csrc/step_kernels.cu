@@ -1224,8 +1224,8 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
                                           const Geom& G, long long T, int strip,
                                           int* __restrict__ st,
                                           long long* __restrict__ px,
-                                          int2* __restrict__ plan, int col_weight,
-                                          int c_lo, int c_hi) {
+                                          int4* __restrict__ plan, int col_weight,
+                                          int c_lo, int c_hi, int* __restrict__ heavy_n) {
   __shared__ long long wt_ll[32];
   __shared__ int wt_i[32];
   __shared__ long long last_id;
@@ -1266,7 +1266,7 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
   int J = 0;
   for (int base = 0; base < K; base += blockDim.x) {
     const int k = base + threadIdx.x;
-    int flag = 0, cA = 0, cB = 0;
+    int flag = 0, cA = 0, cB = 0, heavy = 0;
     if (k < K) {
       cA = st[k];
       const bool more = k + 1 < K;
@@ -1275,10 +1275,13 @@ __device__ __forceinline__ int plan_strip(const int* __restrict__ cstart,
       const long long n = sumw - (long long)col_weight * (min(cB, ncols) - cA) +
                           (cA > 0 ? column_count(cstart, rlo, rhi, cA - 1, nrows) : 0);
       flag = n > 0;
+      // more than twice the target weight (a crowded column): heavy
+      heavy = n > 2 * T ? 1 : 0;
     }
     int jtot;
     const int jin = block_incl_scan<int>(flag, wt_i, jtot);
-    if (flag) plan[J + jin - 1] = make_int2(cA, cB);
+    if (flag) plan[J + jin - 1] = make_int4(cA, cB, heavy, 0);  // P2G takes heavy units first
+    if (flag && heavy) atomicAdd(heavy_n, 1);
     J += jtot;
   }
   return J;
@@ -1293,8 +1296,8 @@ __device__ __forceinline__ long long unit_weight(const Scalars* S,
 __global__ void __launch_bounds__(kPlanThreads)
     k_units_plan(const int* __restrict__ cstart, Geom G, const Scalars* S,
                  int target_units, int seg, int* __restrict__ ustart,
-                 long long* __restrict__ upex, int2* __restrict__ plan,
-                 int* __restrict__ strip_n) {
+                 long long* __restrict__ upex, int4* __restrict__ plan,
+                 int* __restrict__ strip_n, int* __restrict__ heavy_n) {
   if (!S->active) return;
   const int strip = blockIdx.x;
   const size_t b = (size_t)strip * seg;
@@ -1307,18 +1310,43 @@ __global__ void __launch_bounds__(kPlanThreads)
   }
   const int c_lo = L / G.nrows, c_hi = min(H / G.nrows + 1, G.ncols);
   const int J = plan_strip(cstart, G, unit_weight(S, target_units), strip,
-                           ustart + b, upex + b, plan + b, kColWeight, c_lo, c_hi);
+                           ustart + b, upex + b, plan + b, kColWeight, c_lo, c_hi, heavy_n);
   if (threadIdx.x == 0) strip_n[strip] = J;
+}
+
+// The order P2G hands the units out in: the heavy ones first, then the
+// others, each group in list order (a stable partition; heavy(f) is 0 or 1).
+// A unit's ledger slot stays its list position, so the order changes no sum.
+// All threads of the block call it.
+template <class F>
+__device__ __forceinline__ void heavy_first(int total, F heavy, int* __restrict__ uorder,
+                                            int* wt) {
+  int hc = 0;
+  for (int f = threadIdx.x; f < total; f += blockDim.x) hc += heavy(f);
+  int H;
+  block_incl_scan<int>(hc, wt, H);
+  int carry = 0;
+  for (int base = 0; base < total; base += blockDim.x) {
+    const int f = base + threadIdx.x;
+    const int h = f < total ? heavy(f) : 0;
+    int tot;
+    const int incl = block_incl_scan<int>(h, wt, tot);
+    if (f < total) uorder[h ? carry + incl - 1 : H + f - (carry + incl)] = f;
+    carry += tot;
+  }
 }
 
 // One block: strip offsets by a scan of strip_n, then the flat unit list
 // {strip, cA, cB} in (strip, column) order.  ucount[0] = units,
-// ucount[1] = P2G's work cursor.
+// ucount[1] = P2G's work cursor, ucount[2] = heavy units (P2G reads uorder
+// when there are any, else takes the list in order), ucount[3] = the heavy
+// units the plan counts for the next list.
 __global__ void __launch_bounds__(kPlanThreads)
     k_units_flat(const int* __restrict__ strip_n, int strips, int seg,
-                 const int2* __restrict__ plan, int4* __restrict__ ulist,
-                 int* __restrict__ ucount, const Scalars* S) {
+                 const int4* __restrict__ plan, int4* __restrict__ ulist,
+                 int* __restrict__ uorder, int* __restrict__ ucount, const Scalars* S) {
   if (!S->active) return;
+  const int H = ucount[3];  // heavy units, counted by the plan
   extern __shared__ int uoff[];  // strips + 1
   __shared__ int wt_i[32];
   int carry = 0;
@@ -1339,12 +1367,18 @@ __global__ void __launch_bounds__(kPlanThreads)
       const int mid = (lo + hi) >> 1;
       if (uoff[mid] <= f) lo = mid; else hi = mid;
     }
-    const int2 u = plan[(size_t)lo * seg + (f - uoff[lo])];
-    ulist[f] = make_int4(lo, u.x, u.y, 0);
+    const int4 u = plan[(size_t)lo * seg + (f - uoff[lo])];
+    ulist[f] = make_int4(lo, u.x, u.y, u.z);  // w: heavy
+  }
+  if (H > 0) {
+    __syncthreads();
+    heavy_first(total, [&](int f) { return ulist[f].w; }, uorder, wt_i);
   }
   if (threadIdx.x == 0) {
     ucount[0] = total;
     ucount[1] = 0;
+    ucount[2] = H;  // P2G: list order when 0
+    ucount[3] = 0;
   }
 }
 
@@ -1503,21 +1537,24 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     k_p2g(Particles p, const int* __restrict__ perm,
           const int* __restrict__ cstart, Nodes nodes,
           double* __restrict__ led_part, Geom G, Phys P, const Scalars* S,
-          const int4* __restrict__ ulist, const int* __restrict__ ucount) {
+          const int4* __restrict__ ulist, const int* __restrict__ uorder,
+          const int* __restrict__ ucount) {
   constexpr int record = kRecord ? 1 : 0;
   if (!S->active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmem& s = *reinterpret_cast<P2GSmem*>(smem_raw);
-  const int nunits = ucount[0];
+  const int nunits = ucount[0], nheavy = ucount[2];
   __shared__ int next_unit;
   while (true) {
-    // units are taken in list order from a shared cursor: CTAs that drew
-    // light units take more (the per-SM load stays even)
+    // units are taken in the order of uorder (heavy ones first) from a
+    // shared cursor: CTAs that drew light units take more (the per-SM load
+    // stays even)
     if (threadIdx.x == 0) next_unit = atomicAdd(const_cast<int*>(ucount) + 1, 1);
     __syncthreads();
-    const int ui = next_unit;
+    const int k = next_unit;
     __syncthreads();
-    if (ui >= nunits) break;
+    if (k >= nunits) break;
+    const int ui = nheavy ? uorder[k] : k;
     p2g_unit(p, perm, cstart, nodes, led_part, G, P, S, record, s, ui, ulist[ui]);
   }
 }
@@ -1545,13 +1582,13 @@ int setup_p2g() {
 
 void launch_p2g(int grid, cudaStream_t st, Particles p, const int* perm, const int* cstart,
                 Nodes nodes, double* led_part, Geom G, Phys P, const Scalars* S, int record,
-                const int4* ulist, const int* ucount) {
+                const int4* ulist, const int* uorder, const int* ucount) {
   if (record)
     k_p2g<true><<<grid, kP2GThreads, p2g_smem_bytes(), st>>>(p, perm, cstart, nodes, led_part,
-                                                             G, P, S, ulist, ucount);
+                                                             G, P, S, ulist, uorder, ucount);
   else
     k_p2g<false><<<grid, kP2GThreads, p2g_smem_bytes(), st>>>(p, perm, cstart, nodes, led_part,
-                                                              G, P, S, ulist, ucount);
+                                                              G, P, S, ulist, uorder, ucount);
 }
 
 // Block reduction, in a fixed order, of the ledger partials of units
@@ -1991,8 +2028,8 @@ __global__ void __launch_bounds__(kPlanThreads)
                    const Scalars* S, const int* __restrict__ strip_scn,
                    const Scalars* Sg, int target_units, int col_weight,
                    int* __restrict__ ustart,
-                   long long* __restrict__ upex, int2* __restrict__ plan,
-                   int* __restrict__ strip_n) {
+                   long long* __restrict__ upex, int4* __restrict__ plan,
+                   int* __restrict__ strip_n, int* __restrict__ heavy_n) {
   const int b = blockIdx.x;
   const int s = strip_scn[b];
   if (!Sg->active || !S[s].active) {
@@ -2017,7 +2054,7 @@ __global__ void __launch_bounds__(kPlanThreads)
   }
   const int J = plan_strip(cstart + scn[s].c_off, G, unit_weight(Sg, target_units),
                            local, ustart + base, upex + base, plan + base, col_weight,
-                           c_lo, c_hi);
+                           c_lo, c_hi, heavy_n);
   if (threadIdx.x == 0) strip_n[b] = J;
 }
 
@@ -2057,10 +2094,12 @@ __global__ void k_b_tile_flags(const Scn* __restrict__ scn, const Scalars* S, in
 __global__ void __launch_bounds__(kPlanThreads)
     k_b_units_flat(const int* __restrict__ strip_n, int strips,
                    const int* __restrict__ strip_scn, const Scn* __restrict__ scn,
-                   int nscn, const int2* __restrict__ plan, int4* __restrict__ ulist,
-                   int* __restrict__ ucount, int2* __restrict__ scn_units,
+                   int nscn, const int4* __restrict__ plan, int4* __restrict__ ulist,
+                   int* __restrict__ uorder, int* __restrict__ ucount,
+                   int2* __restrict__ scn_units,
                    Scalars* S, const Scalars* Sg) {
   if (!Sg->active) return;
+  const int H = ucount[3];  // heavy units, counted by the plan
   extern __shared__ int uoff[];  // strips + 1
   __shared__ int wt_i[32];
   int carry = 0;
@@ -2085,8 +2124,20 @@ __global__ void __launch_bounds__(kPlanThreads)
     const int local = lo - scn[s].strip_off;
     const size_t base =
         (size_t)scn[s].useg_off + (size_t)local * (scn[s].G.ncols + 1);
-    const int2 u = plan[base + (f - uoff[lo])];
+    const int4 u = plan[base + (f - uoff[lo])];
     ulist[f] = make_int4(s, local, u.x, u.y);
+  }
+  if (H > 0) {
+    __syncthreads();
+    heavy_first(
+      total,
+      [&](int f) {
+        const int4 L = ulist[f];
+        const int st = scn[L.x].strip_off + L.y;
+        const size_t base = (size_t)scn[L.x].useg_off + (size_t)L.y * (scn[L.x].G.ncols + 1);
+        return plan[base + (f - uoff[st])].z;
+      },
+      uorder, wt_i);
   }
   for (int s = threadIdx.x; s < nscn; s += blockDim.x) {
     const int b0 = scn[s].strip_off, b1 = b0 + scn[s].nstrips;
@@ -2101,6 +2152,8 @@ __global__ void __launch_bounds__(kPlanThreads)
   if (threadIdx.x == 0) {
     ucount[0] = total;
     ucount[1] = 0;
+    ucount[2] = H;  // P2G: list order when 0
+    ucount[3] = 0;
   }
 }
 
@@ -2109,19 +2162,20 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinBlocks)
     k_b_p2g(ParticlesT<R> p, const int* __restrict__ perm, const int* __restrict__ cstart,
             V2<R>* __restrict__ vvL,
             double* __restrict__ led_part, const Scn* __restrict__ scn, Scalars* S,
-            const int4* __restrict__ ulist, const int* __restrict__ ucount,
-            const Scalars* Sg) {
+            const int4* __restrict__ ulist, const int* __restrict__ uorder,
+            const int* __restrict__ ucount, const Scalars* Sg) {
   if (!Sg->active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmemT<R>& sm = *reinterpret_cast<P2GSmemT<R>*>(smem_raw);
-  const int nunits = ucount[0];
+  const int nunits = ucount[0], nheavy = ucount[2];
   __shared__ int next_unit;
   while (true) {
     if (threadIdx.x == 0) next_unit = atomicAdd(const_cast<int*>(ucount) + 1, 1);
     __syncthreads();
-    const int ui = next_unit;
+    const int k = next_unit;
     __syncthreads();
-    if (ui >= nunits) break;
+    if (k >= nunits) break;
+    const int ui = nheavy ? uorder[k] : k;  // heavy units first
     const int4 u = ulist[ui];
     const Geom G = scn[u.x].G;
     const Phys P = scn[u.x].P;
@@ -2289,9 +2343,10 @@ void launch_prep(int grid, int block, cudaStream_t st, ParticlesT<R> p, const do
 template <class R>
 void launch_b_p2g(int grid, cudaStream_t st, ParticlesT<R> p, const int* perm,
                   const int* cstart, V2<R>* vvL, double* led_part, const Scn* scn,
-                  Scalars* S, const int4* ulist, const int* ucount, const Scalars* Sg) {
+                  Scalars* S, const int4* ulist, const int* uorder, const int* ucount,
+                  const Scalars* Sg) {
   k_b_p2g<R><<<grid, kP2GThreads, sizeof(P2GSmemT<R>), st>>>(
-      p, perm, cstart, vvL, led_part, scn, S, ulist, ucount, Sg);
+      p, perm, cstart, vvL, led_part, scn, S, ulist, uorder, ucount, Sg);
 }
 
 template <class R>
@@ -2331,7 +2386,7 @@ void launch_b_move(int grid, cudaStream_t st, ParticlesT<R> dst, ParticlesT<R> s
                                Geom, Phys, const Scalars*, int);                      \
   template void launch_b_p2g<R>(int, cudaStream_t, ParticlesT<R>, const int*,         \
                                 const int*, V2<R>*, double*, const Scn*, Scalars*,    \
-                                const int4*, const int*, const Scalars*);             \
+                                const int4*, const int*, const int*, const Scalars*); \
   template int setup_b_p2g<R>();                                                      \
   template void launch_b_g2p<R>(int, cudaStream_t, ParticlesT<R>, ParticlesT<R>,      \
                                 const int*, const int*, const V2<R>*, const double*,  \
